@@ -1,0 +1,53 @@
+// Batched eigensolver workspace and launch descriptor shared by the eigensolver
+// entry points and the synthesis pipeline.
+#pragma once
+
+#include "common.cuh"
+#include "context.hpp"
+
+namespace bippb200 {
+
+template <typename T>
+struct EigWork {
+  int capBatch = 0, Nmax = 0;
+  DevBuf A, G, W64, Linv, T1, Z, d, e, tau;
+  void reserve(bipp_ctx_s* ctx, int nBatch, int Nmax);
+  // compacted eigenvectors (column c = eigenvector of eigenvalue c), ld Nmax
+  typename Cplx<T>::type* X(bool gram);
+};
+
+template <typename T>
+struct EigLaunch {
+  int nBatch = 0;      // matrices in this launch
+  int nBeam = 0;       // rows/cols of S
+  int nAnt = 0;        // antennas (general W only)
+  int Nmax = 0;        // padded size (>= nBeam)
+  const typename Cplx<T>::type* S = nullptr;  // first matrix of this launch
+  long long sStride = 0;
+  int lds = 0;
+  const double* xyz = nullptr;  // positions of all matrices ([batch][3][ldxyz] via xyzStride)
+  long long xyzStride = 0;
+  int ldxyz = 0;
+  const double* wl = nullptr;   // [batch]
+  double hostWl = 0;
+  int mode = 0;                 // 0 eigh_gram flag test, 1 eigh flag test
+  T eps = 0;
+  bool gram = true;
+  bool identityW = true;
+  const typename Cplx<T>::type* W = nullptr;  // general W (single matrix)
+  int ldw = 0;
+  int hostNred = 0;             // nred of the single matrix (general W)
+  // per-matrix outputs indexed by batchOffset + b
+  int* idx = nullptr;           // [batch][Nmax]
+  int* nred = nullptr;          // [batch]
+  long long* nvis = nullptr;    // [batch]
+  int* status = nullptr;        // [batch]
+  double* lam = nullptr;        // [batch][Nmax]
+  int doFlag = 1;
+  int batchOffset = 0;
+};
+
+template <typename T>
+void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w);
+
+}  // namespace bippb200

@@ -1,0 +1,929 @@
+// Batched generalized Hermitian eigensolver kernels (sm_100a).
+//
+// Pipeline per matrix b of a batch (sizes vary per matrix after flagging):
+//   prep_kernel        flag non-zero rows/cols of S, compact S -> A (working precision),
+//                      Gram G_ij = sinc(2|p_i-p_j|/wl) -> G (FP64)       [src/eigensolver.cpp:148-207,
+//                                                                          src/host/gram_matrix.cpp:23-56]
+//   cholesky_kernel    G = L L^H in FP64                                   [LAPACK potrf inside ?hegv]
+//   trinv_kernel       Linv = L^-1 in FP64, rounded to working precision
+//   gemm_kernel        C = Linv S Linv^H (two triangular products)         [hegst]
+//   hetrd_kernel       C = Q T Q^H, T real tridiagonal (Householder)        [hetrd]
+//   tridiag_kernel     eigenpairs of T in FP64: bisection + twisted factorisation
+//   backtransform      Y = Q Z                                              [unmtr]
+//   gemm_kernel        X = Linv^H Y                                         [trsm back-transform]
+// One CTA owns one matrix in the sequential stages; matrices live in HBM with
+// leading dimension Nmax (the batch's padded size).
+#pragma once
+
+#include "common.cuh"
+
+namespace bippb200 {
+
+constexpr int kPrepThreads = 512;
+
+// ------------------------------------------------------------------------------------
+// prep: flagging, compaction, Gram
+// ------------------------------------------------------------------------------------
+// mode 0: eigh_gram flag test |s|^2 > eps (src/eigensolver.cpp:150-158)
+// mode 1: eigh flag test |Re| >= eps || |Im| >= eps (src/eigensolver.cpp:59-68)
+template <typename T>
+__global__ void __launch_bounds__(kPrepThreads)
+prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long sStride, int lds,
+            const double* __restrict__ xyz, long long xyzStride, int ldxyz,
+            const double* __restrict__ wl, int mode, T eps, int withGram, int Nmax,
+            int* __restrict__ idxOut, int* __restrict__ nredOut, long long* __restrict__ nvisOut,
+            typename Cplx<T>::type* __restrict__ A, double2* __restrict__ G, int* __restrict__ status,
+            int doFlag, int doCompact, int batchOffset) {
+  using C = typename Cplx<T>::type;
+  extern __shared__ int smem_i[];
+  int* flags = smem_i;                 // [Nmax]
+  int* idx = smem_i + Nmax;            // [Nmax]
+  __shared__ long long red_ll[32];
+  __shared__ int s_nred;
+  const int b = blockIdx.x;                 // matrix within this launch
+  const int bg = b + batchOffset;           // matrix within the flag/index arrays
+  const C* Sb = S + b * sStride;
+  int* idxB = idxOut + (long long)bg * Nmax;
+  if (doFlag) {
+    for (int i = threadIdx.x; i < nBeam; i += blockDim.x) flags[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    long long cnt = 0;
+    int bad = 0;
+    for (int col = warp; col < nBeam; col += nwarp) {
+      for (int row = col + lane; row < nBeam; row += 32) {
+        C v = Sb[row + (long long)col * lds];
+        if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+        bool nz = (mode == 0) ? (cabs2(v) > eps) : (fabs(v.x) >= eps || fabs(v.y) >= eps);
+        if (nz) {
+          flags[row] = 1;
+          flags[col] = 1;
+          cnt += (row == col) ? 1 : 2;
+        }
+      }
+    }
+    long long nvis = block_sum(cnt, red_ll);
+    if (bad) atomicOr(status + bg, (int)kStatusNonFinite);
+    __syncthreads();
+    // compaction scan (warp 0)
+    if (warp == 0) {
+      const int per = (nBeam + 31) / 32;
+      const int beg = lane * per, end = min(nBeam, beg + per);
+      int c = 0;
+      for (int i = beg; i < end; ++i) c += flags[i];
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      int pos = incl - c;
+      for (int i = beg; i < end; ++i)
+        if (flags[i]) idx[pos++] = i;
+      if (lane == 31) s_nred = incl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      nredOut[bg] = s_nred;
+      nvisOut[bg] = nvis;
+    }
+    for (int i = threadIdx.x; i < s_nred; i += blockDim.x) idxB[i] = idx[i];
+  } else {
+    if (threadIdx.x == 0) s_nred = nredOut[bg];
+    __syncthreads();
+    for (int i = threadIdx.x; i < s_nred; i += blockDim.x) idx[i] = idxB[i];
+    __syncthreads();
+  }
+  if (!doCompact) return;
+  const int nr = s_nred;
+
+  // compacted full Hermitian matrix from the lower triangle of S
+  C* Ab = A + (long long)b * Nmax * Nmax;
+  for (long long e = threadIdx.x; e < (long long)nr * nr; e += blockDim.x) {
+    const int r = (int)(e % nr), c = (int)(e / nr);
+    const int ir = idx[r], ic = idx[c];
+    C v;
+    if (r >= c) {
+      v = Sb[ir + (long long)ic * lds];
+    } else {
+      v = cconj(Sb[ic + (long long)ir * lds]);
+    }
+    if (r == c) v.y = 0;
+    Ab[r + (long long)c * Nmax] = v;
+  }
+  if (withGram) {
+    const double* xb = xyz + bg * xyzStride;
+    const double w = wl[bg];
+    double2* Gb = G + (long long)b * Nmax * Nmax;
+    for (long long e = threadIdx.x; e < (long long)nr * nr; e += blockDim.x) {
+      const int r = (int)(e % nr), c = (int)(e / nr);
+      if (r < c) continue;
+      double g = 1.0;
+      if (r != c) {
+        const int ir = idx[r], ic = idx[c];
+        const double dx = xb[ir] - xb[ic];
+        const double dy = xb[ir + ldxyz] - xb[ic + ldxyz];
+        const double dz = xb[ir + 2 * ldxyz] - xb[ic + 2 * ldxyz];
+        const double x = 2.0 * sqrt(dx * dx + dy * dy + dz * dz) / w;
+        g = (x != 0.0) ? sinpi(x) / (3.14159265358979323846 * x) : 1.0;
+      }
+      Gb[r + (long long)c * Nmax] = make_double2(g, 0.0);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Cholesky (FP64 complex, lower, in place), blocked right-looking, NB = 32
+// ------------------------------------------------------------------------------------
+constexpr int kCholNB = 32;
+constexpr int kCholThreads = 256;
+constexpr size_t kCholSmem = (size_t)(kCholNB + 128) * (kCholNB + 1) * sizeof(double2);
+
+static __global__ void __launch_bounds__(kCholThreads)
+cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status) {
+  const int b = blockIdx.x;
+  const int n = nred[b];
+  double2* Gb = G + (long long)b * Nmax * Nmax;
+  extern __shared__ double2 chol_smem[];
+  double2 (*D)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem);
+  double2 (*Pi)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem + kCholNB * (kCholNB + 1));
+  double2 (*Pj)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem + (kCholNB + 64) * (kCholNB + 1));
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) s_bad = 0;
+  const int tid = threadIdx.x;
+  for (int k0 = 0; k0 < n; k0 += kCholNB) {
+    const int kb = min(kCholNB, n - k0);
+    // 1. load diagonal block (lower)
+    __syncthreads();
+    for (int e = tid; e < kCholNB * kCholNB; e += blockDim.x) {
+      const int r = e % kCholNB, c = e / kCholNB;
+      D[r][c] = (r < kb && c < kb && r >= c) ? Gb[(k0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+    }
+    __syncthreads();
+    // 2. unblocked factorisation in smem
+    for (int j = 0; j < kb; ++j) {
+      if (tid == 0) {
+        double djj = D[j][j].x;
+        if (!(djj > 0.0)) {
+          s_bad = 1;
+          djj = 1e-300;
+        }
+        D[j][j] = make_double2(sqrt(djj), 0.0);
+      }
+      __syncthreads();
+      const double inv = 1.0 / D[j][j].x;
+      for (int r = j + 1 + tid; r < kb; r += blockDim.x) D[r][j] = cscale(D[r][j], inv);
+      __syncthreads();
+      // trailing update inside the block: D[r][c] -= D[r][j] conj(D[c][j]), j < c <= r
+      for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e % kb, c = e / kb;
+        if (c > j && r >= c) {
+          double2 t = D[r][c];
+          double2 a = D[r][j], bb = D[c][j];
+          t.x -= a.x * bb.x + a.y * bb.y;
+          t.y -= a.y * bb.x - a.x * bb.y;
+          D[r][c] = t;
+        }
+      }
+      __syncthreads();
+    }
+    // 3. write back diagonal block
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+      const int r = e % kb, c = e / kb;
+      if (r >= c) Gb[(k0 + r) + (long long)(k0 + c) * Nmax] = D[r][c];
+    }
+    // 4. panel: rows i >= k0+kb: x L_kk^H = a  (row-wise forward substitution)
+    for (int i = k0 + kb + tid; i < n; i += blockDim.x) {
+      double2 x[kCholNB];
+#pragma unroll
+      for (int c = 0; c < kCholNB; ++c) x[c] = (c < kb) ? Gb[i + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+#pragma unroll
+      for (int c = 0; c < kCholNB; ++c) {
+        if (c < kb) {
+          double2 acc = x[c];
+          for (int m = 0; m < c; ++m) {
+            // acc -= x[m] * conj(L[c][m])
+            const double2 l = D[c][m];
+            acc.x -= x[m].x * l.x + x[m].y * l.y;
+            acc.y -= x[m].y * l.x - x[m].x * l.y;
+          }
+          x[c] = cscale(acc, 1.0 / D[c][c].x);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < kCholNB; ++c)
+        if (c < kb) Gb[i + (long long)(k0 + c) * Nmax] = x[c];
+    }
+    __syncthreads();
+    // 5. trailing update A[i,j] -= sum_m P[i,m] conj(P[j,m]) for j <= i, tiles 64x64
+    const int t0 = k0 + kb;
+    const int nt = n - t0;
+    if (nt <= 0) continue;
+    const int ntile = (nt + 63) / 64;
+    for (int ti = 0; ti < ntile; ++ti) {
+      for (int tj = 0; tj <= ti; ++tj) {
+        const int i0 = t0 + ti * 64, j0 = t0 + tj * 64;
+        __syncthreads();
+        for (int e = tid; e < 64 * kCholNB; e += blockDim.x) {
+          const int r = e % 64, c = e / 64;
+          Pi[r][c] = (i0 + r < n && c < kb) ? Gb[(i0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+          Pj[r][c] = (j0 + r < n && c < kb) ? Gb[(j0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+        }
+        __syncthreads();
+        // each thread: 4x4 outputs; thread (tr, tc) in 16x16 grid
+        const int tr = tid % 16, tc = tid / 16;
+        double2 acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[a][c] = make_double2(0, 0);
+        for (int m = 0; m < kb; ++m) {
+          double2 pa[4], pb[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) pa[a] = Pi[tr + 16 * a][m];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) pb[c] = Pj[tc + 16 * c][m];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              acc[a][c].x += pa[a].x * pb[c].x + pa[a].y * pb[c].y;
+              acc[a][c].y += pa[a].y * pb[c].x - pa[a].x * pb[c].y;
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int i = i0 + tr + 16 * a, j = j0 + tc + 16 * c;
+            if (i < n && j < n && j <= i) {
+              double2* p = Gb + i + (long long)j * Nmax;
+              double2 v = *p;
+              v.x -= acc[a][c].x;
+              v.y -= acc[a][c].y;
+              *p = v;
+            }
+          }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_bad) atomicOr(status + b, (int)kStatusCholeskyNotPD);
+}
+
+// ------------------------------------------------------------------------------------
+// triangular inverse of the lower Cholesky factor (FP64), output in working precision
+// ------------------------------------------------------------------------------------
+template <typename C>
+__device__ __forceinline__ void store_conv(C* p, double2 v);
+template <> __device__ __forceinline__ void store_conv<float2>(float2* p, double2 v) { *p = to_f(v); }
+template <> __device__ __forceinline__ void store_conv<double2>(double2* p, double2 v) { *p = v; }
+
+// Linv is computed block row by block row: Linv[I,I] = inv(L[I,I]);
+// Linv[I,J] = -Linv[I,I] sum_{K=J}^{I-1} L[I,K] Linv[K,J].
+// The FP64 inverse is kept in the (now unused) upper part of G's storage? No: G's
+// strictly upper triangle holds no data, so Linv^T is not needed; Linv is written to
+// a separate FP64 buffer W64 and rounded into LinvOut.
+constexpr size_t kTrinvSmem = 3 * 32 * 33 * sizeof(double2);
+
+template <typename C>
+__global__ void __launch_bounds__(256)
+trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __restrict__ LinvOut,
+             const int* __restrict__ nred, int Nmax) {
+  constexpr int NB = 32;
+  const int b = blockIdx.x;
+  const int n = nred[b];
+  const double2* Lb = L + (long long)b * Nmax * Nmax;
+  double2* Wb = W64 + (long long)b * Nmax * Nmax;
+  C* Ob = LinvOut + (long long)b * Nmax * Nmax;
+  extern __shared__ double2 trinv_smem[];
+  double2 (*Dinv)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem);
+  double2 (*Ta)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem + NB * (NB + 1));
+  double2 (*Tb)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem + 2 * NB * (NB + 1));
+  const int tid = threadIdx.x;
+  const int nblk = (n + NB - 1) / NB;
+  for (int I = 0; I < nblk; ++I) {
+    const int i0 = I * NB, ib = min(NB, n - i0);
+    __syncthreads();
+    // load L_II into Ta (lower) and invert into Dinv by column forward substitution
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+      const int r = e % NB, c = e / NB;
+      Ta[r][c] = (r < ib && c < ib && r >= c) ? Lb[(i0 + r) + (long long)(i0 + c) * Nmax] : make_double2(0, 0);
+    }
+    __syncthreads();
+    if (tid < NB) {
+      const int c = tid;  // column c of the inverse
+      for (int r = 0; r < NB; ++r) {
+        double2 acc = make_double2(r == c ? 1.0 : 0.0, 0.0);
+        if (r < ib && c < ib && r >= c) {
+          for (int m = c; m < r; ++m) {
+            // acc -= L[r][m] * X[m]
+            const double2 l = Ta[r][m], x = Dinv[m][c];
+            acc.x -= l.x * x.x - l.y * x.y;
+            acc.y -= l.x * x.y + l.y * x.x;
+          }
+          const double2 d = Ta[r][r];
+          // divide by complex diagonal (real for a Cholesky factor)
+          const double den = d.x * d.x + d.y * d.y;
+          Dinv[r][c] = make_double2((acc.x * d.x + acc.y * d.y) / den, (acc.y * d.x - acc.x * d.y) / den);
+        } else {
+          Dinv[r][c] = make_double2(0, 0);
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+      const int r = e % NB, c = e / NB;
+      if (r < ib && c < ib) {
+        const double2 v = (r >= c) ? Dinv[r][c] : make_double2(0, 0);
+        Wb[(i0 + r) + (long long)(i0 + c) * Nmax] = v;
+        store_conv<C>(Ob + (i0 + r) + (long long)(i0 + c) * Nmax, v);
+      }
+    }
+    // off-diagonal blocks J < I
+    for (int J = 0; J < I; ++J) {
+      const int j0 = J * NB;
+      const int tr = tid % 16, tc = tid / 16;  // 16x16 threads, 2x2 outputs each
+      double2 acc[2][2] = {{make_double2(0, 0), make_double2(0, 0)}, {make_double2(0, 0), make_double2(0, 0)}};
+      for (int K = J; K < I; ++K) {
+        const int k0 = K * NB;
+        __syncthreads();
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+          const int r = e % NB, c = e / NB;
+          Ta[r][c] = (r < ib) ? Lb[(i0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+          Tb[r][c] = Wb[(k0 + r) + (long long)(j0 + c) * Nmax];
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int m = 0; m < NB; ++m) {
+#pragma unroll
+          for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) cfma(acc[a][c], Ta[tr + 16 * a][m], Tb[m][tc + 16 * c]);
+        }
+      }
+      __syncthreads();
+      // Tb <- acc
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) Tb[tr + 16 * a][tc + 16 * c] = acc[a][c];
+      __syncthreads();
+      // out = -Dinv * Tb
+      double2 o[2][2] = {{make_double2(0, 0), make_double2(0, 0)}, {make_double2(0, 0), make_double2(0, 0)}};
+      for (int m = 0; m < NB; ++m) {
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) cfma(o[a][c], Dinv[tr + 16 * a][m], Tb[m][tc + 16 * c]);
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int r = tr + 16 * a, cc = tc + 16 * c;
+          if (r < ib && j0 + cc < n) {
+            const double2 v = make_double2(-o[a][c].x, -o[a][c].y);
+            Wb[(i0 + r) + (long long)(j0 + cc) * Nmax] = v;
+            store_conv<C>(Ob + (i0 + r) + (long long)(j0 + cc) * Nmax, v);
+          }
+        }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// batched complex GEMM with triangular skipping, per-matrix sizes and k-ranges
+// ------------------------------------------------------------------------------------
+template <typename C>
+struct GemmArgs {
+  const C* A; long long strideA; int lda; int opA;   // opA 0: A[i,k]; 1: conj(A[k,i])
+  const C* B; long long strideB; int ldb; int opB;   // opB 0: B[k,j]; 1: conj(B[j,k])
+  C* Cm; long long strideC; int ldc;
+  const int* n;           // per-matrix size
+  int triA;               // 0 none; 1 opA(i,k)=0 for k>i; 2 opA(i,k)=0 for k<i
+  int triB;               // 0 none; 1 opB(k,j)=0 for k>j; 2 opB(k,j)=0 for k<j
+  int outMode;            // 0 full; 1 lower tiles + conj mirror; 2 lower tiles only (i>=j)
+  const void* kscale; long long strideK;   // optional real per-k scale on opA columns
+  const int* kbeg; const int* kend;        // optional per-(matrix,level) k range
+  int levels;             // grid.z = batch * levels (levels >= 1)
+  long long strideCLevel; // output stride per level
+};
+
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 8, kGemmThreads = 256;
+
+template <typename C, typename R>
+__global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
+  const int z = blockIdx.z;
+  const int b = z / g.levels, lvl = z % g.levels;
+  const int n = g.n[b];
+  const int i0 = blockIdx.y * kGemmBM, j0 = blockIdx.x * kGemmBN;
+  if (i0 >= n || j0 >= n) return;
+  if (g.outMode != 0 && j0 > i0 + kGemmBM - 1) return;
+  int kb = 0, ke = n;
+  if (g.kbeg) {
+    kb = g.kbeg[z];
+    ke = g.kend[z];
+  }
+  // triangular limits
+  if (g.triA == 1) ke = min(ke, i0 + kGemmBM);
+  if (g.triA == 2) kb = max(kb, i0);
+  if (g.triB == 1) kb = max(kb, j0);
+  if (g.triB == 2) ke = min(ke, j0 + kGemmBN);
+  const C* A = g.A + b * g.strideA;
+  const C* B = g.B + b * g.strideB;
+  C* Cm = g.Cm + b * g.strideC + lvl * g.strideCLevel;
+  const R* ks = g.kscale ? reinterpret_cast<const R*>(g.kscale) + b * g.strideK : nullptr;
+
+  __shared__ C As[kGemmBK][kGemmBM + 1];
+  __shared__ C Bs[kGemmBK][kGemmBN + 1];
+  const int tid = threadIdx.x;
+  const int tr = tid % 16, tc = tid / 16;
+  C acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[a][c] = mk(R(0), R(0));
+
+  for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
+    // load A tile: opA(i0+r, k0+kk), r<64, kk<8 -> 512 elements, 2 per thread
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int e = tid + t * kGemmThreads;
+      int r, kk;
+      if (g.opA == 0) { r = e % kGemmBM; kk = e / kGemmBM; } else { kk = e % kGemmBK; r = e / kGemmBK; }
+      const int i = i0 + r, k = k0 + kk;
+      C v = mk(R(0), R(0));
+      if (i < n && k < ke) {
+        v = (g.opA == 0) ? A[i + (long long)k * g.lda] : cconj(A[k + (long long)i * g.lda]);
+        if (ks) v = cscale(v, ks[k]);
+      }
+      As[kk][r] = v;
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int e = tid + t * kGemmThreads;
+      int cidx, kk;
+      if (g.opB == 0) { kk = e % kGemmBK; cidx = e / kGemmBK; } else { cidx = e % kGemmBN; kk = e / kGemmBN; }
+      const int j = j0 + cidx, k = k0 + kk;
+      C v = mk(R(0), R(0));
+      if (j < n && k < ke) v = (g.opB == 0) ? B[k + (long long)j * g.ldb] : cconj(B[j + (long long)k * g.ldb]);
+      Bs[kk][cidx] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGemmBK; ++kk) {
+      C av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = As[kk][tr + 16 * a];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) bv[c] = Bs[kk][tc + 16 * c];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cfma(acc[a][c], av[a], bv[c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = i0 + tr + 16 * a, j = j0 + tc + 16 * c;
+      if (i >= n || j >= n) continue;
+      C v = acc[a][c];
+      if (g.outMode == 0) {
+        Cm[i + (long long)j * g.ldc] = v;
+      } else if (i >= j) {
+        if (i == j && g.outMode == 1) v.y = R(0);
+        Cm[i + (long long)j * g.ldc] = v;
+        if (g.outMode == 1 && i != j) Cm[j + (long long)i * g.ldc] = cconj(v);
+      }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Householder tridiagonalisation (lower), fused rank-2 update + next mat-vec
+// ------------------------------------------------------------------------------------
+// Follows the reflector conventions of LAPACK ?hetd2/?larfg: H_i = I - tau v v^H with
+// v(0) = 1, H_i^H (alpha; x) = (beta; 0), beta real; A = Q T Q^H, Q = H_0 H_1 ... .
+// v(1:) is stored below the subdiagonal of column i of A, tau in tauOut, T in (d, e).
+constexpr int kTrdThreads = 1024;
+
+template <typename C, typename R>
+__device__ __forceinline__ void householder(C* __restrict__ col, int m, C* __restrict__ v, R* red,
+                                            C& tauOut, R& betaOut) {
+  // col[0..m): alpha = col[0], x = col[1..m). Produces v[0..m) in smem (v[0] = 1).
+  R part = 0;
+  for (int r = 1 + threadIdx.x; r < m; r += blockDim.x) part += cabs2(col[r]);
+  const R xnorm2 = block_sum(part, red);
+  const C alpha = col[0];
+  C tau;
+  R beta;
+  if (xnorm2 == R(0) && alpha.y == R(0)) {
+    tau = mk(R(0), R(0));
+    beta = alpha.x;
+    for (int r = threadIdx.x; r < m; r += blockDim.x) v[r] = mk(r == 0 ? R(1) : R(0), R(0));
+  } else {
+    const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+    beta = (alpha.x >= R(0)) ? -nrm : nrm;
+    tau = mk((beta - alpha.x) / beta, -alpha.y / beta);
+    // scale = 1 / (alpha - beta)
+    const C am = mk(alpha.x - beta, alpha.y);
+    const R den = am.x * am.x + am.y * am.y;
+    const C sc = mk(am.x / den, -am.y / den);
+    for (int r = threadIdx.x; r < m; r += blockDim.x) v[r] = (r == 0) ? mk(R(1), R(0)) : cmul(col[r], sc);
+  }
+  tauOut = tau;
+  betaOut = beta;
+}
+
+template <typename C, typename R>
+__global__ void __launch_bounds__(kTrdThreads)
+hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
+             double* __restrict__ eOut, C* __restrict__ tauOut) {
+  const int b = blockIdx.x;
+  const int n = nred[b];
+  C* Ab = A + (long long)b * Nmax * Nmax;
+  double* d = dOut + (long long)b * Nmax;
+  double* e = eOut + (long long)b * Nmax;
+  C* taus = tauOut + (long long)b * Nmax;
+  extern __shared__ unsigned char smem_raw[];
+  C* v = reinterpret_cast<C*>(smem_raw);        // [Nmax] current reflector (relative to row i+1)
+  C* w = v + Nmax;                              // [Nmax] w vector
+  C* p = w + Nmax;                              // [Nmax] accumulated tau*A*v for the next step
+  C* vn = p + Nmax;                             // [Nmax] next reflector
+  C* ppart = vn + Nmax;                         // [8][Nmax] partial mat-vec sums
+  __shared__ R red[32];
+  __shared__ C s_tau, s_taun;
+  __shared__ R s_beta;
+  const int tid = threadIdx.x;
+  if (n <= 0) return;
+  if (n == 1) {
+    if (tid == 0) { d[0] = (double)Ab[0].x; }
+    return;
+  }
+
+  // ---- step 0 set-up: reflector of column 0, p = tau A22 v (plain mat-vec) ----
+  {
+    C t; R be;
+    householder<C, R>(Ab + 1, n - 1, v, red, t, be);
+    if (tid == 0) { s_tau = t; s_beta = be; }
+    __syncthreads();
+    const int m = n - 1;
+    // p[r] = tau * sum_c A22[r,c] v[c]; rows split over threads, columns over groups
+    const int groups = kTrdThreads / 128;  // 8 groups of 128 threads
+    const int g = tid / 128, lt = tid % 128;
+    for (int r = lt; r < m; r += 128) {
+      C acc = mk(R(0), R(0));
+      for (int c = g; c < m; c += groups) cfma(acc, Ab[(1 + r) + (long long)(1 + c) * Nmax], v[c]);
+      ppart[g * Nmax + r] = acc;
+    }
+    __syncthreads();
+    for (int r = tid; r < m; r += blockDim.x) {
+      C acc = mk(R(0), R(0));
+      for (int gg = 0; gg < groups; ++gg) acc = acc + ppart[gg * Nmax + r];
+      p[r] = cmul(s_tau, acc);
+    }
+    __syncthreads();
+  }
+
+  for (int i = 0; i < n - 1; ++i) {
+    const int m = n - i - 1;            // size of A22 = A[i+1:, i+1:]
+    const C tau = s_tau;
+    const R beta = s_beta;
+    // store reflector below the subdiagonal, e, tau, d
+    for (int r = 1 + tid; r < m; r += blockDim.x) Ab[(i + 1 + r) + (long long)i * Nmax] = v[r];
+    if (tid == 0) {
+      e[i] = (double)beta;
+      taus[i] = tau;
+      d[i] = (double)Ab[i + (long long)i * Nmax].x;
+      Ab[(i + 1) + (long long)i * Nmax] = mk(beta, R(0));
+    }
+    // w = p - 1/2 tau (p^H v) v
+    R pr = 0, pi = 0;
+    for (int r = tid; r < m; r += blockDim.x) {
+      const C pv = cconjmul(p[r], v[r]);
+      pr += pv.x;
+      pi += pv.y;
+    }
+    pr = block_sum(pr, red);
+    pi = block_sum(pi, red);
+    const C pHv = mk(pr, pi);
+    const C alph = cscale(cmul(tau, pHv), R(-0.5));
+    for (int r = tid; r < m; r += blockDim.x) w[r] = p[r] + cmul(alph, v[r]);
+    __syncthreads();
+    if (m == 1) {
+      // last 1x1 trailing block
+      if (tid == 0) {
+        C a = Ab[(i + 1) + (long long)(i + 1) * Nmax];
+        // a -= v0 conj(w0) + w0 conj(v0)
+        a = a - cmulc(v[0], w[0]) - cmulc(w[0], v[0]);
+        Ab[(i + 1) + (long long)(i + 1) * Nmax] = a;
+        d[i + 1] = (double)a.x;
+      }
+      break;
+    }
+    // update first column of A22 (column i+1, rows i+1..n-1)
+    C* col = Ab + (i + 1) + (long long)(i + 1) * Nmax;
+    for (int r = tid; r < m; r += blockDim.x) {
+      C a = col[r];
+      a = a - cmulc(v[r], w[0]) - cmulc(w[r], v[0]);
+      col[r] = a;
+    }
+    __syncthreads();
+    // next reflector from col[1..m)
+    {
+      C t; R be;
+      householder<C, R>(col + 1, m - 1, vn, red, t, be);
+      if (tid == 0) { s_taun = t; s_beta = be; }
+    }
+    __syncthreads();
+    // fused pass over A33 = A[i+2:, i+2:] (size m-1): rank-2 update with (v[1:], w[1:]),
+    // accumulate pn = A33_new * vn
+    const int mm = m - 1;
+    const int groups = kTrdThreads / 128;
+    const int g = tid / 128, lt = tid % 128;
+    for (int r = lt; r < mm; r += 128) {
+      const C vr = v[1 + r], wr = w[1 + r];
+      C acc = mk(R(0), R(0));
+      C* rowp = Ab + (i + 2 + r) + (long long)(i + 2) * Nmax;
+      for (int c = g; c < mm; c += groups) {
+        C a = rowp[(long long)c * Nmax];
+        a = a - cmulc(vr, w[1 + c]) - cmulc(wr, v[1 + c]);
+        rowp[(long long)c * Nmax] = a;
+        cfma(acc, a, vn[c]);
+      }
+      ppart[g * Nmax + r] = acc;
+    }
+    __syncthreads();
+    const C taun = s_taun;
+    for (int r = tid; r < mm; r += blockDim.x) {
+      C acc = mk(R(0), R(0));
+      for (int gg = 0; gg < groups; ++gg) acc = acc + ppart[gg * Nmax + r];
+      p[r] = cmul(taun, acc);
+      v[r] = vn[r];
+    }
+    if (tid == 0) s_tau = taun;
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// symmetric tridiagonal eigenproblem in FP64: bisection + twisted factorisation
+// ------------------------------------------------------------------------------------
+constexpr int kTriThreads = 256;
+
+__device__ __forceinline__ int sturm_count(const double* __restrict__ d, const double* __restrict__ e2,
+                                           int n, double lam, double pivmin) {
+  int cnt = 0;
+  double q = d[0] - lam;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += (q < 0.0);
+  for (int k = 1; k < n; ++k) {
+    q = (d[k] - lam) - e2[k - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += (q < 0.0);
+  }
+  return cnt;
+}
+
+// work: [2][n][Nmax] FP64 per matrix (Lp and Um of every eigenvalue, interleaved by
+// eigenvalue index so that lanes access consecutive addresses). Z: real eigenvectors,
+// row-major Z[k*Nmax + i] = z_i[k], working precision R.
+template <typename R>
+__global__ void __launch_bounds__(kTriThreads)
+tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, const int* __restrict__ nred,
+               int Nmax, double* __restrict__ lamOut, R* __restrict__ Z, double* __restrict__ work,
+               int* __restrict__ status) {
+  const int b = blockIdx.x;
+  const int n = nred[b];
+  if (n <= 0) return;
+  extern __shared__ double smem_d[];
+  double* d = smem_d;            // [Nmax]
+  double* e = d + Nmax;          // [Nmax]
+  double* e2 = e + Nmax;         // [Nmax]
+  double* lam = e2 + Nmax;       // [Nmax]
+  __shared__ double red[32];
+  const double* db = dIn + (long long)b * Nmax;
+  const double* eb = eIn + (long long)b * Nmax;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    d[k] = db[k];
+    const double ek = (k < n - 1) ? eb[k] : 0.0;
+    e[k] = ek;
+    e2[k] = ek * ek;
+  }
+  __syncthreads();
+  // Gershgorin interval and pivmin
+  double lo = 1e300, hi = -1e300, emax = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double r = fabs(e[k]) + (k > 0 ? fabs(e[k - 1]) : 0.0);
+    lo = fmin(lo, d[k] - r);
+    hi = fmax(hi, d[k] + r);
+    emax = fmax(emax, e2[k]);
+  }
+  lo = block_min(lo, red, 1e300);
+  __syncthreads();
+  hi = block_max(hi, red, -1e300);
+  __syncthreads();
+  emax = block_max(emax, red, 0.0);
+  const double eps = 2.220446049250313e-16;
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  const double pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
+  lo -= 2.0 * eps * tnorm + 4.0 * pivmin;
+  hi += 2.0 * eps * tnorm + 4.0 * pivmin;
+  // bisection for each eigenvalue index
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double a = lo, c = hi;
+    for (int it = 0; it < 128; ++it) {
+      const double mid = 0.5 * (a + c);
+      if (mid <= a || mid >= c) break;
+      if (c - a <= fmax(2.0 * eps * fmax(fabs(a), fabs(c)), eps * tnorm) + pivmin) break;
+      if (sturm_count(d, e2, n, mid, pivmin) > i) c = mid; else a = mid;
+    }
+    lam[i] = 0.5 * (a + c);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) lamOut[(long long)b * Nmax + i] = lam[i];
+
+  // twisted factorisation eigenvectors
+  double* Lp = work + (long long)b * 2 * Nmax * Nmax;
+  double* Um = Lp + (long long)Nmax * Nmax;
+  R* Zb = Z + (long long)b * Nmax * Nmax;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double l = lam[i];
+    // top-down stationary factorisation T - l = L+ D+ L+^T
+    double dp = d[0] - l;
+    for (int k = 0; k < n - 1; ++k) {
+      if (fabs(dp) < pivmin) dp = -pivmin;
+      const double lk = e[k] / dp;
+      Lp[(long long)k * Nmax + i] = lk;
+      dp = (d[k + 1] - l) - lk * e[k];
+    }
+    // bottom-up progressive factorisation, twist index r = argmin |gamma|
+    // gamma_k = D+_k + D-_k - (d_k - l); D+_k is recomputed from Lp on the way.
+    double dm = d[n - 1] - l;
+    // D+_{n-1}: recompute forward value for k = n-1
+    // we store D+ implicitly: D+_{k+1} = (d_{k+1} - l) - Lp_k e_k
+    double best = 1e300;
+    int r = n - 1;
+    {
+      const double dpl = (n > 1) ? ((d[n - 1] - l) - Lp[(long long)(n - 2) * Nmax + i] * e[n - 2]) : (d[0] - l);
+      const double gam = dpl + dm - (d[n - 1] - l);
+      best = fabs(gam);
+      r = n - 1;
+    }
+    for (int k = n - 2; k >= 0; --k) {
+      if (fabs(dm) < pivmin) dm = -pivmin;
+      const double uk = e[k] / dm;
+      Um[(long long)k * Nmax + i] = uk;
+      dm = (d[k] - l) - uk * e[k];
+      const double dpk = (k > 0) ? ((d[k] - l) - Lp[(long long)(k - 1) * Nmax + i] * e[k - 1]) : (d[0] - l);
+      const double gam = dpk + dm - (d[k] - l);
+      if (fabs(gam) < best) {
+        best = fabs(gam);
+        r = k;
+      }
+    }
+    // z_r = 1; z_k = -Lp_k z_{k+1} (k < r); z_{k+1} = -Um_k z_k (k >= r). Every lane
+    // walks the same k (predicated on its own twist index) so accesses stay coalesced.
+    // The FP64 values overwrite Lp/Um; the norm is accumulated in FP64.
+    double nrm2 = 1.0;
+    {
+      double z1 = 1.0, z2 = 0.0;  // z_{k+1}, z_{k+2}
+      for (int k = n - 2; k >= 0; --k) {
+        if (k < r) {
+          double zk;
+          if (z1 != 0.0) zk = -Lp[(long long)k * Nmax + i] * z1;
+          else zk = (e[k] != 0.0) ? -(e[k + 1] / e[k]) * z2 : 0.0;
+          nrm2 += zk * zk;
+          Lp[(long long)k * Nmax + i] = zk;
+          z2 = z1;
+          z1 = zk;
+        }
+      }
+    }
+    {
+      double z1 = 1.0, z2 = 0.0;  // z_k, z_{k-1}
+      for (int k = 0; k < n - 1; ++k) {
+        if (k >= r) {
+          double zn;
+          if (z1 != 0.0) zn = -Um[(long long)k * Nmax + i] * z1;
+          else zn = (e[k] != 0.0) ? -((k > 0 ? e[k - 1] : 0.0) / e[k]) * z2 : 0.0;
+          nrm2 += zn * zn;
+          Um[(long long)k * Nmax + i] = zn;  // z_{k+1}
+          z2 = z1;
+          z1 = zn;
+        }
+      }
+    }
+    const double inv = 1.0 / sqrt(nrm2);
+    for (int k = 0; k < n; ++k) {
+      double zk;
+      if (k < r) zk = Lp[(long long)k * Nmax + i];
+      else if (k == r) zk = 1.0;
+      else zk = Um[(long long)(k - 1) * Nmax + i];
+      Zb[(long long)k * Nmax + i] = (R)(zk * inv);
+    }
+  }
+  __syncthreads();
+  // re-orthogonalise tight clusters (relative gap below 1e-10 of |T|): modified
+  // Gram-Schmidt inside each cluster, in eigenvalue order.
+  const double ctol = 1e-10 * fmax(tnorm, 1e-300);
+  __shared__ int s_any;
+  if (threadIdx.x == 0) {
+    int any = 0;
+    for (int i = 1; i < n; ++i) any |= (lam[i] - lam[i - 1] < ctol);
+    s_any = any;
+  }
+  __syncthreads();
+  if (!s_any) return;
+  if (threadIdx.x == 0) atomicOr(status + b, (int)kStatusClusterFix);
+  for (int i = 1; i < n; ++i) {
+    if (!(lam[i] - lam[i - 1] < ctol)) continue;
+    int j0 = i - 1;
+    while (j0 > 0 && lam[j0] - lam[j0 - 1] < ctol) --j0;
+    for (int j = j0; j < i; ++j) {
+      double part = 0.0;
+      for (int k = threadIdx.x; k < n; k += blockDim.x)
+        part += (double)Zb[(long long)k * Nmax + i] * (double)Zb[(long long)k * Nmax + j];
+      const double dot = block_sum(part, red);
+      for (int k = threadIdx.x; k < n; k += blockDim.x)
+        Zb[(long long)k * Nmax + i] = (R)((double)Zb[(long long)k * Nmax + i] - dot * (double)Zb[(long long)k * Nmax + j]);
+      __syncthreads();
+    }
+    double part = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const double zv = (double)Zb[(long long)k * Nmax + i];
+      part += zv * zv;
+    }
+    const double nr = sqrt(block_sum(part, red));
+    const double inv = nr > 0 ? 1.0 / nr : 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+      Zb[(long long)k * Nmax + i] = (R)((double)Zb[(long long)k * Nmax + i] * inv);
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// back-transform Y = Q Z, Q = H_0 ... H_{n-2}; one CTA per (column chunk, matrix)
+// ------------------------------------------------------------------------------------
+constexpr int kBtThreads = 256;
+
+template <typename C, typename R, int kBtCols>
+__global__ void __launch_bounds__(kBtThreads)
+backtransform_kernel(const C* __restrict__ A, const C* __restrict__ taus, const R* __restrict__ Z,
+                     const int* __restrict__ nred, int Nmax, C* __restrict__ Y) {
+  const int b = blockIdx.y;
+  const int n = nred[b];
+  const int c0 = blockIdx.x * kBtCols;
+  if (c0 >= n) return;
+  const int nc = min(kBtCols, n - c0);
+  extern __shared__ unsigned char smem_raw[];
+  C* ys = reinterpret_cast<C*>(smem_raw);   // [Nmax][kBtCols]
+  C* vs = ys + (long long)Nmax * kBtCols;   // [Nmax]
+  C* part = vs + Nmax;                      // [kBtThreads/kBtCols][kBtCols]
+  const C* Ab = A + (long long)b * Nmax * Nmax;
+  const R* Zb = Z + (long long)b * Nmax * Nmax;
+  const C* tb = taus + (long long)b * Nmax;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < n * kBtCols; e += blockDim.x) {
+    const int k = e / kBtCols, c = e % kBtCols;
+    ys[e] = mk((c < nc) ? Zb[(long long)k * Nmax + c0 + c] : R(0), R(0));
+  }
+  __syncthreads();
+  const int col = tid % kBtCols, rg = tid / kBtCols, nrg = kBtThreads / kBtCols;
+  for (int i = n - 2; i >= 0; --i) {
+    const int m = n - i - 1;  // reflector acts on rows i+1 .. n-1
+    const C tau = tb[i];
+    if (tau.x == R(0) && tau.y == R(0)) continue;
+    for (int r = tid; r < m; r += blockDim.x)
+      vs[r] = (r == 0) ? mk(R(1), R(0)) : Ab[(i + 1 + r) + (long long)i * Nmax];
+    __syncthreads();
+    // dot_c = v^H y_c
+    C acc = mk(R(0), R(0));
+    for (int r = rg; r < m; r += nrg) cfma_cj(acc, vs[r], ys[(i + 1 + r) * kBtCols + col]);
+    part[rg * kBtCols + col] = acc;
+    __syncthreads();
+    if (tid < kBtCols) {
+      C s = mk(R(0), R(0));
+      for (int g = 0; g < nrg; ++g) s = s + part[g * kBtCols + tid];
+      part[tid] = cmul(tau, s);  // tau * v^H y
+    }
+    __syncthreads();
+    const C f = part[col];
+    for (int r = rg; r < m; r += nrg) {
+      C y = ys[(i + 1 + r) * kBtCols + col];
+      y = y - cmul(vs[r], f);
+      ys[(i + 1 + r) * kBtCols + col] = y;
+    }
+    __syncthreads();
+  }
+  C* Yb = Y + (long long)b * Nmax * Nmax;
+  for (int e = tid; e < n * nc; e += blockDim.x) {
+    const int k = e % n, c = e / n;
+    Yb[k + (long long)(c0 + c) * Nmax] = ys[k * kBtCols + c];
+  }
+}
+
+}  // namespace bippb200

@@ -1,0 +1,82 @@
+// NUFFT engine shared by the collect/get plan and the batched pipeline.
+#pragma once
+
+#include <cufft.h>
+
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+#include "context.hpp"
+#include "nufft_kernels.cuh"
+
+namespace bippb200 {
+
+// Pixel lattice fitted to the pixel coordinates (l, m): l = l0 + a Al + b Bl,
+// m = m0 + a Am + b Bm, pixel index p = a Nb + b.
+struct Lattice {
+  bool ok = false;
+  int Na = 0, Nb = 0;
+  double l0 = 0, m0 = 0, Al = 0, Bl = 0, Am = 0, Bm = 0;
+  double maxResidL = 0, maxResidM = 0;  // max |l - lattice|, |m - lattice|
+};
+
+Lattice fit_lattice(const std::vector<double>& l, const std::vector<double>& m);
+
+// ES kernel width and shape for a tolerance at upsampling factor 2 (as used by type-1/3
+// NUFFTs with the "exponential of semicircle" kernel).
+void es_params(double eps, int& W, float& beta);
+
+class NufftCore {
+public:
+  // Pixel side: lattice + per-pixel n (FP64). nch = channels per transform.
+  void setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<double>& n, double eps, int nch,
+             const std::vector<double>* dl = nullptr, const std::vector<double>* dm = nullptr, double su = 1.0,
+             double sv = 1.0, int levels = 0);
+
+  // Per transform: w-range of the points (already scaled to phase units).
+  void begin(double wmin, double wmax);
+  // Per transform (after begin): enable the first-order lattice-residual channels and
+  // the u/v normalisation of their values.
+  void set_corr(bool on, double su, double sv);
+  int* counts() { return counts_.get<int>(); }
+  // After the count kernels: scan -> offsets & cursor; allocate records for nPoints
+  void end_count(long long nPoints);
+  int* cursor() { return cursor_.get<int>(); }
+  PtRec* records() { return rec_.get<PtRec>(); }
+  float2* values() { return vals_.get<float2>(); }
+  long long value_stride() const { return valStride_; }
+  // spread/FFT/w-sum over all slabs and accumulate Re(...) into image[ch][P] (ld P)
+  void execute(float* image, long long ldImage, double* stageMs = nullptr);
+
+  const NufftGeom& geom() const { return g_; }
+  long long num_pixels() const { return (long long)g_.Na * g_.Nb; }
+  int channels() const { return nch_; }
+  bool sincos64() const { return eps_ < 1e-6; }
+  double su() const { return su_; }
+  double sv() const { return sv_; }
+  bool corr_terms() const { return corrTerms_; }
+
+private:
+  bipp_ctx_s* ctx_ = nullptr;
+  NufftGeom g_{};
+  int nch_ = 1, levels_ = 1;
+  double eps_ = 1e-5;
+  double Sn_ = 0;
+  bool corrTerms_ = false, corrCapable_ = false;
+  double su_ = 1, sv_ = 1;
+  long long nkeys_ = 0, valStride_ = 0;
+  DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
+  DevBuf qz_, qw_;
+  std::map<int, cufftHandle> plans_;
+  int slabTiles_ = 1;
+  cufftHandle plan_for(int batch);
+
+public:
+  ~NufftCore();
+};
+
+// Gauss-Legendre nodes/weights on [-1, 1]
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
+
+}  // namespace bippb200

@@ -1,0 +1,605 @@
+// Type-3 NUFFT kernels for image synthesis on a pixel lattice (sm_100a).
+//
+// Target sum (the reference's exact definition, src/host/kernels/nuft_sum.cpp:9-31 with
+// alpha = 1 after the 2 pi/wl uvw scaling of src/nufft_synthesis.cpp:151-155):
+//     I_l(p) += Re sum_k c_lk exp(i (u_k l_p + v_k m_p + w_k n_p))
+// Pixels lie on a lattice l = l0 + a A_l + b B_l, m = m0 + a A_m + b B_m (a slow, b
+// fast), so the (l, m) part is a periodic type-1 transform in the folded phases
+// x_k = u B_l + v B_m, y_k = u A_l + v A_m, and n enters as a 1-D type-3 axis:
+//   spread (ES kernel) onto a grid [level][w-plane][y][x] -> 2-D FFT per plane ->
+//   per-pixel sum over w-planes with exp(i n~_p t_j) -> deconvolve, Re, accumulate.
+// Points are bucket-sorted by tile so each CTA accumulates one output tile in shared
+// memory and writes it once (no global atomics on the grid).
+#pragma once
+
+#include "common.cuh"
+
+namespace bippb200 {
+
+constexpr int kTX = 16, kTY = 16, kTW = 8;       // output tile (cells)
+constexpr int kMaxW = 16;                         // max kernel width
+constexpr int kMaxChan = 12;                      // max channels (levels x correction terms)
+
+struct NufftGeom {
+  // lattice
+  double l0, m0, Al, Bl, Am, Bm;   // pixel (a,b): l = l0 + a Al + b Bl, m = m0 + a Am + b Bm
+  int Na, Nb;                       // lattice extents (a slow)
+  double nc;                        // centre of n
+  double wc;                        // centre of w
+  // fine grid
+  int nx, ny, nw;                   // grid sizes (nx, ny periodic; nw linear)
+  int jc;                           // w-grid index of t = 0
+  double hx, hy, hw;                // grid spacings (x,y in radians per cell; w in w-units)
+  int W;                            // kernel width (cells)
+  float beta;                       // ES kernel shape
+  int ntx, nty, ntw;                // tile counts
+};
+
+// ES kernel exp(beta (sqrt(1 - z^2) - 1)), |z| < 1
+__device__ __forceinline__ float es_kernel(float z, float beta) {
+  const float t = 1.0f - z * z;
+  return t > 0.0f ? __expf(beta * (sqrtf(t) - 1.0f)) : 0.0f;
+}
+
+__device__ __forceinline__ double wrap_pi(double x) {
+  // to [-pi, pi)
+  const double twopi = 6.283185307179586476925286766559;
+  return x - twopi * floor(x / twopi + 0.5);
+}
+
+// grid coordinates of one point: first support cell and offset (gx - ix0) in FP32
+struct PtCoord {
+  int ix0, iy0, iw0;
+  float dx, dy, dw;
+};
+
+// not inlined: the count and scatter passes must compute bit-identical keys
+__device__ __noinline__ PtCoord point_coord(const NufftGeom& g, double u, double v, double w) {
+  const double x = u * g.Bl + v * g.Bm;
+  const double y = u * g.Al + v * g.Am;
+  const double gx = wrap_pi(x) / g.hx;
+  const double gy = wrap_pi(y) / g.hy;
+  const double gw = (w - g.wc) / g.hw + g.jc;
+  const double half = 0.5 * g.W;
+  PtCoord c;
+  c.ix0 = (int)ceil(gx - half);
+  c.iy0 = (int)ceil(gy - half);
+  c.iw0 = (int)ceil(gw - half);
+  c.dx = (float)(gx - c.ix0);
+  c.dy = (float)(gy - c.iy0);
+  c.dw = (float)(gw - c.iw0);
+  c.iw0 = min(max(c.iw0, 0), g.nw - g.W);
+  return c;
+}
+
+// phase of a point at the lattice origin, reduced to [-pi, pi) in FP64
+__device__ __forceinline__ double point_phase(const NufftGeom& g, double u, double v, double w) {
+  const double x = u * g.Bl + v * g.Bm;
+  const double y = u * g.Al + v * g.Am;
+  // exp(i (u l0 + v m0 + x Nb/2 + y Na/2 + w nc)): the Nb/2, Na/2 shifts centre the modes
+  double ph = u * g.l0 + v * g.m0 + w * g.nc;
+  ph = wrap_pi(ph) + wrap_pi(x * (double)(g.Nb / 2)) + wrap_pi(y * (double)(g.Na / 2));
+  return wrap_pi(ph);
+}
+
+__device__ __noinline__ int tile_key(const NufftGeom& g, const PtCoord& c) {
+  int ix = c.ix0 % g.nx; if (ix < 0) ix += g.nx;
+  int iy = c.iy0 % g.ny; if (iy < 0) iy += g.ny;
+  const int tx = ix / kTX, ty = iy / kTY, tw = c.iw0 / kTW;
+  // crossing bits: support [i0, i0+W-1] crosses into the next tile
+  const int bx = ((ix % kTX) + g.W - 1) >= kTX;
+  const int by = ((iy % kTY) + g.W - 1) >= kTY;
+  const int bw = ((c.iw0 % kTW) + g.W - 1) >= kTW;
+  const int tile = (tw * g.nty + ty) * g.ntx + tx;
+  return tile * 8 + (bx | (by << 1) | (bw << 2));
+}
+
+// sorted point record
+struct __align__(16) PtRec {
+  int ix0, iy0, iw0;
+  float dx, dy, dw;
+  int pad0, pad1;
+};
+
+// ---------------------------------------------------------------------------------------
+// point sources: either pipeline form (antenna coordinates + VV lower triangle) or
+// collect/get form (per-baseline float uvw + values)
+// ---------------------------------------------------------------------------------------
+struct PipelinePoints {
+  // step s of the batch, pair (r >= s') of kept antennas
+  int nSteps;
+  const int* nred;            // [steps]
+  const int* idx;             // [steps][Nmax]
+  const double* antUVW;       // [steps][nAnt][3] antenna UVW coordinates (m)
+  const double* uvwScale;     // [steps] 2 pi / wl
+  const long long* pairOffset;// [steps+1] prefix of n(n+1)/2
+  int Nmax, nAnt;
+  const float2* vv;           // [steps][levels][Nmax*Nmax] lower triangle, column-major
+  long long vvStepStride, vvLevelStride;
+  int levels;
+  int stepBase;               // first step of this chunk within the batch (for pairOffset)
+};
+
+struct BaselinePoints {
+  long long n;                // number of points
+  const float* uvw;           // [3][ld] float, in metres (scaled by uvwScale)
+  long long lduvw;
+  double uvwScale;            // 2 pi / wl (or 1)
+  const float2* values;       // [channels][ldv]
+  long long ldv;
+  int levels;
+};
+
+__device__ __noinline__ void pair_from_linear(long long t, int n, int& r, int& s) {
+  // t enumerates the lower triangle column by column: column s holds rows s..n-1
+  // offset(s) = s n - s (s - 1) / 2
+  double nn = (double)n + 0.5;
+  int sc = (int)floor(nn - sqrt(nn * nn - 2.0 * (double)t));
+  if (sc < 0) sc = 0;
+  if (sc > n - 1) sc = n - 1;
+  long long off = (long long)sc * n - (long long)sc * (sc - 1) / 2;
+  while (off > t) { --sc; off = (long long)sc * n - (long long)sc * (sc - 1) / 2; }
+  while (true) {
+    long long nxt = (long long)(sc + 1) * n - (long long)(sc + 1) * sc / 2;
+    if (sc + 1 < n && nxt <= t) { ++sc; off = nxt; } else break;
+  }
+  s = sc;
+  r = sc + (int)(t - off);
+}
+
+// pass 1: keys of pipeline points -> counts
+static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ counts,
+                                      const long long* __restrict__ chunkPairOffset) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    // locate step by binary search in chunkPairOffset[0..nSteps]
+    int lo = 0, hi = P.nSteps;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (chunkPairOffset[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int st = lo;
+    const int n = P.nred[st];
+    int r, s;
+    pair_from_linear(t - chunkPairOffset[st], n, r, s);
+    const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
+    const double* U = P.antUVW + (long long)st * P.nAnt * 3;
+    const double sc = P.uvwScale[st];
+    const double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
+    const double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
+    const double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    const PtCoord c = point_coord(g, u, v, w);
+    atomicAdd(counts + tile_key(g, c), 1);
+  }
+}
+
+// pass 2: scatter records + values (channel-major: vals[ch][sortedIndex])
+static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
+                                        const long long* __restrict__ chunkPairOffset, PtRec* __restrict__ rec,
+                                        float2* __restrict__ vals, long long valStride, int sincos64) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = P.nSteps;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (chunkPairOffset[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int st = lo;
+    const int n = P.nred[st];
+    int r, s;
+    pair_from_linear(t - chunkPairOffset[st], n, r, s);
+    const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
+    const double* U = P.antUVW + (long long)st * P.nAnt * 3;
+    const double sc = P.uvwScale[st];
+    const double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
+    const double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
+    const double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    const PtCoord c = point_coord(g, u, v, w);
+    const int key = tile_key(g, c);
+    const int pos = atomicAdd(cursor + key, 1);
+    if (pos < 0 || pos >= valStride) continue;  // keys of both passes agree; never taken
+    PtRec pr;
+    pr.ix0 = c.ix0; pr.iy0 = c.iy0; pr.iw0 = c.iw0;
+    pr.dx = c.dx; pr.dy = c.dy; pr.dw = c.dw;
+    pr.pad0 = 0; pr.pad1 = 0;
+    rec[pos] = pr;
+    const double ph = point_phase(g, u, v, w);
+    float sn, cs;
+    if (sincos64) { double s64, c64; sincos(ph, &s64, &c64); sn = (float)s64; cs = (float)c64; }
+    else sincosf((float)ph, &sn, &cs);
+    const float wgt = (r == s) ? 1.0f : 2.0f;   // lower triangle stands for (r,s) and (s,r)
+    const float2* vvb = P.vv + (long long)st * P.vvStepStride + r + (long long)s * P.Nmax;
+    for (int l = 0; l < P.levels; ++l) {
+      const float2 a = vvb[(long long)l * P.vvLevelStride];
+      vals[(long long)l * valStride + pos] = make_float2(wgt * (a.x * cs - a.y * sn), wgt * (a.x * sn + a.y * cs));
+    }
+  }
+}
+
+// collect/get form: per-baseline uvw (float, metres) and values; optional first-order
+// lattice-residual channels (values * u/su, values * v/sv)
+static __global__ void baseline_count_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ counts) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
+    const double u = (double)P.uvw[t] * P.uvwScale;
+    const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
+    const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    atomicAdd(counts + tile_key(g, point_coord(g, u, v, w)), 1);
+  }
+}
+
+static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ cursor,
+                                        PtRec* __restrict__ rec, float2* __restrict__ vals, long long valStride,
+                                        int sincos64, int corrTerms, double su, double sv) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
+    const double u = (double)P.uvw[t] * P.uvwScale;
+    const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
+    const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    const PtCoord c = point_coord(g, u, v, w);
+    const int pos = atomicAdd(cursor + tile_key(g, c), 1);
+    if (pos < 0 || pos >= valStride) continue;  // keys of both passes agree; never taken
+    PtRec pr;
+    pr.ix0 = c.ix0; pr.iy0 = c.iy0; pr.iw0 = c.iw0;
+    pr.dx = c.dx; pr.dy = c.dy; pr.dw = c.dw;
+    pr.pad0 = 0; pr.pad1 = 0;
+    rec[pos] = pr;
+    const double ph = point_phase(g, u, v, w);
+    float sn, cs;
+    if (sincos64) { double s64, c64; sincos(ph, &s64, &c64); sn = (float)s64; cs = (float)c64; }
+    else sincosf((float)ph, &sn, &cs);
+    for (int l = 0; l < P.levels; ++l) {
+      const float2 a = P.values[(long long)l * P.ldv + t];
+      const float2 q = make_float2(a.x * cs - a.y * sn, a.x * sn + a.y * cs);
+      vals[(long long)l * valStride + pos] = q;
+      if (corrTerms) {
+        const float fu = (float)(u / su), fv = (float)(v / sv);
+        vals[(long long)(P.levels + l) * valStride + pos] = make_float2(q.x * fu, q.y * fu);
+        vals[(long long)(2 * P.levels + l) * valStride + pos] = make_float2(q.x * fv, q.y * fv);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// exclusive scan (3 phases) of int counts -> int offsets
+// ---------------------------------------------------------------------------------------
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;   // per thread
+
+static __global__ void scan_partial_kernel(const int* __restrict__ in, int* __restrict__ out, long long n,
+                                    int* __restrict__ blockSums) {
+  __shared__ int warpSums[32];
+  const long long base = (long long)blockIdx.x * kScanThreads * kScanItems;
+  int vals[kScanItems];
+  int tsum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const long long idx = base + (long long)threadIdx.x * kScanItems + i;
+    vals[i] = (idx < n) ? in[idx] : 0;
+    tsum += vals[i];
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warpSums[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int ws = warpSums[lane];
+    int wi = ws;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    warpSums[lane] = wi - ws;
+    if (lane == 31) blockSums[blockIdx.x] = wi;
+  }
+  __syncthreads();
+  int run = warpSums[wid] + incl - tsum;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const long long idx = base + (long long)threadIdx.x * kScanItems + i;
+    if (idx < n) out[idx] = run;
+    run += vals[i];
+  }
+}
+
+static __global__ void scan_blocksums_kernel(int* __restrict__ blockSums, int nBlocks, int* __restrict__ total) {
+  // single block, sequential chunks
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nBlocks; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = (i < nBlocks) ? blockSums[i] : 0;
+    // block inclusive scan
+    __shared__ int tmp[1024];
+    tmp[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+      const int t = (threadIdx.x >= o) ? tmp[threadIdx.x - o] : 0;
+      __syncthreads();
+      tmp[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nBlocks) blockSums[i] = carry + tmp[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += tmp[threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+static __global__ void scan_add_kernel(int* __restrict__ out, long long n, const int* __restrict__ blockSums,
+                                int* __restrict__ out2) {
+  const long long base = (long long)blockIdx.x * kScanThreads * kScanItems;
+  const int add = blockSums[blockIdx.x];
+  for (int i = threadIdx.x; i < kScanThreads * kScanItems; i += blockDim.x) {
+    const long long idx = base + i;
+    if (idx < n) {
+      const int v = out[idx] + add;
+      out[idx] = v;
+      if (out2) out2[idx] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// spreading: one CTA per output tile of the current w-slab
+// ---------------------------------------------------------------------------------------
+constexpr int kSpreadThreads = 256;
+
+template <int CH>
+__global__ void __launch_bounds__(kSpreadThreads)
+spread_tile_kernel(NufftGeom g, const int* __restrict__ offsets /*[nkeys+1]*/, const PtRec* __restrict__ rec,
+                   const float2* __restrict__ vals, long long valStride, int nch, int tw0 /*first w tile of slab*/,
+                   int slabTiles, float2* __restrict__ grid /*[ch][slabPlanes][ny][nx]*/) {
+  extern __shared__ float2 acc[];   // [nch][kTW][kTY][kTX]
+  const int tileInSlab = blockIdx.x;
+  const int tx = tileInSlab % g.ntx;
+  const int ty = (tileInSlab / g.ntx) % g.nty;
+  const int twl = tileInSlab / (g.ntx * g.nty);
+  const int tw = tw0 + twl;
+  constexpr int cells = kTX * kTY * kTW;
+  for (int i = threadIdx.x; i < nch * cells; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
+  const int W = g.W;
+  const float half = 0.5f * W;
+  const float invHalf = 1.0f / half;
+  // 27 (source tile, crossing-bits) ranges
+  for (int d = 0; d < 8; ++d) {
+    const int dx = d & 1, dy = (d >> 1) & 1, dw = (d >> 2) & 1;
+    const int stw = tw - dw;
+    if (stw < 0) continue;
+    const int stx = (tx - dx + g.ntx) % g.ntx;
+    const int sty = (ty - dy + g.nty) % g.nty;
+    const int stile = (stw * g.nty + sty) * g.ntx + stx;
+    for (int bits = 0; bits < 8; ++bits) {
+      if ((bits & d) != d) continue;
+      const int key = stile * 8 + bits;
+      const int beg = offsets[key], end = offsets[key + 1];
+      for (int p = beg + threadIdx.x; p < end; p += blockDim.x) {
+        const PtRec pr = rec[p];
+        // kernel values over the support that intersects this tile
+        float kx[kMaxW], ky[kMaxW], kw[kMaxW];
+        // local cell index of support start relative to tile origin (with wrap)
+        int lx = pr.ix0 - x0;
+        lx = ((lx % g.nx) + g.nx) % g.nx;
+        if (lx > g.nx / 2) lx -= g.nx;
+        int ly = pr.iy0 - y0;
+        ly = ((ly % g.ny) + g.ny) % g.ny;
+        if (ly > g.ny / 2) ly -= g.ny;
+        const int lw = pr.iw0 - w0;
+#pragma unroll
+        for (int t = 0; t < kMaxW; ++t) {
+          if (t < W) {
+            kx[t] = es_kernel(((float)t - pr.dx) * invHalf, g.beta);
+            ky[t] = es_kernel(((float)t - pr.dy) * invHalf, g.beta);
+            kw[t] = es_kernel(((float)t - pr.dw) * invHalf, g.beta);
+          }
+        }
+        float2 v[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+        const int xa = max(0, -lx), xb = min(W, kTX - lx);
+        const int ya = max(0, -ly), yb = min(W, kTY - ly);
+        const int wa = max(0, -lw), wb = min(W, kTW - lw);
+        for (int iw = wa; iw < wb; ++iw) {
+          for (int iy = ya; iy < yb; ++iy) {
+            const float kyw = ky[iy] * kw[iw];
+            const int rowBase = ((lw + iw) * kTY + (ly + iy)) * kTX;
+            for (int ix = xa; ix < xb; ++ix) {
+              const float k = kx[ix] * kyw;
+              const int cell = rowBase + lx + ix;
+#pragma unroll
+              for (int c = 0; c < CH; ++c) {
+                if (c < nch) {
+                  atomicAdd(&acc[c * cells + cell].x, k * v[c].x);
+                  atomicAdd(&acc[c * cells + cell].y, k * v[c].y);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // write the tile: grid[ch][plane][y][x], plane relative to slab start
+  const int slabPlanes = slabTiles * kTW;
+  for (int i = threadIdx.x; i < nch * cells; i += blockDim.x) {
+    const int c = i / cells, rem = i % cells;
+    const int lw = rem / (kTX * kTY), ly = (rem / kTX) % kTY, lx = rem % kTX;
+    const long long off = (((long long)c * slabPlanes + (twl * kTW + lw)) * g.ny + (y0 + ly)) * (long long)g.nx + (x0 + lx);
+    grid[off] = acc[i];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// w-sum: acc[ch][p] += sum_{planes j of slab} F[ch][j][a'][b'] exp(i n~_p t_j)
+// ---------------------------------------------------------------------------------------
+static __global__ void wsum_kernel(NufftGeom g, const float2* __restrict__ F, int nch, int slabPlanes, int jFirst,
+                            int planesUsed, const double* __restrict__ nTilde /*[P]*/, float2* __restrict__ acc,
+                            long long accStride) {
+  const long long P = (long long)g.Na * g.Nb;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(p / g.Nb), b = (int)(p % g.Nb);
+    int ap = a - g.Na / 2; if (ap < 0) ap += g.ny;
+    int bp = b - g.Nb / 2; if (bp < 0) bp += g.nx;
+    const double nt = nTilde[p];
+    // exp(i nt t_j), t_j = (j - jc) hw; recurrence in FP64
+    double s0, c0, sd, cd;
+    sincos(nt * (double)(jFirst - g.jc) * g.hw, &s0, &c0);
+    sincos(nt * g.hw, &sd, &cd);
+    double er = c0, ei = s0;
+    float2 sum[kMaxChan];
+#pragma unroll
+    for (int c = 0; c < kMaxChan; ++c) sum[c] = make_float2(0.f, 0.f);
+    for (int j = 0; j < planesUsed; ++j) {
+      const float fr = (float)er, fi = (float)ei;
+      const long long cell = ((long long)j * g.ny + ap) * g.nx + bp;
+#pragma unroll
+      for (int c = 0; c < kMaxChan; ++c) {
+        if (c < nch) {
+          const float2 f = F[(long long)c * slabPlanes * g.ny * g.nx + cell];
+          sum[c].x += f.x * fr - f.y * fi;
+          sum[c].y += f.x * fi + f.y * fr;
+        }
+      }
+      const double nr = er * cd - ei * sd;
+      ei = er * sd + ei * cd;
+      er = nr;
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxChan; ++c) {
+      if (c < nch) {
+        float2 o = acc[(long long)c * accStride + p];
+        o.x += sum[c].x;
+        o.y += sum[c].y;
+        acc[(long long)c * accStride + p] = o;
+      }
+    }
+  }
+}
+
+// image_l[p] += Re(decon_p exp(i wc n~_p) (acc_l + i dl_p su acc_u + i dm_p sv acc_v)); the
+// two extra channel groups carry the first-order lattice-residual terms when enabled.
+static __global__ void finalize_kernel(long long P, int levels, const float2* __restrict__ acc, long long accStride,
+                                const double* __restrict__ decon, const double* __restrict__ nTilde, double wc,
+                                int corrTerms, const double* __restrict__ dl, const double* __restrict__ dm, double su,
+                                double sv, float* __restrict__ image, long long ldImage) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincos(wc * nTilde[p], &sn, &cs);
+    const double dc = decon[p];
+    const double cfx = dc * cs, cfy = dc * sn;
+    for (int l = 0; l < levels; ++l) {
+      double2 a = to_d(acc[(long long)l * accStride + p]);
+      if (corrTerms) {
+        const double2 au = to_d(acc[(long long)(levels + l) * accStride + p]);
+        const double2 av = to_d(acc[(long long)(2 * levels + l) * accStride + p]);
+        const double tu = dl[p] * su, tv = dm[p] * sv;
+        a.x -= tu * au.y + tv * av.y;
+        a.y += tu * au.x + tv * av.x;
+      }
+      image[(long long)l * ldImage + p] += (float)(cfx * a.x - cfy * a.y);
+    }
+  }
+}
+
+// per-pixel deconvolution factor hx hy hw / (psi_x(b') psi_y(a') psi_w(n~)) with
+// psi(xi) = (W h / 2) int_{-1}^{1} es(z) cos(xi W h z / 2) dz (Gauss-Legendre)
+static __global__ void decon_kernel(NufftGeom g, const double* __restrict__ nTilde, const double* __restrict__ qz,
+                             const double* __restrict__ qw, int nq, double* __restrict__ decon) {
+  const long long P = (long long)g.Na * g.Nb;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(p / g.Nb), b = (int)(p % g.Nb);
+    const double bp = (double)(b - g.Nb / 2), ap = (double)(a - g.Na / 2);
+    const double nt = nTilde[p];
+    const double hxh = 0.5 * g.W * g.hx, hyh = 0.5 * g.W * g.hy, hwh = 0.5 * g.W * g.hw;
+    double fx = 0, fy = 0, fw = 0;
+    for (int q = 0; q < nq; ++q) {
+      const double z = qz[q];
+      const double t = 1.0 - z * z;
+      const double k = t > 0 ? exp((double)g.beta * (sqrt(t) - 1.0)) * qw[q] : 0.0;
+      fx += k * cos(bp * hxh * z);
+      fy += k * cos(ap * hyh * z);
+      fw += k * cos(nt * hwh * z);
+    }
+    fx *= hxh; fy *= hyh; fw *= hwh;
+    decon[p] = g.hx * g.hy * g.hw / (fx * fy * fw);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// direct sum out_l[p] += Re sum_k in_lk exp(i alpha (x_p u_k + y_p v_k + z_p w_k))
+// FP64 phase argument reduced to [-pi, pi) before the sine/cosine.
+// ---------------------------------------------------------------------------------------
+constexpr int kDirectThreads = 256;
+constexpr int kDirectChunk = 256;
+
+template <typename TC, typename C, typename TO, int CH>
+__global__ void __launch_bounds__(kDirectThreads)
+direct_sum_kernel(double alpha, long long nIn, const C* __restrict__ input, long long ldIn,
+                  const TC* __restrict__ u, const TC* __restrict__ v, const TC* __restrict__ w, long long nOut,
+                  const TC* __restrict__ x, const TC* __restrict__ y, const TC* __restrict__ z, TO* __restrict__ out,
+                  long long ldOut, int nch, int fp64Trig) {
+  __shared__ double su[kDirectChunk], sv[kDirectChunk], sw[kDirectChunk];
+  __shared__ C sval[CH][kDirectChunk];
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool active = p < nOut;
+  const double xp = active ? (double)x[p] * alpha : 0.0;
+  const double yp = active ? (double)y[p] * alpha : 0.0;
+  const double zp = active ? (double)z[p] * alpha : 0.0;
+  double acc[CH];
+#pragma unroll
+  for (int c = 0; c < CH; ++c) acc[c] = 0.0;
+  const double twopi = 6.283185307179586476925286766559;
+  const double inv2pi = 1.0 / twopi;
+  for (long long k0 = 0; k0 < nIn; k0 += kDirectChunk) {
+    const int nk = (nIn - k0 < (long long)kDirectChunk) ? (int)(nIn - k0) : kDirectChunk;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+      su[i] = (double)u[k0 + i];
+      sv[i] = (double)v[k0 + i];
+      sw[i] = (double)w[k0 + i];
+#pragma unroll
+      for (int c = 0; c < CH; ++c)
+        if (c < nch) sval[c][i] = input[(long long)c * ldIn + k0 + i];
+    }
+    __syncthreads();
+    if (active) {
+      for (int i = 0; i < nk; ++i) {
+        double ph = fma(xp, su[i], fma(yp, sv[i], zp * sw[i]));
+        ph = fma(-twopi, rint(ph * inv2pi), ph);
+        double s, cs;
+        if (fp64Trig) {
+          sincos(ph, &s, &cs);
+        } else {
+          float sf, cf;
+          __sincosf((float)ph, &sf, &cf);
+          s = sf;
+          cs = cf;
+        }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+          if (c < nch) {
+            const C a = sval[c][i];
+            acc[c] = fma((double)a.x, cs, fma(-(double)a.y, s, acc[c]));
+          }
+        }
+      }
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+      if (c < nch) out[(long long)c * ldOut + p] += (TO)acc[c];
+  }
+}
+
+}  // namespace bippb200

@@ -1,0 +1,462 @@
+// Batched Bluebild pipeline: per time step S, antenna positions and wavelength go
+// through flagging, Gram, generalized eigensolve, energy-level binning, virtual
+// visibilities and the NUFFT, with every stage batched over the steps of a call.
+//
+// Reference flow (per step, serial on the host): bipp::eigh_gram
+// (src/eigensolver.cpp:129-225) -> level selection (python/bipp/filter.py,
+// src/image_synthesis.cpp:110-122) -> host::virtual_vis (src/host/virtual_vis.cpp:19-73)
+// -> NUFFT add/get (src/nufft_synthesis.cpp:134-169). Here the steps of one call share
+// one eigensolver launch sequence per chunk of steps and one NUFFT per call ("batched"
+// mode) or run one step and one level at a time ("plain" mode, the straightforward GPU
+// form used as the comparison point).
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "context.hpp"
+#include "eig.hpp"
+#include "eig_kernels.cuh"
+#include "nufft.hpp"
+
+namespace bippb200 {
+
+// antenna UVW coordinates U[b][i][c] = sum_k xyz[b][i][k] basis[k][c] (FP64), uvw scale,
+// and the per-step range of the w coordinate. xyz layout [b][i][3].
+__global__ void antenna_uvw_kernel(int nSteps, int nAnt, const double* __restrict__ xyz, const double* __restrict__ wl,
+                                   const double* __restrict__ basis, double* __restrict__ U, double* __restrict__ scale,
+                                   double* __restrict__ wrange) {
+  const int b = blockIdx.x;
+  if (b >= nSteps) return;
+  __shared__ double bs[9];
+  __shared__ double rmin[32], rmax[32];
+  if (threadIdx.x < 9) bs[threadIdx.x] = basis[threadIdx.x];
+  __syncthreads();
+  double lo = 1e300, hi = -1e300;
+  for (int i = threadIdx.x; i < nAnt; i += blockDim.x) {
+    const double* p = xyz + ((long long)b * nAnt + i) * 3;
+    double u[3];
+    for (int c = 0; c < 3; ++c) u[c] = p[0] * bs[0 + 3 * c] + p[1] * bs[1 + 3 * c] + p[2] * bs[2 + 3 * c];
+    double* o = U + ((long long)b * nAnt + i) * 3;
+    o[0] = u[0];
+    o[1] = u[1];
+    o[2] = u[2];
+    lo = fmin(lo, u[2]);
+    hi = fmax(hi, u[2]);
+  }
+  lo = block_min(lo, rmin, 1e300);
+  hi = block_max(hi, rmax, -1e300);
+  if (threadIdx.x == 0) {
+    const double s = 2.0 * 3.14159265358979323846 / wl[b];
+    scale[b] = s;
+    wrange[b] = (hi - lo) * s;
+  }
+}
+
+// xyz [b][i][3] -> [b][3][nAnt] for the Gram computation of the eigensolver
+__global__ void xyz_transpose_kernel(long long total, int nAnt, const double* __restrict__ in, double* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long b = e / (3ll * nAnt);
+    const int r = (int)(e % (3ll * nAnt));
+    const int c = r / nAnt, i = r % nAnt;
+    out[e] = in[(b * nAnt + i) * 3 + c];
+  }
+}
+
+__device__ __forceinline__ double filter_value(int f, double d) {
+  // python/bipp/filter.py:7-26
+  switch (f) {
+    case 0: return d;
+    case 1: return d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0);
+    case 2: { const double s = d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0); return s * sqrt(s * d); }
+    case 3: return d != 0 ? 1.0 / d : 0.0;
+    case 4: { const double s = d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0); const double r = s * sqrt(s * d); return r != 0 ? 1.0 / r : 0.0; }
+  }
+  return d;
+}
+
+// per step: kscale[b][c] = (1/nVis) filter(d_c); per (step, level) the contiguous range of
+// eigenvalue indices with lo <= d <= hi (eigenvalues are ascending)
+__global__ void levels_kernel(int nSteps, int Nmax, int nLevels, const double* __restrict__ intervals, int filt,
+                              const int* __restrict__ nred, const long long* __restrict__ nvis,
+                              const double* __restrict__ lam, float* __restrict__ kscale, int* __restrict__ kbeg,
+                              int* __restrict__ kend) {
+  const int b = blockIdx.x;
+  if (b >= nSteps) return;
+  const int n = nred[b];
+  const double sc = nvis[b] ? 1.0 / (double)nvis[b] : 0.0;
+  const double* d = lam + (long long)b * Nmax;
+  for (int c = threadIdx.x; c < Nmax; c += blockDim.x)
+    kscale[(long long)b * Nmax + c] = (c < n && d[c] != 0.0) ? (float)(sc * filter_value(filt, d[c])) : 0.0f;
+  if (threadIdx.x < nLevels) {
+    const int l = threadIdx.x;
+    const double lo = intervals[2 * l], hi = intervals[2 * l + 1];
+    int a = 0;
+    while (a < n && d[a] < lo) ++a;
+    int e = a;
+    while (e < n && d[e] <= hi) ++e;
+    kbeg[b * nLevels + l] = a;
+    kend[b * nLevels + l] = e;
+  }
+}
+
+__global__ void scale_images_kernel(float* __restrict__ img, long long n, float s) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    img[i] *= s;
+}
+
+}  // namespace bippb200
+
+using namespace bippb200;
+
+struct bipp_pipeline_s {
+  bipp_ctx_s* ctx = nullptr;
+  size_t nAnt = 0, nLevels = 0, chunk = 256, maxSteps = 0;
+  int filter = 0, mode = 0;
+  double tol = 1e-5;
+  long long P = 0;
+  std::vector<double> intervals;
+  NufftCore core;
+  EigWork<float> eig;
+  DevBuf basis, intervalsD;
+  DevBuf S, xyz, xyzT, wl, antUVW, uvwScale, wrange;
+  DevBuf idx, nred, nvis, status, lam, kscale, kbeg, kend, vv, pairOff;
+  DevBuf images;
+  long long stepsDone = 0;
+  bool timing = false;
+  double stageMs[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<double> lastLam;
+  std::vector<int> lastNred;
+};
+
+static void pipeline_alloc(bipp_pipeline_s* p, size_t steps) {
+  bipp_ctx_s* ctx = p->ctx;
+  const size_t N = p->nAnt, L = p->nLevels;
+  if (steps <= p->maxSteps && p->S.bytes()) return;
+  p->maxSteps = std::max(steps, p->maxSteps);
+  const size_t T = p->maxSteps;
+  p->S.alloc(ctx, T * N * N * sizeof(float2));
+  p->xyz.alloc(ctx, T * N * 3 * sizeof(double));
+  p->xyzT.alloc(ctx, T * N * 3 * sizeof(double));
+  p->wl.alloc(ctx, T * sizeof(double));
+  p->antUVW.alloc(ctx, T * N * 3 * sizeof(double));
+  p->uvwScale.alloc(ctx, T * sizeof(double));
+  p->wrange.alloc(ctx, T * sizeof(double));
+  p->idx.alloc(ctx, T * N * sizeof(int));
+  p->nred.alloc(ctx, T * sizeof(int));
+  p->nvis.alloc(ctx, T * sizeof(long long));
+  p->status.alloc(ctx, T * sizeof(int));
+  p->lam.alloc(ctx, T * N * sizeof(double));
+  p->kscale.alloc(ctx, T * N * sizeof(float));
+  p->kbeg.alloc(ctx, T * L * sizeof(int));
+  p->kend.alloc(ctx, T * L * sizeof(int));
+  p->pairOff.alloc(ctx, (T + 1) * sizeof(long long));
+}
+
+// eigensolve + levels + VV for steps [s0, s0+nb) of the call, then scatter their points.
+static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector<long long>& pairOffH,
+                           int levelsInTransform, int levelOffset, bool scatterOnly, double* ms) {
+  bipp_ctx_s* ctx = p->ctx;
+  const int N = (int)p->nAnt, L = (int)p->nLevels;
+  const long long n2 = (long long)N * N;
+  cudaEvent_t e0, e1, e2;
+  if (ms) {
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    cudaEventRecord(e0, ctx->stream);
+  }
+  float2* X = p->eig.X(true);
+  if (!scatterOnly) {
+    EigLaunch<float> E{};
+    E.nBatch = nb; E.nBeam = N; E.nAnt = N; E.Nmax = N;
+    E.S = p->S.get<float2>() + (long long)s0 * n2; E.sStride = n2; E.lds = N;
+    E.xyz = p->xyzT.get<double>(); E.xyzStride = 3ll * N; E.ldxyz = N; E.wl = p->wl.get<double>();
+    E.mode = 0; E.eps = std::numeric_limits<float>::epsilon(); E.gram = true; E.identityW = true;
+    E.idx = p->idx.get<int>(); E.nred = p->nred.get<int>(); E.nvis = p->nvis.get<long long>();
+    E.status = p->status.get<int>(); E.lam = p->lam.get<double>();
+    E.doFlag = 0; E.batchOffset = s0;
+    eig_launch<float>(ctx, E, p->eig);
+    levels_kernel<<<nb, 128, 0, ctx->stream>>>(nb, N, L, p->intervalsD.get<double>(), p->filter, p->nred.get<int>() + s0,
+                                               p->nvis.get<long long>() + s0, p->lam.get<double>() + (long long)s0 * N,
+                                               p->kscale.get<float>() + (long long)s0 * N, p->kbeg.get<int>() + s0 * L,
+                                               p->kend.get<int>() + s0 * L);
+    B2_CHECK_LAUNCH();
+    // VV[b][l] lower triangle = X diag(kscale) X^H over the level's eigenvalue range
+    GemmArgs<float2> g{};
+    g.A = X; g.strideA = n2; g.lda = N; g.opA = 0;
+    g.B = X; g.strideB = n2; g.ldb = N; g.opB = 1;
+    g.Cm = p->vv.get<float2>(); g.strideC = n2 * L; g.ldc = N; g.strideCLevel = n2;
+    g.n = p->nred.get<int>() + s0; g.outMode = 2; g.levels = L;
+    g.kscale = p->kscale.get<float>() + (long long)s0 * N; g.strideK = N;
+    g.kbeg = p->kbeg.get<int>() + s0 * L; g.kend = p->kend.get<int>() + s0 * L;
+    const int tiles = (N + kGemmBM - 1) / kGemmBM;
+    gemm_kernel<float2, float><<<dim3(tiles, tiles, nb * L), kGemmThreads, 0, ctx->stream>>>(g);
+    B2_CHECK_LAUNCH();
+  }
+  if (ms) cudaEventRecord(e1, ctx->stream);
+  // scatter points of these steps
+  std::vector<long long> rel(nb + 1);
+  for (int i = 0; i <= nb; ++i) rel[i] = pairOffH[s0 + i] - pairOffH[s0];
+  DevBuf relD(ctx, (nb + 1) * sizeof(long long));
+  h2d(ctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
+  PipelinePoints pp{};
+  pp.nSteps = nb;
+  pp.nred = p->nred.get<int>() + s0;
+  pp.idx = p->idx.get<int>() + (long long)s0 * N;
+  pp.antUVW = p->antUVW.get<double>() + (long long)s0 * N * 3;
+  pp.uvwScale = p->uvwScale.get<double>() + s0;
+  pp.Nmax = N;
+  pp.nAnt = N;
+  pp.vv = p->vv.get<float2>() + (long long)levelOffset * n2;
+  pp.vvStepStride = n2 * L;
+  pp.vvLevelStride = n2;
+  pp.levels = levelsInTransform;
+  const long long total = rel[nb];
+  if (total > 0) {
+    const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
+    pipeline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.cursor(), relD.get<long long>(),
+                                                         p->core.records(), p->core.values(), p->core.value_stride(),
+                                                         p->core.sincos64() ? 1 : 0);
+    B2_CHECK_LAUNCH();
+  }
+  if (ms) {
+    cudaEventRecord(e2, ctx->stream);
+    cudaEventSynchronize(e2);
+    float a, b;
+    cudaEventElapsedTime(&a, e0, e1);
+    cudaEventElapsedTime(&b, e1, e2);
+    ms[0] += a;
+    ms[2] += b;
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+  }
+}
+
+static void pipeline_count(bipp_pipeline_s* p, int s0, int nb, const std::vector<long long>& pairOffH) {
+  bipp_ctx_s* ctx = p->ctx;
+  const int N = (int)p->nAnt;
+  std::vector<long long> rel(nb + 1);
+  for (int i = 0; i <= nb; ++i) rel[i] = pairOffH[s0 + i] - pairOffH[s0];
+  DevBuf relD(ctx, (nb + 1) * sizeof(long long));
+  h2d(ctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
+  PipelinePoints pp{};
+  pp.nSteps = nb;
+  pp.nred = p->nred.get<int>() + s0;
+  pp.idx = p->idx.get<int>() + (long long)s0 * N;
+  pp.antUVW = p->antUVW.get<double>() + (long long)s0 * N * 3;
+  pp.uvwScale = p->uvwScale.get<double>() + s0;
+  pp.Nmax = N;
+  pp.nAnt = N;
+  const long long total = rel[nb];
+  if (total > 0) {
+    const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
+    pipeline_count_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.counts(), relD.get<long long>());
+    B2_CHECK_LAUNCH();
+  }
+  sync(ctx);
+}
+
+static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, const double* xyz, const double* wl,
+                             int onDevice) {
+  bipp_ctx_s* ctx = p->ctx;
+  require(nSteps > 0, "no steps");
+  require(s && xyz && wl, "null pointer", BIPP_INVALID_POINTER_ERROR);
+  pipeline_alloc(p, nSteps);
+  const int N = (int)p->nAnt, L = (int)p->nLevels;
+  const long long n2 = (long long)N * N;
+  const int T = (int)nSteps;
+  cudaEvent_t ev0, ev1;
+  if (p->timing) { cudaEventCreate(&ev0); cudaEventCreate(&ev1); cudaEventRecord(ev0, ctx->stream); }
+  // inputs
+  const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  B2_CUDA(cudaMemcpyAsync(p->S.get(), s, (size_t)T * n2 * sizeof(float2), kind, ctx->stream));
+  B2_CUDA(cudaMemcpyAsync(p->xyz.get(), xyz, (size_t)T * N * 3 * sizeof(double), kind, ctx->stream));
+  B2_CUDA(cudaMemcpyAsync(p->wl.get(), wl, (size_t)T * sizeof(double), kind, ctx->stream));
+  antenna_uvw_kernel<<<T, 256, 0, ctx->stream>>>(T, N, p->xyz.get<double>(), p->wl.get<double>(), p->basis.get<double>(),
+                                                 p->antUVW.get<double>(), p->uvwScale.get<double>(),
+                                                 p->wrange.get<double>());
+  xyz_transpose_kernel<<<1024, 256, 0, ctx->stream>>>((long long)T * 3 * N, N, p->xyz.get<double>(), p->xyzT.get<double>());
+  p->status.zero();
+  // flags for every step
+  {
+    const size_t smem = 2 * (size_t)N * sizeof(int);
+    auto k = prep_kernel<float>;
+    smem_optin(k, smem);
+    k<<<T, kPrepThreads, smem, ctx->stream>>>(N, p->S.get<float2>(), n2, N, p->xyzT.get<double>(), 3ll * N, N,
+                                              p->wl.get<double>(), 0, std::numeric_limits<float>::epsilon(), 1, N,
+                                              p->idx.get<int>(), p->nred.get<int>(), p->nvis.get<long long>(),
+                                              nullptr, nullptr, p->status.get<int>(), 1, 0, 0);
+    B2_CHECK_LAUNCH();
+  }
+  std::vector<int> nredH(T);
+  std::vector<double> wr(T);
+  d2h(ctx, nredH.data(), p->nred.get(), T * sizeof(int));
+  d2h(ctx, wr.data(), p->wrange.get(), T * sizeof(double));
+  sync(ctx);
+  if (p->timing) {
+    cudaEventRecord(ev1, ctx->stream);
+    cudaEventSynchronize(ev1);
+    float a;
+    cudaEventElapsedTime(&a, ev0, ev1);
+    p->stageMs[2] += a;
+  }
+  std::vector<long long> pairOff(T + 1, 0);
+  for (int b = 0; b < T; ++b) pairOff[b + 1] = pairOff[b] + (long long)nredH[b] * (nredH[b] + 1) / 2;
+  double Xw = 0;
+  for (int b = 0; b < T; ++b) Xw = std::max(Xw, wr[b]);
+  const int chunk = (int)p->chunk;
+  p->eig.reserve(ctx, std::min(chunk, T), N);
+  p->vv.ensure(ctx, (size_t)std::min(chunk, T) * L * n2 * sizeof(float2));
+  double* ms = p->timing ? p->stageMs : nullptr;
+
+  if (p->mode == 0) {
+    // batched: one NUFFT over all steps of the call, all levels as channels
+    p->core.begin(-Xw, Xw);
+    for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
+    p->core.end_count(pairOff[T]);
+    for (int s0 = 0; s0 < T; s0 += chunk) pipeline_chunk(p, s0, std::min(chunk, T - s0), pairOff, L, 0, false, ms);
+    double nm[3] = {0, 0, 0};
+    p->core.execute(p->images.get<float>(), p->P, p->timing ? nm : nullptr);
+    p->stageMs[3] += nm[0];
+    p->stageMs[4] += nm[1];
+    p->stageMs[5] += nm[2];
+  } else {
+    // plain: one step at a time, one NUFFT per step and level
+    for (int b = 0; b < T; ++b) {
+      for (int l = 0; l < L; ++l) {
+        p->core.begin(-wr[b], wr[b]);
+        pipeline_count(p, b, 1, pairOff);
+        p->core.end_count(pairOff[b + 1] - pairOff[b]);
+        pipeline_chunk(p, b, 1, pairOff, 1, l, l > 0, ms);
+        double nm[3] = {0, 0, 0};
+        p->core.execute(p->images.get<float>() + (long long)l * p->P, p->P, p->timing ? nm : nullptr);
+        p->stageMs[3] += nm[0];
+        p->stageMs[4] += nm[1];
+        p->stageMs[5] += nm[2];
+      }
+    }
+  }
+  // keep eigenvalues of this call for calibration (host copy on demand)
+  p->lastNred = nredH;
+  p->stepsDone += T;
+  std::vector<int> st(T);
+  d2h(ctx, st.data(), p->status.get(), T * sizeof(int));
+  sync(ctx);
+  if (p->timing) { cudaEventDestroy(ev0); cudaEventDestroy(ev1); }
+  for (int b = 0; b < T; ++b)
+    if (st[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
+}
+
+extern "C" {
+
+BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, bipp_pipeline_t* out) {
+  return guard([&] {
+    require(ctx && cfg && out, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    require(cfg->nAntenna > 0 && cfg->nAntenna <= 4096, "nAntenna must be in [1, 4096]");
+    require(cfg->nLevels >= 1 && cfg->nLevels <= 4, "nLevels must be in [1, 4]");
+    require(cfg->intervals && cfg->pixelN && cfg->uvwBasis, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    require(cfg->gridA >= 2 && cfg->gridB >= 2, "pixel lattice must be at least 2 x 2");
+    require(cfg->filter >= 0 && cfg->filter <= 4, "unknown filter");
+    auto p = std::make_unique<bipp_pipeline_s>();
+    p->ctx = ctx;
+    p->nAnt = cfg->nAntenna;
+    p->nLevels = cfg->nLevels;
+    p->chunk = cfg->chunkSteps ? cfg->chunkSteps : 256;
+    p->filter = cfg->filter;
+    p->mode = cfg->mode;
+    p->tol = cfg->tolerance > 0 ? cfg->tolerance : 1e-5;
+    p->intervals.assign(cfg->intervals, cfg->intervals + 2 * cfg->nLevels);
+    Lattice lat;
+    lat.ok = true;
+    lat.Na = (int)cfg->gridA;
+    lat.Nb = (int)cfg->gridB;
+    lat.l0 = cfg->lattice[0]; lat.m0 = cfg->lattice[1];
+    lat.Al = cfg->lattice[2]; lat.Bl = cfg->lattice[3];
+    lat.Am = cfg->lattice[4]; lat.Bm = cfg->lattice[5];
+    p->P = (long long)cfg->gridA * cfg->gridB;
+    std::vector<double> n(cfg->pixelN, cfg->pixelN + p->P);
+    p->core.setup(ctx, lat, n, p->tol, p->mode == 0 ? (int)cfg->nLevels : 1);
+    p->basis.alloc(ctx, 9 * sizeof(double));
+    h2d(ctx, p->basis.get(), cfg->uvwBasis, 9 * sizeof(double));
+    p->intervalsD.alloc(ctx, p->intervals.size() * sizeof(double));
+    h2d(ctx, p->intervalsD.get(), p->intervals.data(), p->intervals.size() * sizeof(double));
+    p->images.alloc(ctx, (size_t)cfg->nLevels * p->P * sizeof(float));
+    p->images.zero();
+    if (cfg->maxSteps) pipeline_alloc(p.get(), cfg->maxSteps);
+    sync(ctx);
+    *out = p.release();
+  });
+}
+
+BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz, const double* wl,
+                                int onDevice) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
+  });
+}
+
+BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize, int onDevice) {
+  return guard([&] {
+    require(pl && images, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    bipp_ctx_s* ctx = pl->ctx;
+    const long long n = (long long)pl->nLevels * pl->P;
+    const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    B2_CUDA(cudaMemcpyAsync(images, pl->images.get(), n * sizeof(float), kind, ctx->stream));
+    if (normalize && pl->stepsDone > 0) {
+      const float s = 1.0f / (float)pl->stepsDone;
+      if (onDevice) {
+        scale_images_kernel<<<1024, 256, 0, ctx->stream>>>(images, n, s);
+        B2_CHECK_LAUNCH();
+        sync(ctx);
+      } else {
+        sync(ctx);
+        for (long long i = 0; i < n; ++i) images[i] *= s;
+      }
+    } else {
+      sync(ctx);
+    }
+  });
+}
+
+BippError bipp_pipeline_reset(bipp_pipeline_t pl) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    pl->images.zero();
+    pl->stepsDone = 0;
+    for (double& x : pl->stageMs) x = 0;
+    sync(pl->ctx);
+  });
+}
+
+BippError bipp_pipeline_last_eigenvalues(bipp_pipeline_t pl, double* d, int* nReduced) {
+  return guard([&] {
+    require(pl && d && nReduced, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    const size_t T = pl->lastNred.size();
+    d2h(pl->ctx, d, pl->lam.get(), T * pl->nAnt * sizeof(double));
+    sync(pl->ctx);
+    for (size_t b = 0; b < T; ++b) {
+      nReduced[b] = pl->lastNred[b];
+      for (size_t c = pl->lastNred[b]; c < pl->nAnt; ++c) d[b * pl->nAnt + c] = 0.0;
+    }
+  });
+}
+
+BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    if (enable >= 0) pl->timing = enable != 0;
+    if (ms)
+      for (int i = 0; i < 6; ++i) ms[i] = pl->stageMs[i];
+  });
+}
+
+BippError bipp_pipeline_destroy(bipp_pipeline_t pl) {
+  return guard([&] {
+    if (!pl) return;
+    bipp_ctx_s* ctx = pl->ctx;
+    delete pl;
+    sync(ctx);
+  });
+}
+
+}  // extern "C"

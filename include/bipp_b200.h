@@ -1,0 +1,234 @@
+/*
+ * bipp_b200.h - C ABI of the B200-native Bluebild imaging path.
+ *
+ * Every entry point takes plain pointers and sizes and returns a BippError. Array
+ * layouts are those of the reference API: column-major with leading dimensions,
+ * complex values as interleaved (re, im) pairs (std::complex layout), uvw and lmn as
+ * (n x 3) column-major, i.e. three separate coordinate arrays. Unless stated
+ * otherwise pointers are host pointers and calls are synchronous on return.
+ * After a failure, bipp_last_error() returns a message for the calling thread.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   Context                       include/bipp/context.hpp:17-76, src/context_internal.cpp:27-73
+ *   eigh / eigh_gram              include/bipp/bipp.hpp:47-75, src/eigensolver.cpp:40-225
+ *   host::gram_matrix             src/host/gram_matrix.hpp:15-17
+ *   host::virtual_vis             src/host/virtual_vis.hpp:15-17
+ *   nuft_sum (host and GPU)       src/host/kernels/nuft_sum.hpp, src/gpu/kernels/nuft_sum.hpp
+ *   NUFFTInterface add/get_image  src/nufft_interface.hpp:13-21, src/gpu/nufft.hpp:28-235
+ *   DomainPartition::grid         src/host/domain_partition.hpp:35-101
+ *   image_synthesis               include/bipp/image_synthesis.hpp:160-163, src/image_synthesis.cpp:28-182
+ */
+#pragma once
+
+#include <stddef.h>
+
+#include "bipp/enums.h"
+#include "bipp/errors.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BIPP_B200_EXPORT __attribute__((visibility("default")))
+
+typedef struct bipp_ctx_s* bipp_ctx_t;
+typedef struct bipp_nufft_s* bipp_nufft_t;
+typedef struct bipp_pipeline_s* bipp_pipeline_t;
+
+/* Message of the last failed call on this thread (empty if none). */
+BIPP_B200_EXPORT const char* bipp_last_error(void);
+
+/* ---- context ------------------------------------------------------------------- */
+
+/* Create a context on the current CUDA device (replaces Context(BippProcessingUnit),
+ * include/bipp/context.hpp:25). BIPP_PU_AUTO and BIPP_PU_GPU select the GPU;
+ * BIPP_PU_CPU is rejected with BIPP_INVALID_PARAMETER_ERROR: this library has no CPU
+ * path. Fails with BIPP_GPU_SUPPORT_ERROR when no CUDA device is present. */
+BIPP_B200_EXPORT BippError bipp_ctx_create(BippProcessingUnit pu, bipp_ctx_t* ctx);
+/* As bipp_ctx_create on an explicit device (the reference picks rank % deviceCount,
+ * src/context_internal.cpp:59-66). */
+BIPP_B200_EXPORT BippError bipp_ctx_create_on_device(BippProcessingUnit pu, int device, bipp_ctx_t* ctx);
+BIPP_B200_EXPORT BippError bipp_ctx_destroy(bipp_ctx_t ctx);
+/* Processing unit actually used (always BIPP_PU_GPU). Context::processing_unit(),
+ * include/bipp/context.hpp:60. */
+BIPP_B200_EXPORT BippError bipp_ctx_processing_unit(bipp_ctx_t ctx, BippProcessingUnit* pu);
+/* CUDA stream used by the context (as void*, a cudaStream_t). */
+BIPP_B200_EXPORT BippError bipp_ctx_stream(bipp_ctx_t ctx, void** stream);
+
+/* ---- eigensolvers ----------------------------------------------------------------- */
+
+/* Generalized eigenproblem S x = d G x with G the beamformed Gram matrix of the
+ * antenna positions; replaces bipp::eigh_gram<float/double> (include/bipp/bipp.hpp:70-75,
+ * src/eigensolver.cpp:129-225). s: nBeam x nBeam (lower triangle used), w: nAntenna x
+ * nBeam, xyz: nAntenna x 3. Outputs d[nBeam] ascending, zero padded; v nAntenna x nBeam
+ * zero padded; *nBeamReduced and *scale = 1/nVis as the reference's returned pair. */
+BIPP_B200_EXPORT BippError bipp_eigh_gram_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam,
+                                            const void* s, size_t lds, const void* w, size_t ldw,
+                                            const float* xyz, size_t ldxyz, float* d, void* v, size_t ldv,
+                                            size_t* nBeamReduced, float* scale);
+BIPP_B200_EXPORT BippError bipp_eigh_gram_d(bipp_ctx_t ctx, double wl, size_t nAntenna, size_t nBeam,
+                                            const void* s, size_t lds, const void* w, size_t ldw,
+                                            const double* xyz, size_t ldxyz, double* d, void* v, size_t ldv,
+                                            size_t* nBeamReduced, double* scale);
+
+/* Standard Hermitian eigenproblem of S; replaces bipp::eigh<float/double>
+ * (include/bipp/bipp.hpp:47-51, src/eigensolver.cpp:40-127). */
+BIPP_B200_EXPORT BippError bipp_eigh_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam, const void* s,
+                                       size_t lds, const void* w, size_t ldw, float* d, void* v, size_t ldv,
+                                       size_t* nBeamReduced, float* scale);
+BIPP_B200_EXPORT BippError bipp_eigh_d(bipp_ctx_t ctx, double wl, size_t nAntenna, size_t nBeam, const void* s,
+                                       size_t lds, const void* w, size_t ldw, double* d, void* v, size_t ldv,
+                                       size_t* nBeamReduced, double* scale);
+
+/* Batched eigh_gram with W = I (nBeam = nAntenna) over nBatch independent time steps,
+ * one launch sequence for the whole batch. The per-step loop of the reference's
+ * dataset creation (python/bipp/apps/create_dataset.py:78-103) calls eigh_gram once per
+ * step; this is its batched form. s: [nBatch][nAntenna x nAntenna] (lds = nAntenna),
+ * xyz: [nBatch][nAntenna x 3], wl: [nBatch]; d: [nBatch][nAntenna], v: [nBatch][nAntenna x
+ * nAntenna]; nBeamReduced, scale: [nBatch]. */
+BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna,
+                                                    const float* wl, const void* s, const float* xyz, float* d,
+                                                    void* v, size_t* nBeamReduced, float* scale);
+
+/* Gram matrix G = W^H sinc(2|p_i - p_j| / wl) W, nBeam x nBeam complex; replaces
+ * bipp::host::gram_matrix (src/host/gram_matrix.hpp:15-17). */
+BIPP_B200_EXPORT BippError bipp_gram_matrix_s(bipp_ctx_t ctx, size_t nAntenna, size_t nBeam, const void* w,
+                                              size_t ldw, const float* xyz, size_t ldxyz, float wl, void* g,
+                                              size_t ldg);
+BIPP_B200_EXPORT BippError bipp_gram_matrix_d(bipp_ctx_t ctx, size_t nAntenna, size_t nBeam, const void* w,
+                                              size_t ldw, const double* xyz, size_t ldxyz, double wl, void* g,
+                                              size_t ldg);
+
+/* Virtual visibilities VV = V_k diag(scale d_k) V_k^H over the non-zero entries of d,
+ * written as a column-major nAntenna x nAntenna matrix; replaces
+ * bipp::host::virtual_vis (src/host/virtual_vis.hpp:15-17). */
+BIPP_B200_EXPORT BippError bipp_virtual_vis_s(bipp_ctx_t ctx, float scale, size_t nAntenna, size_t nBeam,
+                                              const float* d, const void* v, size_t ldv, void* vv);
+BIPP_B200_EXPORT BippError bipp_virtual_vis_d(bipp_ctx_t ctx, double scale, size_t nAntenna, size_t nBeam,
+                                              const double* d, const void* v, size_t ldv, void* vv);
+
+/* Direct sum out[p] += Re sum_k input_k exp(i alpha (x_p u_k + y_p v_k + z_p w_k));
+ * replaces bipp::host::nuft_sum / bipp::gpu::nuft_sum (src/host/kernels/nuft_sum.cpp:9-31,
+ * src/gpu/kernels/nuft_sum.cu:24-84). The phase argument is formed and reduced in FP64;
+ * the _s variant evaluates sine/cosine in FP32 on the reduced argument, _d in FP64. */
+BIPP_B200_EXPORT BippError bipp_nuft_sum_s(bipp_ctx_t ctx, float alpha, size_t nIn, const void* input,
+                                           const float* u, const float* v, const float* w, size_t nOut,
+                                           const float* x, const float* y, const float* z, float* out);
+BIPP_B200_EXPORT BippError bipp_nuft_sum_d(bipp_ctx_t ctx, double alpha, size_t nIn, const void* input,
+                                           const double* u, const double* v, const double* w, size_t nOut,
+                                           const double* x, const double* y, const double* z, double* out);
+/* Multi-channel direct sum on DEVICE pointers (FP64 coordinates and outputs, FP32 complex
+ * values [nch][ldIn]): the GPU check used for large pixel subsets. */
+BIPP_B200_EXPORT BippError bipp_nuft_sum_multi_device(bipp_ctx_t ctx, double alpha, size_t nIn, size_t nch,
+                                                      const void* values, size_t ldIn, const double* u,
+                                                      const double* v, const double* w, size_t nOut,
+                                                      const double* x, const double* y, const double* z,
+                                                      double* out, size_t ldOut, int fp64Trig);
+
+/* Bucket partition of points into a regular grid of groups; replaces
+ * DomainPartition::grid (src/host/domain_partition.hpp:35-101). permut[i] is the sorted
+ * position of point i; groupBegin/groupSize have dims[0]*dims[1]*dims[2] entries. A grid of
+ * one group returns the identity (DomainPartition::none). */
+BIPP_B200_EXPORT BippError bipp_domain_partition_grid_s(bipp_ctx_t ctx, const size_t* dims, size_t n,
+                                                        const float* x, const float* y, const float* z,
+                                                        size_t* permut, size_t* groupBegin, size_t* groupSize);
+BIPP_B200_EXPORT BippError bipp_domain_partition_grid_d(bipp_ctx_t ctx, const size_t* dims, size_t n,
+                                                        const double* x, const double* y, const double* z,
+                                                        size_t* permut, size_t* groupBegin, size_t* groupSize);
+
+/* ---- NUFFT synthesis: collect / get ---------------------------------------------------- */
+
+/* Mirrors NufftSynthesisOptions and Partition (include/bipp/image_synthesis.hpp:23-148). */
+typedef struct {
+  int precision;            /* BippPrecision */
+  float tolerance;          /* NUFFT tolerance */
+  size_t sampleBatchSize;   /* 0 = automatic */
+  int partitionMethod;      /* 0 = Auto, 1 = None, 2 = Grid */
+  size_t partitionGrid[3];  /* Grid dimensions (u, v, w) */
+  int normalizeImage;       /* divide by the number of samples */
+  int applyScaling;         /* accepted; scale is always applied, as in the reference */
+} bipp_nufft_options;
+
+/* Create a collector for nImages images over nPixel output points (lmn: nPixel x 3,
+ * FP32 as the ImageProp interface provides) and nBaselines points per added sample;
+ * replaces gpu::NUFFT (src/gpu/nufft.hpp:31-62). */
+BIPP_B200_EXPORT BippError bipp_nufft_create(bipp_ctx_t ctx, const bipp_nufft_options* opt, size_t nPixel,
+                                             const float* lmn, size_t ldlmn, size_t nImages, size_t nBaselines,
+                                             bipp_nufft_t* plan);
+/* Append one sample: uvw nBaselines x 3 already scaled by 2 pi / wl (as the reference's
+ * add, src/nufft_interface.hpp:16), values nBaselines x nImages complex. */
+BIPP_B200_EXPORT BippError bipp_nufft_add_s(bipp_nufft_t plan, const float* uvw, size_t lduvw, const void* values,
+                                            size_t ldvalues);
+BIPP_B200_EXPORT BippError bipp_nufft_add_d(bipp_nufft_t plan, const double* uvw, size_t lduvw,
+                                            const void* values, size_t ldvalues);
+/* Transform what was collected and return image imgIdx (nPixel floats, accumulated real
+ * part); src/nufft_interface.hpp:18. */
+BIPP_B200_EXPORT BippError bipp_nufft_get_image(bipp_nufft_t plan, size_t imgIdx, float* image);
+BIPP_B200_EXPORT BippError bipp_nufft_destroy(bipp_nufft_t plan);
+
+/* ---- image synthesis over a dataset -------------------------------------------------------- */
+
+/* Dataset accessors (include/bipp/dataset.hpp:14-41), called on the host. */
+typedef struct {
+  void* user;
+  size_t (*num_samples)(void* user);
+  size_t (*num_antenna)(void* user);
+  size_t (*num_beam)(void* user);
+  void (*eig_vec)(void* user, size_t index, void* v, size_t ldv);      /* complex float */
+  void (*eig_val)(void* user, size_t index, float* d);
+  void (*uvw)(void* user, size_t index, float* uvw, size_t lduvw);     /* metres */
+  float (*wl)(void* user, size_t index);
+  float (*scale)(void* user, size_t index);
+} bipp_dataset_callbacks;
+
+/* image_synthesis (include/bipp/image_synthesis.hpp:160-163) for nImages selections that
+ * share the same nSamples sample ids. sampleIds: [nImages][nSamples]; eigvals:
+ * [nImages][nSamples] pointers to nBeam scaled eigenvalues; images: [nImages][nPixel]
+ * output (written, not accumulated). Validation and normalisation follow
+ * src/image_synthesis.cpp:36-69, 152-163. */
+BIPP_B200_EXPORT BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt,
+                                                const bipp_dataset_callbacks* dataset, size_t nImages,
+                                                size_t nSamples, const size_t* sampleIds,
+                                                const float* const* eigvals, size_t nPixel, const float* lmn,
+                                                size_t ldlmn, float* images);
+
+/* ---- batched pipeline: S, positions -> eigensolve -> levels -> VV -> NUFFT images ----- */
+
+typedef struct {
+  size_t nAntenna;        /* antennas per step (W = I) */
+  size_t nLevels;         /* energy levels */
+  const double* intervals;/* [nLevels][2] (lo, hi) eigenvalue intervals */
+  int filter;             /* 0 lsq, 1 std, 2 sqrt, 3 inv, 4 inv_sqrt (python/bipp/filter.py) */
+  double tolerance;       /* NUFFT tolerance */
+  size_t gridA, gridB;    /* pixel lattice extents (a slow, b fast); nPixel = gridA * gridB */
+  double lattice[6];      /* l0, m0, A_l, B_l, A_m, B_m: l = l0 + a A_l + b B_l, m = m0 + a A_m + b B_m */
+  const double* pixelN;   /* [nPixel] n coordinate of each pixel (FP64) */
+  const double* uvwBasis; /* [9] column-major 3x3 (columns U, V, W in the position frame) */
+  size_t chunkSteps;      /* steps per eigensolver launch sequence (0 = 256) */
+  size_t maxSteps;        /* maximum steps per process() call */
+  int mode;               /* 0 batched (one NUFFT per call), 1 plain (one NUFFT per step and level) */
+} bipp_pipeline_config;
+
+BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg,
+                                                bipp_pipeline_t* pipeline);
+/* Process nSteps time steps: s [nSteps][nAntenna x nAntenna] complex float (lower triangle
+ * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. onDevice != 0: the
+ * three pointers are device pointers, else host pointers (copied in by the call). The
+ * steps' contributions are accumulated into the images. */
+BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s,
+                                                 const double* xyz, const double* wl, int onDevice);
+/* Images [nLevels][nPixel] (normalised by the number of processed steps if normalize),
+ * to host (onDevice == 0) or device memory. */
+BIPP_B200_EXPORT BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize, int onDevice);
+BIPP_B200_EXPORT BippError bipp_pipeline_reset(bipp_pipeline_t pl);
+/* Eigenvalues [maxSteps][nAntenna] and nBeamReduced of the last process() call (host). */
+BIPP_B200_EXPORT BippError bipp_pipeline_last_eigenvalues(bipp_pipeline_t pl, double* d, int* nReduced);
+/* Accumulated device time (ms) per stage since the last reset: [0] eigensolver,
+ * [1] virtual visibilities, [2] NUFFT point preparation and sort, [3] spreading, [4] FFT,
+ * [5] w-sum and finalisation. Only filled when timing is enabled. */
+BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms);
+BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,146 @@
+"""Generate the golden fixtures of tests/golden/ by running the reference's own CPU code.
+
+Run in a container where the reference tree and oracle/_ref/libbipp_ref.so exist:
+
+    make -C oracle REF=/root/reference && python tests/golden/make_golden.py /root/reference
+
+Outputs (compressed .npz, a few hundred KB in total):
+  lofar.npz      inputs of the reference's test data tests/data/lofar_input.json (2 samples,
+                 55 antennas, beamformed W) and the outputs of the reference's
+                 eigh_gram<float/double> (src/eigensolver.cpp:129-225) and virtual_vis
+                 (src/host/virtual_vis.cpp:19-73) for the two intervals of that test
+                 (tests/test_nufft_synthesis_lofar.cpp:112-124).
+  synth_eig.npz  seeded synthetic steps (60 antennas, one with flagged antennas), reference
+                 eigh_gram / eigh outputs in both precisions, virtual_vis per level.
+  nuft.npz       reference nuft_sum<double/float> (src/host/kernels/nuft_sum.cpp:9-31) on a
+                 seeded small problem.
+  partition.npz  reference DomainPartition::grid (src/host/domain_partition.hpp:35-101) on the
+                 seeded distributions of tests/test_domain_partition.cpp:102-131 (numpy RNG).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref  # noqa: E402
+from bipp_b200 import simulate as sim  # noqa: E402
+
+
+def lofar(refdir: str):
+    d = json.load(open(os.path.join(refdir, "tests", "data", "lofar_input.json")))
+    out = {"wl": d["wl"], "n_eig": d["n_eig_int"], "intervals": np.array(d["intervals_int"])}
+    xyzs, ss, ws, uvws = [], [], [], []
+    for it in d["data"]:
+        xyzs.append(np.array(it["xyz"]).T)
+        ss.append((np.array(it["s_real"]) + 1j * np.array(it["s_imag"])).T)
+        ws.append((np.array(it["w_real"]) + 1j * np.array(it["w_imag"])).T)
+        # the test rescales uvw back by wl / 2 pi (tests/test_nufft_synthesis_lofar.cpp:144-150)
+        uvws.append(np.array(it["uvw"]).T * (d["wl"] / (2 * np.pi)))
+    out["xyz"] = np.array(xyzs)
+    out["s"] = np.array(ss)
+    out["w"] = np.array(ws)
+    out["uvw"] = np.array(uvws, dtype=np.float32)
+    for prec, dt in (("f32", np.float32), ("f64", np.float64)):
+        vs, ds, nrs, scs, vvs = [], [], [], [], []
+        for k in range(len(ss)):
+            v, dd, nr, sc = ref.eigh_gram(d["wl"], ss[k], ws[k], xyzs[k], dtype=dt)
+            vs.append(v)
+            ds.append(dd)
+            nrs.append(nr)
+            scs.append(sc)
+            lv = []
+            for lo, hi in d["intervals_int"]:
+                dl = dd.copy()
+                n_eig = d["n_eig_int"]
+                dl[:n_eig] *= (dl[:n_eig] >= lo) & (dl[:n_eig] <= hi)
+                dl[n_eig:] = 0
+                lv.append(ref.virtual_vis(sc, dl, v, dtype=dt))
+            vvs.append(lv)
+        out[f"v_{prec}"] = np.array(vs)
+        out[f"d_{prec}"] = np.array(ds)
+        out[f"nred_{prec}"] = np.array(nrs)
+        out[f"scale_{prec}"] = np.array(scs)
+        out[f"vv_{prec}"] = np.array(vvs)
+    np.savez_compressed(os.path.join(HERE, "lofar.npz"), **out)
+
+
+def synth_eig():
+    cfg = sim.config_c1(n_steps=3)
+    obs = sim.observation(cfg)
+    masks = np.ones((3, cfg.n_antenna), dtype=bool)
+    masks[1, [3, 17, 40, 41]] = False  # one step with flagged antennas
+    s, xyz = sim.visibilities(obs, [0, 1, 2], masks=masks)
+    s = s.numpy()
+    xyz = xyz.numpy()
+    n = cfg.n_antenna
+    w = np.eye(n)
+    out = {"wl": cfg.wl, "s": s, "xyz": xyz}
+    intervals = np.array([[0.0, 50.0], [50.0, np.finfo(np.float32).max]])
+    out["intervals"] = intervals
+    for prec, dt in (("f32", np.float32), ("f64", np.float64)):
+        res = {k: [] for k in ("v", "d", "nred", "scale", "vv", "sv", "sd", "snred", "sscale")}
+        for k in range(3):
+            v, dd, nr, sc = ref.eigh_gram(cfg.wl, s[k], w, xyz[k], dtype=dt)
+            res["v"].append(v)
+            res["d"].append(dd)
+            res["nred"].append(nr)
+            res["scale"].append(sc)
+            res["vv"].append([ref.virtual_vis(sc, dd * ((dd >= lo) & (dd <= hi)), v, dtype=dt) for lo, hi in intervals])
+            v2, d2, nr2, sc2 = ref.eigh(cfg.wl, s[k], w, dtype=dt)
+            res["sv"].append(v2)
+            res["sd"].append(d2)
+            res["snred"].append(nr2)
+            res["sscale"].append(sc2)
+        for key, val in res.items():
+            out[f"{key}_{prec}"] = np.array(val)
+    np.savez_compressed(os.path.join(HERE, "synth_eig.npz"), **out)
+
+
+def nuft():
+    rng = np.random.default_rng(7)
+    m, p = 500, 300
+    vals = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    u, v, w = rng.uniform(-1, 1, (3, m)) * np.array([[3000.0], [3000.0], [200.0]])
+    x, y = rng.uniform(-0.15, 0.15, (2, p))
+    z = np.sqrt(1 - x ** 2 - y ** 2)
+    alpha = 2 * np.pi / 2.0
+    out64 = ref.nuft_sum(alpha, vals, u, v, w, x, y, z, dtype=np.float64)
+    out32 = ref.nuft_sum(alpha, vals, u, v, w, x, y, z, dtype=np.float32)
+    np.savez_compressed(os.path.join(HERE, "nuft.npz"), alpha=alpha, vals=vals, u=u, v=v, w=w, x=x, y=y, z=z,
+                        out64=out64, out32=out32)
+
+
+def partition():
+    out = {}
+    rng = np.random.default_rng(42)
+    for n in (1, 100, 4000):
+        x = rng.uniform(-5.0, 10.0, n)
+        y = rng.uniform(2.0, 20.0, n)
+        z = rng.uniform(100.0, 5000.0, n)
+        for prec, dt in (("f32", np.float32), ("f64", np.float64)):
+            pm, gb, gs = ref.partition_grid([2, 3, 4], x.astype(dt), y.astype(dt), z.astype(dt), dtype=dt)
+            out[f"x_{n}_{prec}"] = x.astype(dt)
+            out[f"y_{n}_{prec}"] = y.astype(dt)
+            out[f"z_{n}_{prec}"] = z.astype(dt)
+            out[f"permut_{n}_{prec}"] = pm
+            out[f"begin_{n}_{prec}"] = gb
+            out[f"size_{n}_{prec}"] = gs
+    np.savez_compressed(os.path.join(HERE, "partition.npz"), **out)
+
+
+if __name__ == "__main__":
+    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    lofar(refdir)
+    synth_eig()
+    nuft()
+    partition()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,65 @@
+"""CPU: the C-ABI library loads, exports every entry point declared in
+include/bipp_b200.h, and fails loudly (no CPU fallback) without a GPU."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "bipp_b200.h")).read()
+    return sorted(set(re.findall(r"BIPP_B200_EXPORT\s+[\w\s\*]+?\b(bipp_\w+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for n in ("bipp_eigh_gram_s", "bipp_eigh_gram_d", "bipp_nufft_add_s", "bipp_nufft_get_image",
+              "bipp_nuft_sum_s", "bipp_image_synthesis", "bipp_pipeline_process", "bipp_domain_partition_grid_s"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from bipp_b200 import _lib
+
+    lib = _lib.load()
+    for n in _declared():
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, n
+
+
+def test_library_is_sm100a_and_in_tree():
+    from bipp_b200 import _lib
+
+    assert os.path.dirname(_lib.LIB_PATH) == os.path.join(ROOT, "bipp_b200")
+    assert os.path.getsize(_lib.LIB_PATH) > 100_000
+
+
+def test_no_cpu_processing_unit():
+    import bipp_b200 as bipp
+
+    with pytest.raises(bipp.BippError):
+        bipp.Context("CPU")
+
+
+def test_context_without_gpu_raises_gpu_support_error():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import bipp_b200 as bipp
+
+    with pytest.raises(bipp.GPUError):
+        bipp.Context("GPU")
+
+
+def test_error_message_plumbing():
+    from bipp_b200 import _lib
+
+    lib = _lib.load()
+    h = C.c_void_p()
+    rc = lib.bipp_ctx_create(1, C.byref(h))  # CPU rejected
+    assert rc == 3
+    assert b"CPU" in lib.bipp_last_error()

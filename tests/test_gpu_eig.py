@@ -1,0 +1,187 @@
+"""GPU parity of the eigensolver entry points against the reference's own outputs
+(golden fixtures from the compiled reference) and the FP64 oracle.
+
+Tolerances: FP64 entry points agree with the reference's zhegv to 1e-10 relative;
+FP32 entry points agree with the FP64 reference to 1e-5 relative on eigenvalues
+(normwise, max|d - d_ref| / max|d_ref|) and 1e-4 on V diag(d) V^H."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import bluebild as bb
+
+pytestmark = pytest.mark.gpu
+
+
+def _prod(v, d):
+    v = v.astype(np.complex128)
+    return (v * d.astype(np.float64)) @ v.conj().T
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_lofar_eigh_gram_general_w(ctx, prec):
+    import bipp_b200 as bipp
+
+    g = golden("lofar.npz")
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = bipp.eigh_gram_full(dt(g["wl"]), g["s"][k].astype(ct), g["w"][k].astype(ct),
+                                           g["xyz"][k].astype(dt), ctx=ctx)
+        assert nr == int(g[f"nred_{prec}"][k])
+        assert abs(sc - float(g[f"scale_{prec}"][k])) <= 1e-6 * sc
+        dref = g["d_f64"][k]
+        tol_d, tol_p = (1e-10, 1e-9) if prec == "f64" else (1e-5, 1e-4)
+        assert _rel(d, dref) <= tol_d
+        assert np.all(d[nr:] == 0)
+        assert _rel(_prod(v, d), _prod(g["v_f64"][k], dref)) <= tol_p
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_synthetic_eigh_gram_with_flagging(ctx, prec):
+    import bipp_b200 as bipp
+
+    g = golden("synth_eig.npz")
+    n = g["s"].shape[1]
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = bipp.eigh_gram_full(dt(g["wl"]), g["s"][k].astype(ct), np.eye(n, dtype=ct),
+                                           g["xyz"][k].astype(dt), ctx=ctx)
+        assert nr == int(g[f"nred_{prec}"][k])
+        assert abs(sc - float(g[f"scale_{prec}"][k])) <= 1e-6 * sc
+        tol_d, tol_p = (1e-10, 1e-9) if prec == "f64" else (1e-5, 1e-4)
+        assert _rel(d, g["d_f64"][k]) <= tol_d
+        assert _rel(_prod(v, d), _prod(g["v_f64"][k], g["d_f64"][k])) <= tol_p
+        # flagged antennas give zero rows of v
+        if nr < n:
+            flagged = np.abs(g["s"][k]).sum(0) == 0
+            assert np.all(v[flagged] == 0)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_synthetic_eigh_standard(ctx, prec):
+    import bipp_b200 as bipp
+
+    g = golden("synth_eig.npz")
+    n = g["s"].shape[1]
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = bipp.eigh(dt(g["wl"]), g["s"][k].astype(ct), np.eye(n, dtype=ct), ctx=ctx, full=True)
+        assert nr == int(g[f"snred_{prec}"][k])
+        tol_d, tol_p = (1e-10, 1e-9) if prec == "f64" else (1e-5, 1e-4)
+        assert _rel(d, g["sd_f64"][k]) <= tol_d
+        assert _rel(_prod(v, d), _prod(g["sv_f64"][k], g["sd_f64"][k])) <= tol_p
+
+
+def test_eigenvector_g_orthonormality(ctx):
+    import bipp_b200 as bipp
+
+    g = golden("synth_eig.npz")
+    n = g["s"].shape[1]
+    s, xyz = g["s"][0], g["xyz"][0]
+    v, d, nr, sc = bipp.eigh_gram_full(float(g["wl"]), s, np.eye(n), xyz, ctx=ctx)
+    G = bb.gram_matrix(np.eye(n), xyz, float(g["wl"]))
+    x = v[:, :nr]
+    assert np.abs(x.conj().T @ G @ x - np.eye(nr)).max() < 1e-9
+    assert np.abs(s @ x - G @ x * d[:nr]).max() < 1e-9 * np.abs(s).max()
+
+
+@pytest.mark.parametrize("n", [64, 200, 512])
+def test_larger_sizes_against_fp64_oracle(ctx, n):
+    """FP32 GPU eigensolve at N up to 512 (the 512-antenna workload size) against scipy
+    FP64, with random flagging."""
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    cfg = sim.config_c2(n_antenna=n, n_steps=2, n_src=min(200, n // 2))
+    obs = sim.observation(cfg)
+    masks = np.ones((2, n), dtype=bool)
+    rng = np.random.default_rng(n)
+    masks[1, rng.choice(n, size=n // 5, replace=False)] = False
+    s, xyz = sim.visibilities(obs, [0, 1], masks=masks)
+    s, xyz = s.numpy(), xyz.numpy()
+    for k in range(2):
+        v, d, nr, sc = bipp.eigh_gram_full(np.float32(cfg.wl), s[k].astype(np.complex64), np.eye(n, dtype=np.complex64),
+                                           xyz[k].astype(np.float32), ctx=ctx)
+        vo, do, nro, sco = bb.eigh_gram(cfg.wl, s[k].astype(np.complex64).astype(np.complex128), np.eye(n),
+                                        xyz[k].astype(np.float32).astype(np.float64))
+        assert nr == nro
+        assert _rel(d, do) <= 1e-5
+        assert _rel(_prod(v, d), _prod(vo, do)) <= 1e-4
+
+
+def test_batched_eigh_gram_matches_single(ctx):
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    cfg = sim.config_c2(n_antenna=96, n_steps=5, n_src=40, keep=(70, 96))
+    obs = sim.observation(cfg)
+    masks = sim.keep_masks(cfg)
+    s, xyz = sim.visibilities(obs, list(range(5)), masks=masks)
+    s, xyz = s.numpy(), xyz.numpy()
+    wl = np.full(5, cfg.wl, dtype=np.float32)
+    v, d, nred, scale = bipp.eigh_gram_batched(wl, s, xyz, ctx=ctx)
+    for k in range(5):
+        vs, ds, nrs, scs = bipp.eigh_gram_full(np.float32(cfg.wl), s[k], np.eye(96, dtype=np.complex64),
+                                               xyz[k].astype(np.float32), ctx=ctx)
+        assert nred[k] == nrs == masks[k].sum()
+        assert abs(scale[k] - scs) <= 1e-7 * scs
+        assert _rel(d[k], ds) <= 1e-6
+        assert _rel(_prod(v[k], d[k]), _prod(vs, ds)) <= 1e-5
+
+
+def test_all_flagged_step(ctx):
+    import bipp_b200 as bipp
+
+    n = 16
+    v, d, nr, sc = bipp.eigh_gram_full(2.0, np.zeros((n, n), np.complex128), np.eye(n), np.random.rand(n, 3), ctx=ctx)
+    assert nr == 0 and sc == 0.0 and np.all(d == 0) and np.all(v == 0)
+
+
+def test_invalid_gram_raises_eigensolver_error(ctx):
+    """A non-finite antenna position makes a Cholesky pivot of G NaN: the FP64 Cholesky
+    reports it and the call raises EigensolverError, as LAPACK ?potrf/?hegv does in the
+    reference (src/host/lapack_api.hpp:133)."""
+    import bipp_b200 as bipp
+
+    n = 8
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    s = a @ a.conj().T
+    xyz = rng.uniform(0, 100, (n, 3))
+    xyz[3, 0] = np.nan
+    with pytest.raises(bipp.EigensolverError):
+        bipp.eigh_gram(2.0, s, np.eye(n), xyz, ctx=ctx)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_gram_matrix(ctx, prec):
+    import bipp_b200 as bipp
+
+    g = golden("lofar.npz")
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    G = bipp.gram_matrix(g["xyz"][0].astype(dt), g["w"][0].astype(ct), dt(g["wl"]), ctx=ctx)
+    Gr = bb.gram_matrix(g["w"][0].astype(ct), g["xyz"][0].astype(dt), float(dt(g["wl"])))
+    assert _rel(G, Gr) <= (1e-12 if prec == "f64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_virtual_vis(ctx, prec):
+    import bipp_b200 as bipp
+
+    g = golden("lofar.npz")
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    n_eig = int(g["n_eig"])
+    for k in range(2):
+        d = g[f"d_{prec}"][k]
+        for lv, (lo, hi) in enumerate(g["intervals"]):
+            dl = d.copy()
+            dl[:n_eig] *= (dl[:n_eig] >= lo) & (dl[:n_eig] <= hi)
+            dl[n_eig:] = 0
+            vv = bipp.virtual_vis(dt(g[f"scale_{prec}"][k]), dl.astype(dt), g[f"v_{prec}"][k].astype(ct), ctx=ctx)
+            ref_vv = g[f"vv_{prec}"][k][lv]
+            scale = max(np.abs(ref_vv).max(), 1e-30)
+            assert np.abs(vv - ref_vv).max() <= (1e-12 if prec == "f64" else 1e-5) * scale

@@ -1,0 +1,129 @@
+"""CPU: the numpy restatement (oracle/bluebild.py) pinned against the reference's own
+outputs (golden fixtures made by running the compiled reference sources), and against
+the compiled reference directly when it is available in this container."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import bluebild as bb
+from oracle import ref
+
+
+def _pair_product(v, d):
+    return (v * d) @ v.conj().T
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_lofar_eigh_gram(prec):
+    g = golden("lofar.npz")
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = bb.eigh_gram(float(g["wl"]), g["s"][k], g["w"][k], g["xyz"][k])
+        assert nr == int(g[f"nred_{prec}"][k]) == 54
+        assert abs(sc - float(g[f"scale_{prec}"][k])) <= 1e-6 * sc
+        dref = g[f"d_{prec}"][k]
+        tol = 1e-12 if prec == "f64" else 2e-5
+        assert np.abs(d - dref).max() <= tol * np.abs(dref).max()
+        p = _pair_product(v, d)
+        pref = _pair_product(g[f"v_{prec}"][k].astype(np.complex128), dref.astype(np.float64))
+        assert np.abs(p - pref).max() <= (1e-11 if prec == "f64" else 1e-4) * np.abs(pref).max()
+
+
+def test_lofar_virtual_vis():
+    g = golden("lofar.npz")
+    for k in range(g["s"].shape[0]):
+        d = g["d_f64"][k]
+        n_eig = int(g["n_eig"])
+        for lv, (lo, hi) in enumerate(g["intervals"]):
+            dl = d.copy()
+            dl[:n_eig] *= (dl[:n_eig] >= lo) & (dl[:n_eig] <= hi)
+            dl[n_eig:] = 0
+            vv = bb.virtual_vis(float(g["scale_f64"][k]), dl, g["v_f64"][k])
+            ref_vv = g["vv_f64"][k][lv]
+            assert np.abs(vv - ref_vv).max() <= 1e-12 * max(np.abs(ref_vv).max(), 1e-300)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_synthetic_eigh_and_flagging(prec):
+    g = golden("synth_eig.npz")
+    n = g["s"].shape[1]
+    for k in range(g["s"].shape[0]):
+        dt = np.float64 if prec == "f64" else np.float32
+        v, d, nr, sc = bb.eigh_gram(float(g["wl"]), g["s"][k], np.eye(n), g["xyz"][k], dtype=dt)
+        assert nr == int(g[f"nred_{prec}"][k])
+        assert abs(sc - float(g[f"scale_{prec}"][k])) <= 1e-6 * sc
+        dref = g[f"d_{prec}"][k]
+        tol = 1e-12 if prec == "f64" else 2e-5
+        assert np.abs(d - dref).max() <= tol * np.abs(dref).max()
+        v2, d2, nr2, sc2 = bb.eigh(float(g["wl"]), g["s"][k], np.eye(n), dtype=dt)
+        assert nr2 == int(g[f"snred_{prec}"][k])
+        assert np.abs(d2 - g[f"sd_{prec}"][k]).max() <= tol * np.abs(g[f"sd_{prec}"][k]).max()
+    # step 1 has four flagged antennas
+    assert int(g["nred_f64"][1]) == n - 4
+
+
+def test_nuft_sum_oracle():
+    g = golden("nuft.npz")
+    out = bb.nuft_sum(float(g["alpha"]), g["vals"], g["u"], g["v"], g["w"], g["x"], g["y"], g["z"])
+    assert np.abs(out - g["out64"]).max() <= 1e-10 * np.abs(g["out64"]).max()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("n", [100, 4000])
+def test_partition_oracle(n, prec):
+    g = golden("partition.npz")
+    dt = np.float32 if prec == "f32" else np.float64
+    pm, gb, gs = bb.partition_grid([2, 3, 4], g[f"x_{n}_{prec}"], g[f"y_{n}_{prec}"], g[f"z_{n}_{prec}"], dtype=dt)
+    assert (pm == g[f"permut_{n}_{prec}"]).all()
+    assert (gb == g[f"begin_{n}_{prec}"]).all()
+    assert (gs == g[f"size_{n}_{prec}"]).all()
+
+
+def test_partition_invariants():
+    """The reference's DomainPartition test invariants (tests/test_domain_partition.cpp:24-94)."""
+    rng = np.random.default_rng(3)
+    for n in (1, 100, 4000):
+        x, y, z = rng.uniform(-5, 10, n), rng.uniform(2, 20, n), rng.uniform(100, 5000, n)
+        pm, gb, gs = bb.partition_grid([2, 3, 4], x, y, z)
+        cover = np.zeros(n, bool)
+        for b, s in zip(gb, gs):
+            cover[int(b):int(b + s)] = True
+        assert cover.all()
+        assert sorted(pm.tolist()) == list(range(n))
+        for c, dims in ((x, 2), (y, 3), (z, 4)):
+            spacing = (c.max() - c.min()) / dims
+            srt = np.empty(n)
+            srt[pm.astype(np.int64)] = c
+            for b, s in zip(gb, gs):
+                if s:
+                    seg = srt[int(b):int(b + s)]
+                    assert seg.max() - seg.min() <= spacing + 1e-12
+
+
+def test_energy_levels_and_filters():
+    d = np.array([-1.0, 0.0, 0.5, 2.0, 9.0])
+    assert np.allclose(bb.level_eigenvalues(d, 0.0, 1.0), [0, 0, 0.5, 0, 0])
+    assert np.allclose(bb.apply_filter("std", d), np.sign(d))
+    assert np.allclose(bb.apply_filter("sqrt", d), np.sign(d) * np.sqrt(np.abs(d)))
+    inv = bb.apply_filter("inv", d)
+    assert inv[1] == 0 and np.isclose(inv[3], 0.5)
+    iv = bb.centroid_to_intervals(np.array([10.0, 1.0, 0.1]), 0.0, 100.0)
+    assert np.allclose(iv[:, 0], [5.5, 0.55, 0.0]) and np.allclose(iv[:, 1], [100.0, 5.5, 0.55])
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+def test_restatement_vs_compiled_reference_random():
+    rng = np.random.default_rng(11)
+    n = 24
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    s = a @ a.conj().T / n
+    np.fill_diagonal(s, 0)
+    s[:, 5] = 0
+    s[5, :] = 0
+    xyz = rng.uniform(-50, 50, (n, 3))
+    w = np.eye(n)
+    v_r, d_r, nr_r, sc_r = ref.eigh_gram(2.0, s, w, xyz)
+    v_o, d_o, nr_o, sc_o = bb.eigh_gram(2.0, s, w, xyz)
+    assert nr_r == nr_o == n - 1 and sc_r == sc_o
+    assert np.abs(d_r - d_o).max() <= 1e-12 * np.abs(d_r).max()
+    g_r = ref.gram_matrix(w, xyz, 2.0)
+    assert np.abs(g_r - bb.gram_matrix(w, xyz, 2.0)).max() <= 1e-14
