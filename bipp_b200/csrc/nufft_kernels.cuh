@@ -54,7 +54,7 @@ struct PtCoord {
 };
 
 // not inlined: the count and scatter passes must compute bit-identical keys
-__device__ __noinline__ PtCoord point_coord(const NufftGeom& g, double u, double v, double w) {
+static __device__ __noinline__ PtCoord point_coord(const NufftGeom& g, double u, double v, double w) {
   const double x = u * g.Bl + v * g.Bm;
   const double y = u * g.Al + v * g.Am;
   const double gx = wrap_pi(x) / g.hx;
@@ -82,7 +82,7 @@ __device__ __forceinline__ double point_phase(const NufftGeom& g, double u, doub
   return wrap_pi(ph);
 }
 
-__device__ __noinline__ int tile_key(const NufftGeom& g, const PtCoord& c) {
+static __device__ __noinline__ int tile_key(const NufftGeom& g, const PtCoord& c) {
   int ix = c.ix0 % g.nx; if (ix < 0) ix += g.nx;
   int iy = c.iy0 % g.ny; if (iy < 0) iy += g.ny;
   const int tx = ix / kTX, ty = iy / kTY, tw = c.iw0 / kTW;
@@ -130,7 +130,7 @@ struct BaselinePoints {
   int levels;
 };
 
-__device__ __noinline__ void pair_from_linear(long long t, int n, int& r, int& s) {
+static __device__ __noinline__ void pair_from_linear(long long t, int n, int& r, int& s) {
   // t enumerates the lower triangle column by column: column s holds rows s..n-1
   // offset(s) = s n - s (s - 1) / 2
   double nn = (double)n + 0.5;
