@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Bluebild imaging throughput: time-steps/s at 512 antennas and a 1024^2 image.
+
+Workload (one bench step = one batch): 2048 time steps of a 512-antenna log-radial
+array (35 km), 380-512 antennas kept per step, 200-source sky, 4 energy levels,
+1024 x 1024 pixel lattice over 16 deg, NUFFT tolerance 1e-5; per time step: flagging,
+Gram, generalized eigensolve, level binning, virtual visibilities, NUFFT synthesis.
+Seeded synthetic inputs (the reference's datasets are not available); inputs (4.3 GB of
+visibilities per batch) are larger than L2, so no extra flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference's own CPU code (oracle/_ref, compiled from the
+reference sources) on the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-steps/s at 512 antennas, 1024^2 px (4 levels, NUFFT eps 1e-5)"
+UNIT = "time-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--time-steps", type=int, default=2048)
+    ap.add_argument("--antennas", type=int, default=512)
+    ap.add_argument("--image", type=int, default=1024)
+    ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--stages", action="store_true", help="report per-stage device times")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(cfg, rank, device):
+    """Seeded C2-shaped inputs on the GPU: S^T per step (column-major S), xyz, wl."""
+    import torch
+
+    from bipp_b200 import simulate as sim
+
+    obs = sim.observation(cfg)
+    masks = sim.keep_masks(cfg)
+    T, N = cfg.n_steps, cfg.n_antenna
+    S = torch.empty((T, N, N), dtype=torch.complex64, device=device)
+    xyz = torch.empty((T, N, 3), dtype=torch.float64, device=device)
+    chunk = 64
+    for s0 in range(0, T, chunk):
+        steps = list(range(s0, min(T, s0 + chunk)))
+        s, x = sim.visibilities(obs, steps, device=device, dtype=torch.complex64, masks=masks)
+        S[s0:s0 + len(steps)] = s.transpose(1, 2)
+        xyz[s0:s0 + len(steps)] = x
+    wl = torch.full((T,), cfg.wl, dtype=torch.float64, device=device)
+    torch.cuda.synchronize()
+    return obs, S, xyz, wl
+
+
+def lattice_of(obs, n):
+    l = obs.lmn[:, 0].reshape(n, n)
+    m = obs.lmn[:, 1].reshape(n, n)
+    return (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
+
+
+def calibrate_levels(ctx, cfg, S, xyz, n_cal=64):
+    """Energy levels: k-means (log) over positive eigenvalues of the first n_cal steps
+    (python/bipp/parameter_estimator.py:55-105), then frozen."""
+    import bipp_b200 as bipp
+    from bipp_b200.parameter_estimator import infer_intervals
+
+    n_cal = min(n_cal, cfg.n_steps)
+    s_host = S[:n_cal].transpose(1, 2).cpu().numpy()
+    x_host = xyz[:n_cal].cpu().numpy()
+    _, d, nred, _ = bipp.eigh_gram_batched(np.full(n_cal, cfg.wl, np.float32), s_host, x_host, ctx=ctx)
+    return infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d)
+
+
+def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, threads=None):
+    """The reference's CPU path (compiled reference sources) on a bounded sample:
+    eigh_gram<float> + virtual_vis<float> per level on n_eig_steps steps, and the
+    reference direct sum nuft_sum<double> over all baselines of one step for n_pix
+    pixels, extrapolated to the full image and all levels (the reference's CPU NUFFT,
+    neonufft, is not available). Returns (steps/s, cores, sample description)."""
+    from oracle import ref
+
+    from bipp_b200 import simulate as sim
+
+    threads = threads or os.cpu_count() or 1
+    ref.set_threads(threads)
+    obs = sim.observation(cfg)
+    N = cfg.n_antenna
+    w = np.eye(N, dtype=np.complex64)
+    t_eig = t_vv = 0.0
+    last = None
+    for k in range(n_eig_steps):
+        s = S[k].transpose(0, 1).cpu().numpy().T  # logical S
+        x = xyz[k].cpu().numpy().astype(np.float32)
+        t0 = time.perf_counter()
+        v, d, nr, sc = ref.eigh_gram(cfg.wl, s, w, x, dtype=np.float32)
+        t1 = time.perf_counter()
+        vvs = []
+        for lo, hi in intervals:
+            vvs.append(ref.virtual_vis(sc, d * ((d >= lo) & (d <= hi)), v, dtype=np.float32))
+        t2 = time.perf_counter()
+        t_eig += t1 - t0
+        t_vv += t2 - t1
+        last = (vvs, xyz[k].cpu().numpy())
+    t_eig /= n_eig_steps
+    t_vv /= n_eig_steps
+    vvs, x = last
+    uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / cfg.wl)
+    rng = np.random.default_rng(0)
+    pix = rng.choice(obs.lmn.shape[0], n_pix, replace=False)
+    lmn = obs.lmn[pix]
+    vals = vvs[0].reshape(-1, order="F").astype(np.complex128)
+    t0 = time.perf_counter()
+    ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], lmn[:, 0], lmn[:, 1], lmn[:, 2], threads=threads)
+    t_pix = time.perf_counter() - t0
+    t_nuft = t_pix * (obs.lmn.shape[0] / n_pix) * len(intervals)
+    per_step = t_eig + t_vv + t_nuft
+    desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} on {n_eig_steps} steps "
+            f"({t_eig:.3f}+{t_vv:.3f} s/step); nuft_sum<double> all {N * N} baselines x {n_pix} px "
+            f"({t_pix:.2f} s) extrapolated to {obs.lmn.shape[0]} px x {len(intervals)} levels "
+            f"({t_nuft:.1f} s/step); neonufft unavailable")
+    return 1.0 / per_step, threads, desc
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation on host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    from bipp_b200 import simulate as sim
+
+    cfg = sim.config_c2(n_antenna=args.antennas, image_size=args.image, n_steps=max(8, args.steps + args.warmup))
+    obs = sim.observation(cfg)
+    masks = sim.keep_masks(cfg)
+    s, x = sim.visibilities(obs, list(range(cfg.n_steps)), dtype=torch.complex64, masks=masks)
+    S = s.transpose(1, 2)
+    from bipp_b200.parameter_estimator import infer_intervals
+    from oracle import ref
+
+    ref.set_threads(os.cpu_count() or 1)
+    d_all = []
+    for k in range(2):
+        _, d, _, _ = ref.eigh_gram(cfg.wl, s[k].numpy(), np.eye(cfg.n_antenna), x[k].numpy().astype(np.float32),
+                                   dtype=np.float32)
+        d_all.append(d)
+    intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, np.concatenate(d_all))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, cores, desc = cpu_reference_sample(cfg, S[k:k + 1], x[k:k + 1], intervals, n_eig_steps=1, n_pix=1024)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded C2-shaped observation)",
+            "config": {"workload": "c2: 512 antennas log-radial 35 km, 380-512 kept/step, 200 sources, 4 levels, "
+                                   "1024^2 px over 16 deg, eps 1e-5", "time_steps_per_batch": args.time_steps},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    ctx = bipp.Context("GPU", device=local)
+    cfg = sim.config_c2(n_antenna=args.antennas, image_size=args.image, n_steps=args.time_steps, seed=2 + rank)
+    obs, S, xyz, wl = make_inputs(cfg, rank, device)
+    intervals = calibrate_levels(ctx, cfg, S, xyz)
+    n = cfg.image_size
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
+                       tolerance=cfg.eps, chunk_steps=256, max_steps=cfg.n_steps, mode=args.mode)
+    T = cfg.n_steps
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+
+    def one_step():
+        pl.process_device(T, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())
+
+    for _ in range(args.warmup):
+        one_step()
+    pl.reset()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            one_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms_t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = args.steps * T * world / (ms_max / 1000.0)
+
+    # images: one reduction of the level images over ranks per run (SUM, to rank 0)
+    img = torch.empty((cfg.n_levels, n * n), dtype=torch.float32, device=device)
+    pl.images_device(img.data_ptr(), normalize=False)
+    if world > 1:
+        dist.reduce(img, dst=0, op=dist.ReduceOp.SUM)
+
+    # per-stage breakdown (separate, untimed pass)
+    stages = None
+    if args.stages or rank == 0:
+        pl.reset()
+        pl.stage_times(True)
+        one_step()
+        st = pl.stage_times(False)
+        stages = dict(zip(["eigensolve_levels_vv", "vv", "prep_sort_scatter", "spread", "fft", "wsum"],
+                          [round(float(x), 3) for x in st]))
+
+    # end to end through the public API: pinned host inputs copied in every step,
+    # images read back every step
+    e2e = None
+    if not args.no_e2e:
+        S_h = torch.empty(S.shape, dtype=S.dtype, pin_memory=True)
+        S_h.copy_(S)
+        xyz_h = xyz.cpu().pin_memory()
+        wl_h = wl.cpu().pin_memory()
+        img_h = torch.empty((cfg.n_levels, n * n), dtype=torch.float32, pin_memory=True)
+        del S
+        torch.cuda.empty_cache()
+        pl.reset()
+        pl.process_host_ptr(T, S_h.data_ptr(), xyz_h.data_ptr(), wl_h.data_ptr())  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            pl.reset()
+            pl.process_host_ptr(T, S_h.data_ptr(), xyz_h.data_ptr(), wl_h.data_ptr())
+            pl.images_ptr(img_h.data_ptr(), normalize=True, on_device=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = torch.tensor([e0.elapsed_time(e1)], device=device, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(ems, op=dist.ReduceOp.MAX)
+        e2e = {"value": args.e2e_steps * T * world / (float(ems.item()) / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(S_h.numel() * 8 + xyz_h.numel() * 8 + wl_h.numel() * 8),
+               "d2h_bytes_per_step": int(img_h.numel() * 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            Sc = S_h if not args.no_e2e else S  # noqa: F821
+            v, cores, desc = cpu_reference_sample(cfg, Sc, xyz, intervals)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded C2-shaped observation, generated on the GPU)",
+                "config": {"workload": "c2: 512 antennas log-radial 35 km, 380-512 kept/step, 200 sources, "
+                                       "4 levels, 1024^2 px over 16 deg, eps 1e-5",
+                           "time_steps_per_batch": T, "mode": args.mode, "parallelism": f"dp{world} (steps)",
+                           "l2": "inputs (4.3 GB/batch) larger than L2; no flush"},
+                "clocks": clk.summary(), "gpu_launches": None, "stages_ms": stages, "e2e": e2e,
+                "cpu_baseline": cpu, "roofline": None}
+        print(json.dumps(line))
+    pl.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

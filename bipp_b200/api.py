@@ -537,6 +537,16 @@ class Pipeline:
         check(self.ctx._lib.bipp_pipeline_process(self.handle, int(n_steps), C.c_void_p(s_ptr), C.c_void_p(xyz_ptr),
                                                   C.c_void_p(wl_ptr), 1))
 
+    def process_host_ptr(self, n_steps, s_ptr, xyz_ptr, wl_ptr):
+        """process() on host pointers already in the library layout (s column-major per
+        step); the call copies them to the device (pinned memory gives full bandwidth)."""
+        check(self.ctx._lib.bipp_pipeline_process(self.handle, int(n_steps), C.c_void_p(s_ptr), C.c_void_p(xyz_ptr),
+                                                  C.c_void_p(wl_ptr), 0))
+
+    def images_ptr(self, ptr, normalize=True, on_device=False):
+        check(self.ctx._lib.bipp_pipeline_images(self.handle, C.c_void_p(ptr), 1 if normalize else 0,
+                                                 1 if on_device else 0))
+
     def images(self, normalize=True):
         out = np.zeros((self.n_levels, self.grid[0] * self.grid[1]), dtype=np.float32)
         check(self.ctx._lib.bipp_pipeline_images(self.handle, _ptr(out), 1 if normalize else 0, 0))

@@ -84,10 +84,11 @@ inline void d2h(bipp_ctx_s* c, void* dst, const void* src, size_t bytes) {
 }
 inline void sync(bipp_ctx_s* c) { B2_CUDA(cudaStreamSynchronize(c->stream)); }
 
-// Allow a kernel to use more than 48 KB of dynamic shared memory.
+// Allow a kernel to use large dynamic shared memory (dynamic + static above 48 KB needs
+// the opt-in, so it is requested for anything above 32 KB of dynamic memory).
 template <typename K>
 inline void smem_optin(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) B2_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  if (bytes > 32 * 1024) B2_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 // Run an API body, translating exceptions into BippError codes.

@@ -340,6 +340,12 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
         store_conv<C>(Ob + (i0 + r) + (long long)(i0 + c) * Nmax, v);
       }
     }
+    // strictly upper blocks J > I are zero (the GEMMs read whole tiles of Linv)
+    for (long long e = tid; e < (long long)ib * (n - i0 - ib); e += blockDim.x) {
+      const int r = (int)(e % ib), c = i0 + ib + (int)(e / ib);
+      Wb[(i0 + r) + (long long)c * Nmax] = make_double2(0, 0);
+      store_conv<C>(Ob + (i0 + r) + (long long)c * Nmax, make_double2(0, 0));
+    }
     // off-diagonal blocks J < I
     for (int J = 0; J < I; ++J) {
       const int j0 = J * NB;
@@ -428,8 +434,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   // triangular limits
   if (g.triA == 1) ke = min(ke, i0 + kGemmBM);
   if (g.triA == 2) kb = max(kb, i0);
-  if (g.triB == 1) kb = max(kb, j0);
-  if (g.triB == 2) ke = min(ke, j0 + kGemmBN);
+  if (g.triB == 1) ke = min(ke, j0 + kGemmBN);
+  if (g.triB == 2) kb = max(kb, j0);
   const C* A = g.A + b * g.strideA;
   const C* B = g.B + b * g.strideB;
   C* Cm = g.Cm + b * g.strideC + lvl * g.strideCLevel;
