@@ -303,8 +303,11 @@ def main():
         pl.stage_times(True)
         one_step()
         st = pl.stage_times(False)
-        stages = dict(zip(["eigensolve_levels_vv", "vv", "prep_sort_scatter", "spread", "fft", "wsum"],
+        stages = dict(zip(["eigensolve", "levels_vv", "flags_sort_scatter", "spread", "fft", "wsum"],
                           [round(float(x), 3) for x in st]))
+        kt = pl.kernel_times()
+        stages["eig_kernels"] = dict(zip(["prep_gram", "cholesky_fp64", "trinv_fp64", "reduction_gemms", "hetrd",
+                                          "tridiag_fp64", "backtransform", "x_gemm"], [round(float(x), 3) for x in kt]))
 
     # end to end through the public API: pinned host inputs copied in every step,
     # images read back every step

@@ -569,6 +569,13 @@ class Pipeline:
         check(self.ctx._lib.bipp_pipeline_stage_times(self.handle, -1 if enable is None else int(enable), _ptr(ms)))
         return ms
 
+    def kernel_times(self):
+        """Eigensolver kernel times (ms): prep, cholesky, trinv, reduction GEMMs, hetrd,
+        tridiagonal eigenpairs, back-transform, Linv^H Y GEMM."""
+        ms = np.zeros(8, dtype=np.float64)
+        check(self.ctx._lib.bipp_pipeline_kernel_times(self.handle, _ptr(ms)))
+        return ms
+
     def close(self):
         if getattr(self, "handle", None):
             self.ctx._lib.bipp_pipeline_destroy(self.handle)

@@ -107,6 +107,37 @@ __global__ void pad_eigenvalues_kernel(int nBatch, int nBeam, const int* __restr
   }
 }
 
+// events between the kernels of one eigensolver sequence (only when timing is requested)
+struct SeqTimer {
+  cudaStream_t st;
+  double* out;
+  cudaEvent_t ev[kEigTimers + 1];
+  int last = -1;
+  SeqTimer(cudaStream_t s, double* o) : st(s), out(o) {
+    if (!out) return;
+    for (auto& e : ev) cudaEventCreate(&e);
+  }
+  // mark the start of stage i (closing the previous one)
+  void mark(int i) {
+    if (!out) return;
+    cudaEventRecord(ev[i], st);
+    last = i;
+  }
+  void finish(const int* order, int n) {
+    if (!out) return;
+    cudaEventRecord(ev[kEigTimers], st);
+    cudaEventSynchronize(ev[kEigTimers]);
+    for (int k = 0; k < n; ++k) {
+      const int a = order[k];
+      const int b = (k + 1 < n) ? order[k + 1] : kEigTimers;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[a], ev[b]);
+      out[a] += ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+};
+
 // ---------------------------------------------------------------------------------------
 // EigWork
 // ---------------------------------------------------------------------------------------
@@ -142,8 +173,13 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   C* T1 = w.T1.template get<C>();
   R* Z = w.Z.template get<R>();
   const int* nred = L.nred + L.batchOffset;
+  SeqTimer tm(st, L.kernelMs);
+  int order[kEigTimers];
+  int no = 0;
+  auto mark = [&](int i) { tm.mark(i); order[no++] = i; };
 
   // 1. flags (optional) + compaction (+ Gram for W = I)
+  mark(0);
   {
     const size_t smem = 2 * (size_t)Nmax * sizeof(int);
     auto k = prep_kernel<T>;
@@ -166,13 +202,16 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   }
   const int tiles = (Nmax + kGemmBM - 1) / kGemmBM;
   if (L.gram) {
+    mark(1);
     smem_optin(cholesky_kernel, kCholSmem);
     cholesky_kernel<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset);
     B2_CHECK_LAUNCH();
+    mark(2);
     smem_optin(trinv_kernel<C>, kTrinvSmem);
     trinv_kernel<C><<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax);
     B2_CHECK_LAUNCH();
     // T1 = Linv * A
+    mark(3);
     GemmArgs<C> g1{};
     g1.A = Linv; g1.strideA = n2; g1.lda = Nmax; g1.opA = 0;
     g1.B = A; g1.strideB = n2; g1.ldb = Nmax; g1.opB = 0;
@@ -190,6 +229,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     B2_CHECK_LAUNCH();
   }
   // 3. tridiagonalisation
+  mark(4);
   {
     const size_t smem = 12 * (size_t)Nmax * sizeof(C);
     auto k = hetrd_kernel<C, R>;
@@ -199,6 +239,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     B2_CHECK_LAUNCH();
   }
   // 4. tridiagonal eigenpairs (FP64); workspace aliases W64 (free after trinv)
+  mark(5);
   {
     const size_t smem = 4 * (size_t)Nmax * sizeof(double);
     auto k = tridiag_kernel<R>;
@@ -209,6 +250,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     B2_CHECK_LAUNCH();
   }
   // 5. back-transform Y = Q Z -> T1
+  mark(6);
   {
     size_t smem16 = ((size_t)Nmax * 16 + Nmax + kBtThreads) * sizeof(C);
     if (smem16 <= ctx->maxSmemOptin) {
@@ -225,6 +267,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   }
   // 6. X = Linv^H Y -> X (G storage) ; or X = Y for the standard problem
   if (L.gram) {
+    mark(7);
     GemmArgs<C> g3{};
     g3.A = Linv; g3.strideA = n2; g3.lda = Nmax; g3.opA = 1;
     g3.B = T1; g3.strideB = n2; g3.ldb = Nmax; g3.opB = 0;
@@ -233,6 +276,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);
     B2_CHECK_LAUNCH();
   }
+  tm.finish(order, no);
 }
 
 template <typename T>

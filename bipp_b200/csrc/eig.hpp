@@ -45,7 +45,12 @@ struct EigLaunch {
   double* lam = nullptr;        // [batch][Nmax]
   int doFlag = 1;
   int batchOffset = 0;
+  // optional per-kernel device time accumulation (ms): prep, cholesky, trinv, reduction
+  // GEMMs, hetrd, tridiagonal eigenpairs, back-transform, Linv^H Y GEMM
+  double* kernelMs = nullptr;
 };
+
+constexpr int kEigTimers = 8;
 
 template <typename T>
 void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w);

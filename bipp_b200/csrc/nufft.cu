@@ -184,6 +184,7 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
       g_, nTilde_.get<double>(), qz_.get<double>(), qw_.get<double>(), (int)qx.size(), decon_.get<double>());
   B2_CHECK_LAUNCH();
   acc_.alloc(ctx, (size_t)levels_ * (corrCapable_ ? 3 : 1) * P * sizeof(float2));
+  zeroAcc_.alloc(ctx, kMaxChan * sizeof(double));
   sync(ctx);
 }
 
@@ -208,6 +209,7 @@ void NufftCore::begin(double wmin, double wmax) {
   require(nkeys_ < (1ll << 31) - 2, "NUFFT grid too large");
   counts_.ensure(ctx_, (nkeys_ + 1) * sizeof(int));
   B2_CUDA(cudaMemsetAsync(counts_.get(), 0, (nkeys_ + 1) * sizeof(int), ctx_->stream));
+  B2_CUDA(cudaMemsetAsync(zeroAcc_.get(), 0, kMaxChan * sizeof(double), ctx_->stream));
 }
 
 void NufftCore::end_count(long long nPoints) {
@@ -229,13 +231,17 @@ void NufftCore::end_count(long long nPoints) {
 }
 
 template <int CH>
-static void launch_spread(const NufftGeom& g, int grid, size_t smem, cudaStream_t st, const int* offs,
-                          const PtRec* rec, const float2* vals, long long vs, int nch, int tw0, int slabTiles,
-                          float2* out) {
-  auto k = spread_tile_kernel<CH>;
+static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStream_t st, const int* offs,
+                          const PtRec* rec, const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
+                          int slabPlanes, float2* out) {
+  auto k = spread_warp_kernel<CH>;
   smem_optin(k, smem);
-  k<<<grid, kSpreadThreads, smem, st>>>(g, offs, rec, vals, vs, nch, tw0, slabTiles, out);
+  k<<<nItems, kSpreadThreads, smem, st>>>(g, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out);
 }
+
+// points per spreading part: heavier tiles are split so that no CTA serialises the
+// dense core of the uv plane (short baselines)
+constexpr int kSpreadCap = 4096;
 
 void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const long long P = num_pixels();
@@ -246,31 +252,60 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const size_t budget = std::min<size_t>(std::max<size_t>(freeB / 4, planeBytes * kTW * nch_), (size_t)8 << 30);
   int slabTiles = (int)std::max<size_t>(1, budget / (planeBytes * kTW * nch_));
   slabTiles = std::min(slabTiles, g_.ntw);
-  // balance slabs
   const int nslab = (g_.ntw + slabTiles - 1) / slabTiles;
   slabTiles = (g_.ntw + nslab - 1) / nslab;
   slabTiles_ = slabTiles;
   const int slabPlanes = slabTiles * kTW;
   grid_.ensure(ctx_, (size_t)nch_ * slabPlanes * planeBytes);
   B2_CUDA(cudaMemsetAsync(acc_.get(), 0, (size_t)nch_ * P * sizeof(float2), ctx_->stream));
-  const size_t smem = (size_t)nch_ * kTX * kTY * kTW * sizeof(float2);
+  // per-tile loads -> work items (non-empty tiles, heavy tiles split), grouped by slab
+  const int ntiles = g_.ntx * g_.nty * g_.ntw;
+  load_.ensure(ctx_, (size_t)ntiles * sizeof(int));
+  tile_load_kernel<<<std::min(4096, (ntiles + 255) / 256), 256, 0, ctx_->stream>>>(g_, offsets_.get<int>(),
+                                                                                   load_.get<int>());
+  B2_CHECK_LAUNCH();
+  std::vector<int> loads(ntiles);
+  d2h(ctx_, loads.data(), load_.get(), (size_t)ntiles * sizeof(int));
+  sync(ctx_);
+  std::vector<SpreadItem> items;
+  std::vector<int> slabBegin(nslab + 1, 0);
+  const int tilesPerPlaneSet = g_.ntx * g_.nty;
+  for (int sl = 0; sl < nslab; ++sl) {
+    slabBegin[sl] = (int)items.size();
+    const int t0 = sl * slabTiles * tilesPerPlaneSet;
+    const int t1 = std::min(ntiles, (sl + 1) * slabTiles * tilesPerPlaneSet);
+    for (int t = t0; t < t1; ++t) {
+      const int ld = loads[t];
+      if (!ld) continue;
+      const int np = (ld + kSpreadCap - 1) / kSpreadCap;
+      for (int q = 0; q < np; ++q) items.push_back(SpreadItem{t, q, np, ld});
+    }
+  }
+  slabBegin[nslab] = (int)items.size();
+  items_.ensure(ctx_, std::max<size_t>(1, items.size()) * sizeof(SpreadItem));
+  h2d(ctx_, items_.get(), items.data(), items.size() * sizeof(SpreadItem));
+  const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);
   cudaEvent_t ev[4];
   if (stageMs)
     for (auto& e : ev) B2_CUDA(cudaEventCreate(&e));
   float tSpread = 0, tFft = 0, tW = 0;
-  for (int tw0 = 0; tw0 < g_.ntw; tw0 += slabTiles) {
+  for (int sl = 0; sl < nslab; ++sl) {
+    const int tw0 = sl * slabTiles;
     const int tiles = std::min(slabTiles, g_.ntw - tw0);
-    const int gridBlocks = g_.ntx * g_.nty * tiles;
+    const int nItems = slabBegin[sl + 1] - slabBegin[sl];
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
-    if (nch_ <= 4)
-      launch_spread<4>(g_, gridBlocks, smem, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),
-                       valStride_, nch_, tw0, slabTiles, grid_.get<float2>());
-    else
-      launch_spread<kMaxChan>(g_, gridBlocks, smem, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(),
-                              vals_.get<float2>(), valStride_, nch_, tw0, slabTiles, grid_.get<float2>());
-    B2_CHECK_LAUNCH();
+    B2_CUDA(cudaMemsetAsync(grid_.get(), 0, (size_t)nch_ * slabPlanes * planeBytes, ctx_->stream));
+    if (nItems > 0) {
+      const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];
+      if (nch_ <= 4)
+        launch_spread<4>(g_, nItems, smem, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),
+                         valStride_, nch_, it, tw0, slabPlanes, grid_.get<float2>());
+      else
+        launch_spread<kMaxChan>(g_, nItems, smem, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(),
+                                vals_.get<float2>(), valStride_, nch_, it, tw0, slabPlanes, grid_.get<float2>());
+      B2_CHECK_LAUNCH();
+    }
     if (stageMs) B2_CUDA(cudaEventRecord(ev[1], ctx_->stream));
-    // planes beyond the last tile of a partial slab are unused; transform the whole slab
     cufftHandle h = plan_for(nch_ * slabPlanes);
     B2_CUFFT(cufftExecC2C(h, reinterpret_cast<cufftComplex*>(grid_.get()), reinterpret_cast<cufftComplex*>(grid_.get()),
                           CUFFT_INVERSE));
@@ -292,7 +327,8 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const int blocks = (int)std::min<long long>((P + 255) / 256, 65535);
   finalize_kernel<<<blocks, 256, 0, ctx_->stream>>>(P, levels_, acc_.get<float2>(), P, decon_.get<double>(),
                                                     nTilde_.get<double>(), g_.wc, corrTerms_ ? 1 : 0,
-                                                    dl_.get<double>(), dm_.get<double>(), su_, sv_, image, ldImage);
+                                                    dl_.get<double>(), dm_.get<double>(), su_, sv_, image, ldImage,
+                                                    zeroAcc_.get<double>());
   B2_CHECK_LAUNCH();
   if (stageMs) {
     stageMs[0] += tSpread;
@@ -302,7 +338,7 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   }
 }
 
-__global__ void f2d_kernel(const float* __restrict__ in, long long n, double* __restrict__ out) {
+static __global__ void f2d_kernel(const float* __restrict__ in, long long n, double* __restrict__ out) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = (double)in[i];
 }
@@ -428,7 +464,8 @@ static void nufft_transform_lattice(bipp_nufft_s* p, long long n, long long ld) 
   p->core.end_count(n);
   baseline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(g, bp, p->core.cursor(), p->core.records(), p->core.values(),
                                                        p->core.value_stride(), p->core.sincos64() ? 1 : 0,
-                                                       p->core.corr_terms() ? 1 : 0, p->core.su(), p->core.sv());
+                                                       p->core.corr_terms() ? 1 : 0, p->core.su(), p->core.sv(),
+                                                       p->core.zero_acc());
   B2_CHECK_LAUNCH();
   p->core.execute(p->images.get<float>(), (long long)p->nPixel);
 }

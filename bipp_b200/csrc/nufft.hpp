@@ -46,6 +46,8 @@ public:
   PtRec* records() { return rec_.get<PtRec>(); }
   float2* values() { return vals_.get<float2>(); }
   long long value_stride() const { return valStride_; }
+  // per-channel accumulator of zero-baseline values (added to every pixel)
+  double* zero_acc() { return zeroAcc_.get<double>(); }
   // spread/FFT/w-sum over all slabs and accumulate Re(...) into image[ch][P] (ld P)
   void execute(float* image, long long ldImage, double* stageMs = nullptr);
 
@@ -67,7 +69,7 @@ private:
   double su_ = 1, sv_ = 1;
   long long nkeys_ = 0, valStride_ = 0;
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
-  DevBuf qz_, qw_;
+  DevBuf qz_, qw_, zeroAcc_, load_, items_;
   std::map<int, cufftHandle> plans_;
   int slabTiles_ = 1;
   cufftHandle plan_for(int batch);

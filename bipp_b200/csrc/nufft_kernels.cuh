@@ -162,6 +162,7 @@ static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long
     const int n = P.nred[st];
     int r, s;
     pair_from_linear(t - chunkPairOffset[st], n, r, s);
+    if (r == s) continue;  // zero baseline: added analytically (Re of the trace of VV)
     const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
     const double* U = P.antUVW + (long long)st * P.nAnt * 3;
     const double sc = P.uvwScale[st];
@@ -188,6 +189,7 @@ static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, lo
     const int n = P.nred[st];
     int r, s;
     pair_from_linear(t - chunkPairOffset[st], n, r, s);
+    if (r == s) continue;  // zero baseline: added analytically (Re of the trace of VV)
     const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
     const double* U = P.antUVW + (long long)st * P.nAnt * 3;
     const double sc = P.uvwScale[st];
@@ -216,6 +218,21 @@ static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, lo
   }
 }
 
+// zeroAcc[l] += sum_steps sum_r Re VV_l[r, r] (the r == s points skipped by the scatter)
+static __global__ void vv_trace_kernel(int nSteps, int levels, const int* __restrict__ nred, const float2* __restrict__ vv,
+                                       long long vvStepStride, long long vvLevelStride, int Nmax,
+                                       double* __restrict__ zeroAcc) {
+  __shared__ double red[32];
+  const int b = blockIdx.x / levels, l = blockIdx.x % levels;
+  if (b >= nSteps) return;
+  const int n = nred[b];
+  const float2* m = vv + (long long)b * vvStepStride + (long long)l * vvLevelStride;
+  double acc = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) acc += (double)m[r + (long long)r * Nmax].x;
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) atomicAdd(zeroAcc + l, acc);
+}
+
 // collect/get form: per-baseline uvw (float, metres) and values; optional first-order
 // lattice-residual channels (values * u/su, values * v/sv)
 static __global__ void baseline_count_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ counts) {
@@ -223,17 +240,24 @@ static __global__ void baseline_count_kernel(NufftGeom g, BaselinePoints P, int*
     const double u = (double)P.uvw[t] * P.uvwScale;
     const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
     const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    if (u == 0.0 && v == 0.0 && w == 0.0) continue;  // zero baseline: added analytically
     atomicAdd(counts + tile_key(g, point_coord(g, u, v, w)), 1);
   }
 }
 
 static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ cursor,
                                         PtRec* __restrict__ rec, float2* __restrict__ vals, long long valStride,
-                                        int sincos64, int corrTerms, double su, double sv) {
+                                        int sincos64, int corrTerms, double su, double sv,
+                                        double* __restrict__ zeroAcc) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
     const double u = (double)P.uvw[t] * P.uvwScale;
     const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
     const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    if (u == 0.0 && v == 0.0 && w == 0.0) {
+      // exp(i 0) = 1 at every pixel: Re(value) adds to the whole image
+      for (int l = 0; l < P.levels; ++l) atomicAdd(zeroAcc + l, (double)P.values[(long long)l * P.ldv + t].x);
+      continue;
+    }
     const PtCoord c = point_coord(g, u, v, w);
     const int pos = atomicAdd(cursor + tile_key(g, c), 1);
     if (pos < 0 || pos >= valStride) continue;  // keys of both passes agree; never taken
@@ -348,29 +372,30 @@ static __global__ void scan_add_kernel(int* __restrict__ out, long long n, const
 }
 
 // ---------------------------------------------------------------------------------------
-// spreading: one CTA per output tile of the current w-slab
+// spreading: one CTA per work item (an output tile of the current w-slab, or one part of
+// a heavily loaded tile); one warp per point, lanes over the W^3 support cells, shared-
+// memory accumulation with a bank swizzle, one write of the tile (global atomics only for
+// tiles split into several parts).
 // ---------------------------------------------------------------------------------------
 constexpr int kSpreadThreads = 256;
+constexpr int kTileCells = kTX * kTY * kTW;
 
-template <int CH>
-__global__ void __launch_bounds__(kSpreadThreads)
-spread_tile_kernel(NufftGeom g, const int* __restrict__ offsets /*[nkeys+1]*/, const PtRec* __restrict__ rec,
-                   const float2* __restrict__ vals, long long valStride, int nch, int tw0 /*first w tile of slab*/,
-                   int slabTiles, float2* __restrict__ grid /*[ch][slabPlanes][ny][nx]*/) {
-  extern __shared__ float2 acc[];   // [nch][kTW][kTY][kTX]
-  const int tileInSlab = blockIdx.x;
-  const int tx = tileInSlab % g.ntx;
-  const int ty = (tileInSlab / g.ntx) % g.nty;
-  const int twl = tileInSlab / (g.ntx * g.nty);
-  const int tw = tw0 + twl;
-  constexpr int cells = kTX * kTY * kTW;
-  for (int i = threadIdx.x; i < nch * cells; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
-  __syncthreads();
-  const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
-  const int W = g.W;
-  const float half = 0.5f * W;
-  const float invHalf = 1.0f / half;
-  // 27 (source tile, crossing-bits) ranges
+struct SpreadItem {
+  int tile;    // tile index (tw * nty + ty) * ntx + tx
+  int part;    // part index
+  int nparts;  // number of parts of this tile
+  int load;    // points of the tile (all parts)
+};
+
+// The 27 (source tile, crossing bits) key ranges whose points reach tile (tx, ty, tw).
+struct TileRanges {
+  int beg[27], end[27];
+  int n;
+};
+
+__device__ __forceinline__ void tile_ranges(const NufftGeom& g, const int* __restrict__ offsets, int tx, int ty, int tw,
+                                            TileRanges& R) {
+  R.n = 0;
   for (int d = 0; d < 8; ++d) {
     const int dx = d & 1, dy = (d >> 1) & 1, dw = (d >> 2) & 1;
     const int stw = tw - dw;
@@ -381,61 +406,111 @@ spread_tile_kernel(NufftGeom g, const int* __restrict__ offsets /*[nkeys+1]*/, c
     for (int bits = 0; bits < 8; ++bits) {
       if ((bits & d) != d) continue;
       const int key = stile * 8 + bits;
-      const int beg = offsets[key], end = offsets[key + 1];
-      for (int p = beg + threadIdx.x; p < end; p += blockDim.x) {
-        const PtRec pr = rec[p];
-        // kernel values over the support that intersects this tile
-        float kx[kMaxW], ky[kMaxW], kw[kMaxW];
-        // local cell index of support start relative to tile origin (with wrap)
-        int lx = pr.ix0 - x0;
-        lx = ((lx % g.nx) + g.nx) % g.nx;
-        if (lx > g.nx / 2) lx -= g.nx;
-        int ly = pr.iy0 - y0;
-        ly = ((ly % g.ny) + g.ny) % g.ny;
-        if (ly > g.ny / 2) ly -= g.ny;
-        const int lw = pr.iw0 - w0;
+      R.beg[R.n] = offsets[key];
+      R.end[R.n] = offsets[key + 1];
+      ++R.n;
+    }
+  }
+}
+
+static __global__ void tile_load_kernel(NufftGeom g, const int* __restrict__ offsets, int* __restrict__ load) {
+  const int ntiles = g.ntx * g.nty * g.ntw;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int tx = t % g.ntx, ty = (t / g.ntx) % g.nty, tw = t / (g.ntx * g.nty);
+    TileRanges R;
+    tile_ranges(g, offsets, tx, ty, tw, R);
+    int s = 0;
+    for (int i = 0; i < R.n; ++i) s += R.end[i] - R.beg[i];
+    load[t] = s;
+  }
+}
+
+// swizzled cell index inside the tile: x is rotated by W * (y / 2) so that the W x W
+// footprint of a point covers distinct banks
+__device__ __forceinline__ int tile_cell(int x, int y, int w, int W) {
+  return (w * kTY + y) * kTX + ((x + W * (y >> 1)) & (kTX - 1));
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kSpreadThreads)
+spread_warp_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
+                   const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
+                   int tw0, int slabPlanes, float2* __restrict__ grid) {
+  extern __shared__ float sacc[];   // [nch][2][kTileCells]  (re, im planes)
+  const SpreadItem it = items[blockIdx.x];
+  const int tx = it.tile % g.ntx, ty = (it.tile / g.ntx) % g.nty, tw = it.tile / (g.ntx * g.nty);
+  const int twl = tw - tw0;
+  for (int i = threadIdx.x; i < nch * 2 * kTileCells; i += blockDim.x) sacc[i] = 0.f;
+  __syncthreads();
+  const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
+  const int W = g.W;
+  const int W3 = W * W * W;
+  const float invHalf = 2.0f / (float)W;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  // this part's window of the concatenated ranges
+  const long long lo = (long long)it.load * it.part / it.nparts;
+  const long long hi = (long long)it.load * (it.part + 1) / it.nparts;
+  TileRanges R;
+  tile_ranges(g, offsets, tx, ty, tw, R);
+  long long base = 0;
+  for (int ri = 0; ri < R.n; ++ri) {
+    const long long len = R.end[ri] - R.beg[ri];
+    const long long a = max(lo, base), b = min(hi, base + len);
+    for (long long q = a + warp; q < b; q += nwarp) {
+      const int p = R.beg[ri] + (int)(q - base);
+      const PtRec pr = rec[p];
+      int lx = pr.ix0 - x0;
+      lx = ((lx % g.nx) + g.nx) % g.nx;
+      if (lx > g.nx / 2) lx -= g.nx;
+      int ly = pr.iy0 - y0;
+      ly = ((ly % g.ny) + g.ny) % g.ny;
+      if (ly > g.ny / 2) ly -= g.ny;
+      const int lw = pr.iw0 - w0;
+      float kx = 0.f, ky = 0.f, kw = 0.f;
+      if (lane < W) {
+        kx = es_kernel(((float)lane - pr.dx) * invHalf, g.beta);
+        ky = es_kernel(((float)lane - pr.dy) * invHalf, g.beta);
+        kw = es_kernel(((float)lane - pr.dw) * invHalf, g.beta);
+      }
+      float2 v[CH];
 #pragma unroll
-        for (int t = 0; t < kMaxW; ++t) {
-          if (t < W) {
-            kx[t] = es_kernel(((float)t - pr.dx) * invHalf, g.beta);
-            ky[t] = es_kernel(((float)t - pr.dy) * invHalf, g.beta);
-            kw[t] = es_kernel(((float)t - pr.dw) * invHalf, g.beta);
-          }
-        }
-        float2 v[CH];
+      for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+      for (int c0 = 0; c0 < W3; c0 += 32) {
+        const int c = c0 + lane;
+        const int x = c % W, y = (c / W) % W, w = c / (W * W);
+        const float wx = __shfl_sync(0xffffffffu, kx, x);
+        const float wy = __shfl_sync(0xffffffffu, ky, y);
+        const float ww = __shfl_sync(0xffffffffu, kw, w & 31);
+        const int cx = lx + x, cy = ly + y, cw = lw + w;
+        if (c < W3 && cx >= 0 && cx < kTX && cy >= 0 && cy < kTY && cw >= 0 && cw < kTW) {
+          const float k = wx * wy * ww;
+          const int cell = tile_cell(cx, cy, cw, W);
 #pragma unroll
-        for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
-        const int xa = max(0, -lx), xb = min(W, kTX - lx);
-        const int ya = max(0, -ly), yb = min(W, kTY - ly);
-        const int wa = max(0, -lw), wb = min(W, kTW - lw);
-        for (int iw = wa; iw < wb; ++iw) {
-          for (int iy = ya; iy < yb; ++iy) {
-            const float kyw = ky[iy] * kw[iw];
-            const int rowBase = ((lw + iw) * kTY + (ly + iy)) * kTX;
-            for (int ix = xa; ix < xb; ++ix) {
-              const float k = kx[ix] * kyw;
-              const int cell = rowBase + lx + ix;
-#pragma unroll
-              for (int c = 0; c < CH; ++c) {
-                if (c < nch) {
-                  atomicAdd(&acc[c * cells + cell].x, k * v[c].x);
-                  atomicAdd(&acc[c * cells + cell].y, k * v[c].y);
-                }
-              }
+          for (int ch = 0; ch < CH; ++ch) {
+            if (ch < nch) {
+              atomicAdd(&sacc[(ch * 2) * kTileCells + cell], k * v[ch].x);
+              atomicAdd(&sacc[(ch * 2 + 1) * kTileCells + cell], k * v[ch].y);
             }
           }
         }
       }
     }
+    base += len;
   }
   __syncthreads();
-  // write the tile: grid[ch][plane][y][x], plane relative to slab start
-  const int slabPlanes = slabTiles * kTW;
-  for (int i = threadIdx.x; i < nch * cells; i += blockDim.x) {
-    const int c = i / cells, rem = i % cells;
+  // write the tile: grid[ch][plane][y][x], plane relative to the slab start
+  for (int i = threadIdx.x; i < nch * kTileCells; i += blockDim.x) {
+    const int c = i / kTileCells, rem = i % kTileCells;
     const int lw = rem / (kTX * kTY), ly = (rem / kTX) % kTY, lx = rem % kTX;
+    const int cell = tile_cell(lx, ly, lw, W);
+    const float2 val = make_float2(sacc[(c * 2) * kTileCells + cell], sacc[(c * 2 + 1) * kTileCells + cell]);
     const long long off = (((long long)c * slabPlanes + (twl * kTW + lw)) * g.ny + (y0 + ly)) * (long long)g.nx + (x0 + lx);
-    grid[off] = acc[i];
+    if (it.nparts == 1) {
+      grid[off] = val;
+    } else if (val.x != 0.f || val.y != 0.f) {
+      atomicAdd(&grid[off].x, val.x);
+      atomicAdd(&grid[off].y, val.y);
+    }
   }
 }
 
@@ -491,7 +566,8 @@ static __global__ void wsum_kernel(NufftGeom g, const float2* __restrict__ F, in
 static __global__ void finalize_kernel(long long P, int levels, const float2* __restrict__ acc, long long accStride,
                                 const double* __restrict__ decon, const double* __restrict__ nTilde, double wc,
                                 int corrTerms, const double* __restrict__ dl, const double* __restrict__ dm, double su,
-                                double sv, float* __restrict__ image, long long ldImage) {
+                                double sv, float* __restrict__ image, long long ldImage,
+                                const double* __restrict__ zeroAcc) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
     double sn, cs;
     sincos(wc * nTilde[p], &sn, &cs);
@@ -506,7 +582,7 @@ static __global__ void finalize_kernel(long long P, int levels, const float2* __
         a.x -= tu * au.y + tv * av.y;
         a.y += tu * au.x + tv * av.x;
       }
-      image[(long long)l * ldImage + p] += (float)(cfx * a.x - cfy * a.y);
+      image[(long long)l * ldImage + p] += (float)(cfx * a.x - cfy * a.y + zeroAcc[l]);
     }
   }
 }

@@ -126,6 +126,7 @@ struct bipp_pipeline_s {
   long long stepsDone = 0;
   bool timing = false;
   double stageMs[6] = {0, 0, 0, 0, 0, 0};
+  double eigMs[kEigTimers] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> lastLam;
   std::vector<int> lastNred;
 };
@@ -175,7 +176,9 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     E.idx = p->idx.get<int>(); E.nred = p->nred.get<int>(); E.nvis = p->nvis.get<long long>();
     E.status = p->status.get<int>(); E.lam = p->lam.get<double>();
     E.doFlag = 0; E.batchOffset = s0;
+    E.kernelMs = ms ? p->eigMs : nullptr;
     eig_launch<float>(ctx, E, p->eig);
+    if (ms) cudaEventRecord(e1, ctx->stream);
     levels_kernel<<<nb, 128, 0, ctx->stream>>>(nb, N, L, p->intervalsD.get<double>(), p->filter, p->nred.get<int>() + s0,
                                                p->nvis.get<long long>() + s0, p->lam.get<double>() + (long long)s0 * N,
                                                p->kscale.get<float>() + (long long)s0 * N, p->kbeg.get<int>() + s0 * L,
@@ -193,7 +196,12 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     gemm_kernel<float2, float><<<dim3(tiles, tiles, nb * L), kGemmThreads, 0, ctx->stream>>>(g);
     B2_CHECK_LAUNCH();
   }
-  if (ms) cudaEventRecord(e1, ctx->stream);
+  // zero baselines (r == s) of the levels in this transform
+  vv_trace_kernel<<<nb * levelsInTransform, 128, 0, ctx->stream>>>(
+      nb, levelsInTransform, p->nred.get<int>() + s0, p->vv.get<float2>() + (long long)levelOffset * n2, n2 * L, n2, N,
+      p->core.zero_acc());
+  B2_CHECK_LAUNCH();
+  if (ms) cudaEventRecord(e2, ctx->stream);
   // scatter points of these steps
   std::vector<long long> rel(nb + 1);
   for (int i = 0; i <= nb; ++i) rel[i] = pairOffH[s0 + i] - pairOffH[s0];
@@ -220,14 +228,20 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     B2_CHECK_LAUNCH();
   }
   if (ms) {
-    cudaEventRecord(e2, ctx->stream);
-    cudaEventSynchronize(e2);
-    float a, b;
-    cudaEventElapsedTime(&a, e0, e1);
-    cudaEventElapsedTime(&b, e1, e2);
+    cudaEvent_t e3;
+    cudaEventCreate(&e3);
+    cudaEventRecord(e3, ctx->stream);
+    cudaEventSynchronize(e3);
+    float a = 0, b = 0, c = 0;
+    if (!scatterOnly) {
+      cudaEventElapsedTime(&a, e0, e1);
+      cudaEventElapsedTime(&b, e1, e2);
+    }
+    cudaEventElapsedTime(&c, e2, e3);
     ms[0] += a;
-    ms[2] += b;
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    ms[1] += b;
+    ms[2] += c;
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   }
 }
 
@@ -424,6 +438,7 @@ BippError bipp_pipeline_reset(bipp_pipeline_t pl) {
     pl->images.zero();
     pl->stepsDone = 0;
     for (double& x : pl->stageMs) x = 0;
+    for (double& x : pl->eigMs) x = 0;
     sync(pl->ctx);
   });
 }
@@ -447,6 +462,13 @@ BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms) 
     if (enable >= 0) pl->timing = enable != 0;
     if (ms)
       for (int i = 0; i < 6; ++i) ms[i] = pl->stageMs[i];
+  });
+}
+
+BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms) {
+  return guard([&] {
+    require(pl && ms, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    for (int i = 0; i < kEigTimers; ++i) ms[i] = pl->eigMs[i];
   });
 }
 

@@ -227,6 +227,11 @@ BIPP_B200_EXPORT BippError bipp_pipeline_last_eigenvalues(bipp_pipeline_t pl, do
  * [1] virtual visibilities, [2] NUFFT point preparation and sort, [3] spreading, [4] FFT,
  * [5] w-sum and finalisation. Only filled when timing is enabled. */
 BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms);
+/* Accumulated device time (ms) of the eigensolver kernels since the last reset, when
+ * timing is enabled: [0] flagging/compaction/Gram, [1] FP64 Cholesky, [2] triangular
+ * inverse, [3] reduction GEMMs, [4] Householder tridiagonalisation, [5] tridiagonal
+ * eigenpairs, [6] back-transform, [7] Linv^H Y GEMM. */
+BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
 
 #ifdef __cplusplus
