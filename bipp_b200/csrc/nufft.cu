@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <limits>
 #include <numeric>
 #include <vector>
@@ -249,7 +250,10 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   // slab size under a memory budget
   size_t freeB = 0, totalB = 0;
   B2_CUDA(cudaMemGetInfo(&freeB, &totalB));
-  const size_t budget = std::min<size_t>(std::max<size_t>(freeB / 4, planeBytes * kTW * nch_), (size_t)8 << 30);
+  // grid slab budget: a quarter of free memory, at most 8 GB (BIPP_B200_SLAB_BYTES lowers it)
+  size_t cap = (size_t)8 << 30;
+  if (const char* e = std::getenv("BIPP_B200_SLAB_BYTES")) cap = std::max<size_t>(1, std::strtoull(e, nullptr, 10));
+  const size_t budget = std::min<size_t>(std::max<size_t>(freeB / 4, planeBytes * kTW * nch_), cap);
   int slabTiles = (int)std::max<size_t>(1, budget / (planeBytes * kTW * nch_));
   slabTiles = std::min(slabTiles, g_.ntw);
   const int nslab = (g_.ntw + slabTiles - 1) / slabTiles;
