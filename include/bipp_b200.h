@@ -90,6 +90,30 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatc
                                                     const float* wl, const void* s, const float* xyz, float* d,
                                                     void* v, size_t* nBeamReduced, float* scale);
 
+/* Largest antenna count accepted by bipp_eigh_gram_noalloc_s. */
+#define BIPP_NOALLOC_MAX_ANTENNA 128
+
+/* No counterpart in the reference. eigh_gram for one time step (W = I, nBeam = nAntenna)
+ * that allocates no device memory, for callers that cannot let a library call
+ * cudaMalloc/cudaFree: an imager embedded in a host framework whose caching allocator
+ * owns all device memory, or a real-time correlator loop that must not block on the
+ * device-wide synchronisation of cudaFree. Intermediates live in one file-scope
+ * __device__ array of about 1 MB, held by every GPU that loads the library until the
+ * process exits; nAntenna above BIPP_NOALLOC_MAX_ANTENNA is rejected with
+ * BIPP_INVALID_PARAMETER_ERROR. All pointers are DEVICE pointers owned by the caller:
+ * s (nAntenna x nAntenna complex float, lower triangle used, lds), xyz (nAntenna x 3
+ * double, ldxyz); outputs d[nAntenna] (ascending, zero padded), v (nAntenna x nAntenna,
+ * ldv, zero padded), *nBeamReduced, *scale (= 1/nVis) and *info (1 if the Cholesky
+ * factorisation of G failed, else 0). The call is asynchronous on `stream` (a
+ * cudaStream_t). Every call on a device shares the array, so calls that overlap on the
+ * GPU race; serialise them (one stream, or events). The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and should come before any stream
+ * capture. Results agree with bipp_eigh_gram_s. */
+BIPP_B200_EXPORT BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl, size_t nAntenna,
+                                                    const void* s, size_t lds, const double* xyz, size_t ldxyz,
+                                                    float* d, void* v, size_t ldv, int* nBeamReduced, float* scale,
+                                                    int* info);
+
 /* Gram matrix G = W^H sinc(2|p_i - p_j| / wl) W, nBeam x nBeam complex; replaces
  * bipp::host::gram_matrix (src/host/gram_matrix.hpp:15-17). */
 BIPP_B200_EXPORT BippError bipp_gram_matrix_s(bipp_ctx_t ctx, size_t nAntenna, size_t nBeam, const void* w,
