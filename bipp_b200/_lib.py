@@ -86,6 +86,7 @@ SIGNATURES = {
     "bipp_pipeline_last_eigenvalues": [_p, _p, _p],
     "bipp_pipeline_stage_times": [_p, _i, _p],
     "bipp_pipeline_kernel_times": [_p, _p],
+    "bipp_pipeline_nufft_stats": [_p, _p],
     "bipp_pipeline_destroy": [_p],
 }
 

@@ -576,6 +576,12 @@ class Pipeline:
         check(self.ctx._lib.bipp_pipeline_kernel_times(self.handle, _ptr(ms)))
         return ms
 
+    def nufft_stats(self):
+        """Last NUFFT: dict(points, slabs, grid_bytes, items, nx, ny, nw, W)."""
+        st = np.zeros(8, dtype=np.int64)
+        check(self.ctx._lib.bipp_pipeline_nufft_stats(self.handle, _ptr(st)))
+        return dict(zip(["points", "slabs", "grid_bytes", "items", "nx", "ny", "nw", "W"], [int(x) for x in st]))
+
     def close(self):
         if getattr(self, "handle", None):
             self.ctx._lib.bipp_pipeline_destroy(self.handle)

@@ -582,7 +582,15 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
     const int g = tid / 128, lt = tid % 128;
     for (int r = lt; r < m; r += 128) {
       C acc = mk(R(0), R(0));
-      for (int c = g; c < m; c += groups) cfma(acc, Ab[(1 + r) + (long long)(1 + c) * Nmax], v[c]);
+      int c = g;
+      for (; c + 7 * groups < m; c += 8 * groups) {
+        C a[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a[u] = Ab[(1 + r) + (long long)(1 + c + u * groups) * Nmax];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cfma(acc, a[u], v[c + u * groups]);
+      }
+      for (; c < m; c += groups) cfma(acc, Ab[(1 + r) + (long long)(1 + c) * Nmax], v[c]);
       ppart[g * Nmax + r] = acc;
     }
     __syncthreads();
@@ -654,7 +662,24 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
       const C vr = v[1 + r], wr = w[1 + r];
       C acc = mk(R(0), R(0));
       C* rowp = Ab + (i + 2 + r) + (long long)(i + 2) * Nmax;
-      for (int c = g; c < mm; c += groups) {
+      int c = g;
+      // eight independent loads in flight per thread before the updates
+      constexpr int U = sizeof(C) == 8 ? 8 : 4;  // FP64 complex keeps 4 to stay within 64 registers
+      for (; c + (U - 1) * groups < mm; c += U * groups) {
+        C a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) a[u] = rowp[(long long)(c + u * groups) * Nmax];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int cc = c + u * groups;
+          a[u] = a[u] - cmulc(vr, w[1 + cc]) - cmulc(wr, v[1 + cc]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) rowp[(long long)(c + u * groups) * Nmax] = a[u];
+#pragma unroll
+        for (int u = 0; u < U; ++u) cfma(acc, a[u], vn[c + u * groups]);
+      }
+      for (; c < mm; c += groups) {
         C a = rowp[(long long)c * Nmax];
         a = a - cmulc(vr, w[1 + c]) - cmulc(wr, v[1 + c]);
         rowp[(long long)c * Nmax] = a;

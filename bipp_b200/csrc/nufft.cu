@@ -231,13 +231,27 @@ void NufftCore::end_count(long long nPoints) {
   vals_.ensure(ctx_, (size_t)nch_ * valStride_ * sizeof(float2));
 }
 
+template <int CH, int W>
+static void launch_spread_w(const NufftGeom& g, int nItems, size_t smem, cudaStream_t st, const int* offs,
+                            const PtRec* rec, const float2* vals, long long vs, int nch, const SpreadItem* items,
+                            int tw0, int slabPlanes, float2* out) {
+  auto k = spread_warp_kernel<CH, W>;
+  smem_optin(k, smem);
+  k<<<nItems, kSpreadThreads, smem, st>>>(g, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out);
+}
+
 template <int CH>
 static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStream_t st, const int* offs,
                           const PtRec* rec, const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
                           int slabPlanes, float2* out) {
-  auto k = spread_warp_kernel<CH>;
-  smem_optin(k, smem);
-  k<<<nItems, kSpreadThreads, smem, st>>>(g, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out);
+  switch (g.W) {
+#define B2_W(w) \
+  case w: launch_spread_w<CH, w>(g, nItems, smem, st, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out); break;
+    B2_W(2) B2_W(3) B2_W(4) B2_W(5) B2_W(6) B2_W(7) B2_W(8) B2_W(9) B2_W(10) B2_W(11) B2_W(12) B2_W(13) B2_W(14)
+    B2_W(15) B2_W(16)
+#undef B2_W
+    default: throw Error(BIPP_INTERNAL_ERROR, "unsupported NUFFT kernel width");
+  }
 }
 
 // points per spreading part: heavier tiles are split so that no CTA serialises the
@@ -286,6 +300,15 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     }
   }
   slabBegin[nslab] = (int)items.size();
+  {
+    int total = 0;
+    d2h(ctx_, &total, offsets_.get<int>() + nkeys_, sizeof(int));
+    sync(ctx_);
+    lastPoints = total;
+    lastSlabs = nslab;
+    lastItems = (long long)items.size();
+    lastGridBytes = (long long)g_.ntw * kTW * (long long)planeBytes * nch_;
+  }
   items_.ensure(ctx_, std::max<size_t>(1, items.size()) * sizeof(SpreadItem));
   h2d(ctx_, items_.get(), items.data(), items.size() * sizeof(SpreadItem));
   const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);

@@ -52,6 +52,9 @@ public:
   void execute(float* image, long long ldImage, double* stageMs = nullptr);
 
   const NufftGeom& geom() const { return g_; }
+  // statistics of the last execute(): points spread, slabs (spreading launches), bytes of
+  // grid written by the spreading (all slabs), work items
+  long long lastPoints = 0, lastSlabs = 0, lastGridBytes = 0, lastItems = 0;
   long long num_pixels() const { return (long long)g_.Na * g_.Nb; }
   int channels() const { return nch_; }
   bool sincos64() const { return eps_ < 1e-6; }

@@ -431,71 +431,87 @@ __device__ __forceinline__ int tile_cell(int x, int y, int w, int W) {
   return (w * kTY + y) * kTX + ((x + W * (y >> 1)) & (kTX - 1));
 }
 
-template <int CH>
+template <int CH, int W>
 __global__ void __launch_bounds__(kSpreadThreads)
 spread_warp_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                    const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                    int tw0, int slabPlanes, float2* __restrict__ grid) {
   extern __shared__ float sacc[];   // [nch][2][kTileCells]  (re, im planes)
+  __shared__ int rBeg[27], rPre[28];
   const SpreadItem it = items[blockIdx.x];
   const int tx = it.tile % g.ntx, ty = (it.tile / g.ntx) % g.nty, tw = it.tile / (g.ntx * g.nty);
   const int twl = tw - tw0;
   for (int i = threadIdx.x; i < nch * 2 * kTileCells; i += blockDim.x) sacc[i] = 0.f;
+  if (threadIdx.x == 0) {
+    TileRanges R;
+    tile_ranges(g, offsets, tx, ty, tw, R);
+    int pre = 0;
+    for (int i = 0; i < R.n; ++i) {
+      rBeg[i] = R.beg[i];
+      rPre[i] = pre;
+      pre += R.end[i] - R.beg[i];
+    }
+    for (int i = R.n; i < 28; ++i) rPre[i] = pre;
+  }
   __syncthreads();
   const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
-  const int W = g.W;
-  const int W3 = W * W * W;
+  constexpr int W3 = W * W * W;
+  constexpr int nIter = (W3 + 31) / 32;
   const float invHalf = 2.0f / (float)W;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  // this part's window of the concatenated ranges
-  const long long lo = (long long)it.load * it.part / it.nparts;
-  const long long hi = (long long)it.load * (it.part + 1) / it.nparts;
-  TileRanges R;
-  tile_ranges(g, offsets, tx, ty, tw, R);
-  long long base = 0;
-  for (int ri = 0; ri < R.n; ++ri) {
-    const long long len = R.end[ri] - R.beg[ri];
-    const long long a = max(lo, base), b = min(hi, base + len);
-    for (long long q = a + warp; q < b; q += nwarp) {
-      const int p = R.beg[ri] + (int)(q - base);
-      const PtRec pr = rec[p];
-      int lx = pr.ix0 - x0;
-      lx = ((lx % g.nx) + g.nx) % g.nx;
-      if (lx > g.nx / 2) lx -= g.nx;
-      int ly = pr.iy0 - y0;
-      ly = ((ly % g.ny) + g.ny) % g.ny;
-      if (ly > g.ny / 2) ly -= g.ny;
-      const int lw = pr.iw0 - w0;
-      float kx = 0.f, ky = 0.f, kw = 0.f;
-      if (lane < W) {
-        kx = es_kernel(((float)lane - pr.dx) * invHalf, g.beta);
-        ky = es_kernel(((float)lane - pr.dy) * invHalf, g.beta);
-        kw = es_kernel(((float)lane - pr.dw) * invHalf, g.beta);
-      }
-      float2 v[CH];
+  // lane-constant support offsets (x, y, w) of the cells this lane covers, packed 8 bits each
+  unsigned cellOff[nIter];
 #pragma unroll
-      for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
-      for (int c0 = 0; c0 < W3; c0 += 32) {
-        const int c = c0 + lane;
-        const int x = c % W, y = (c / W) % W, w = c / (W * W);
-        const float wx = __shfl_sync(0xffffffffu, kx, x);
-        const float wy = __shfl_sync(0xffffffffu, ky, y);
-        const float ww = __shfl_sync(0xffffffffu, kw, w & 31);
-        const int cx = lx + x, cy = ly + y, cw = lw + w;
-        if (c < W3 && cx >= 0 && cx < kTX && cy >= 0 && cy < kTY && cw >= 0 && cw < kTW) {
-          const float k = wx * wy * ww;
-          const int cell = tile_cell(cx, cy, cw, W);
+  for (int i = 0; i < nIter; ++i) {
+    const int c = i * 32 + lane;
+    const int x = c % W, y = (c / W) % W, w = c / (W * W);
+    cellOff[i] = (c < W3) ? (unsigned)(x | (y << 8) | (w << 16)) : 0xffffffffu;
+  }
+  // this part's window of the concatenated ranges, dealt to the warps round robin
+  const int lo = (int)((long long)it.load * it.part / it.nparts);
+  const int hi = (int)((long long)it.load * (it.part + 1) / it.nparts);
+  int ri = 0;
+  for (int q = lo + warp; q < hi; q += nwarp) {
+    while (q >= rPre[ri + 1]) ++ri;
+    const int p = rBeg[ri] + (q - rPre[ri]);
+    const PtRec pr = rec[p];
+    int lx = pr.ix0 - x0;
+    lx = ((lx % g.nx) + g.nx) % g.nx;
+    if (lx > g.nx / 2) lx -= g.nx;
+    int ly = pr.iy0 - y0;
+    ly = ((ly % g.ny) + g.ny) % g.ny;
+    if (ly > g.ny / 2) ly -= g.ny;
+    const int lw = pr.iw0 - w0;
+    float kx = 0.f, ky = 0.f, kw = 0.f;
+    if (lane < W) {
+      kx = es_kernel(((float)lane - pr.dx) * invHalf, g.beta);
+      ky = es_kernel(((float)lane - pr.dy) * invHalf, g.beta);
+      kw = es_kernel(((float)lane - pr.dw) * invHalf, g.beta);
+    }
+    float2 v[CH];
 #pragma unroll
-          for (int ch = 0; ch < CH; ++ch) {
-            if (ch < nch) {
-              atomicAdd(&sacc[(ch * 2) * kTileCells + cell], k * v[ch].x);
-              atomicAdd(&sacc[(ch * 2 + 1) * kTileCells + cell], k * v[ch].y);
-            }
+    for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < nIter; ++i) {
+      const unsigned o = cellOff[i];
+      const int x = o & 0xff, y = (o >> 8) & 0xff, w = (o >> 16) & 0xff;
+      const float wx = __shfl_sync(0xffffffffu, kx, x & 31);
+      const float wy = __shfl_sync(0xffffffffu, ky, y & 31);
+      const float ww = __shfl_sync(0xffffffffu, kw, w & 31);
+      const int cx = lx + x, cy = ly + y, cw = lw + w;
+      if (o != 0xffffffffu && (unsigned)cx < (unsigned)kTX && (unsigned)cy < (unsigned)kTY &&
+          (unsigned)cw < (unsigned)kTW) {
+        const float k = wx * wy * ww;
+        const int cell = tile_cell(cx, cy, cw, W);
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+          if (ch < nch) {
+            atomicAdd(&sacc[(ch * 2) * kTileCells + cell], k * v[ch].x);
+            atomicAdd(&sacc[(ch * 2 + 1) * kTileCells + cell], k * v[ch].y);
           }
         }
       }
     }
-    base += len;
   }
   __syncthreads();
   // write the tile: grid[ch][plane][y][x], plane relative to the slab start

@@ -465,6 +465,21 @@ BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms) 
   });
 }
 
+BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats) {
+  return guard([&] {
+    require(pl && stats, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    const NufftGeom& g = pl->core.geom();
+    stats[0] = pl->core.lastPoints;
+    stats[1] = pl->core.lastSlabs;
+    stats[2] = pl->core.lastGridBytes;
+    stats[3] = pl->core.lastItems;
+    stats[4] = g.nx;
+    stats[5] = g.ny;
+    stats[6] = g.nw;
+    stats[7] = g.W;
+  });
+}
+
 BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms) {
   return guard([&] {
     require(pl && ms, "null pointer", BIPP_INVALID_POINTER_ERROR);

@@ -256,6 +256,10 @@ BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int ena
  * inverse, [3] reduction GEMMs, [4] Householder tridiagonalisation, [5] tridiagonal
  * eigenpairs, [6] back-transform, [7] Linv^H Y GEMM. */
 BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms);
+/* Statistics of the last NUFFT of the pipeline (8 values): points spread, spreading
+ * launches (w-slabs), grid bytes written by the spreading, spreading work items, fine
+ * grid sizes nx, ny, nw, kernel width W. */
+BIPP_B200_EXPORT BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
 
 #ifdef __cplusplus
