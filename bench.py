@@ -194,6 +194,52 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
     return 1.0 / per_step, threads, desc
 
 
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "of measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+def profiled_traffic_per_point():
+    """DRAM bytes per spread point, from the committed ncu summary of the spreading
+    kernel (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its points)."""
+    path = os.path.join(ROOT, "profiles", "spread_warp_kernel_c2.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.startswith("traffic_bytes_per_point:"):
+                    return float(ln.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def spread_roofline(stats, spread_ms, n_levels):
+    """Roofline of the dominant kernel, the NUFFT spreader (one launch per w-slab).
+
+    Algorithmic bytes of one batch: every point read once (3 FP32 coordinates + one
+    complex FP32 value per level) and every fine-grid cell written once per level:
+    points * (12 + 8 L) + L * cells * 8 (= the grid bytes). Per launch = batch / slabs;
+    the launch duration is the spreading kernels' CUDA-event time / slabs."""
+    slabs = max(1, stats["slabs"])
+    bytes_batch = stats["points"] * (12 + 8 * n_levels) + stats["grid_bytes"]
+    per_launch = bytes_batch / slabs
+    dur_s = spread_ms / 1000.0 / slabs
+    peaks, label = measured_peaks()
+    achieved = per_launch / dur_s / 1e9
+    flops = stats["points"] * n_levels * 4 * stats["W"] ** 3 / slabs  # real weight x complex value: 4 flops
+    tpp = profiled_traffic_per_point()
+    traffic = tpp * stats["points"] / slabs if tpp else None
+    return {"kernel": "spread_warp_kernel", "bound": "hbm", "achieved": round(achieved, 2),
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 5),
+            "peak_source": label, "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch),
+            "launches_per_step": slabs, "launch_ms": round(dur_s * 1000.0, 3),
+            "flops_per_launch": int(flops), "achieved_tflops": round(flops / dur_s / 1e12, 3),
+            "note": "spreading is shared-memory-atomic/issue bound; the HBM fraction is its floor"}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation on host cores (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -275,12 +321,14 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_launch0 = bipp.kernel_launch_count()
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             one_step()
         ev1.record(stream)
         torch.cuda.synchronize()
+    gpu_launches = bipp.kernel_launch_count() - n_launch0
     if world > 1:
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
@@ -297,17 +345,18 @@ def main():
         dist.reduce(img, dst=0, op=dist.ReduceOp.SUM)
 
     # per-stage breakdown (separate, untimed pass)
-    stages = None
+    stages = roof = None
     if args.stages or rank == 0:
         pl.reset()
         pl.stage_times(True)
         one_step()
         st = pl.stage_times(False)
-        stages = dict(zip(["eigensolve", "levels_vv", "flags_sort_scatter", "spread", "fft", "wsum"],
+        stages = dict(zip(["eigensolve", "levels_vv", "flags_sort_scatter", "spread", "fft", "wsum", "grid_clear"],
                           [round(float(x), 3) for x in st]))
         kt = pl.kernel_times()
         stages["eig_kernels"] = dict(zip(["prep_gram", "cholesky_fp64", "trinv_fp64", "reduction_gemms", "hetrd",
                                           "tridiag_fp64", "backtransform", "x_gemm"], [round(float(x), 3) for x in kt]))
+        roof = spread_roofline(pl.nufft_stats(), float(st[3]), cfg.n_levels)
 
     # end to end through the public API: pinned host inputs copied in every step,
     # images read back every step
@@ -357,8 +406,8 @@ def main():
                                        "4 levels, 1024^2 px over 16 deg, eps 1e-5",
                            "time_steps_per_batch": T, "mode": args.mode, "parallelism": f"dp{world} (steps)",
                            "l2": "inputs (4.3 GB/batch) larger than L2; no flush"},
-                "clocks": clk.summary(), "gpu_launches": None, "stages_ms": stages, "e2e": e2e,
-                "cpu_baseline": cpu, "roofline": None}
+                "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,
+                "cpu_baseline": cpu, "roofline": roof}
         print(json.dumps(line))
     pl.close()
     ctx.close()

@@ -20,6 +20,7 @@ from .api import (  # noqa: F401
     eigh_gram_full,
     gram_matrix,
     image_synthesis,
+    kernel_launch_count,
     nuft_sum,
     virtual_vis,
 )

@@ -52,6 +52,7 @@ class PipelineConfig(C.Structure):
 # symbol -> argtypes (all return BippError as int unless listed in _RESTYPE)
 SIGNATURES = {
     "bipp_last_error": [],
+    "bipp_kernel_launch_count": [],
     "bipp_ctx_create": [_i, C.POINTER(_p)],
     "bipp_ctx_create_on_device": [_i, _i, C.POINTER(_p)],
     "bipp_ctx_destroy": [_p],
@@ -93,6 +94,9 @@ SIGNATURES = {
 _lib = None
 
 
+RESTYPES = {"bipp_last_error": C.c_char_p, "bipp_kernel_launch_count": C.c_ulonglong}
+
+
 def load(path: str = LIB_PATH):
     """Load the shared library and declare every exported entry point."""
     global _lib
@@ -104,7 +108,7 @@ def load(path: str = LIB_PATH):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = C.c_char_p if name == "bipp_last_error" else C.c_int
+        fn.restype = RESTYPES.get(name, C.c_int)
     _lib = lib
     return lib
 

@@ -75,6 +75,11 @@ def default_context() -> Context:
         return _default_ctx
 
 
+def kernel_launch_count() -> int:
+    """Kernels this library has launched in this process so far (cuFFT's excluded)."""
+    return int(_lib.load().bipp_kernel_launch_count())
+
+
 def _prec(wl, *arrays):
     dbl = isinstance(wl, (np.float64, float)) and not isinstance(wl, np.float32)
     for a in arrays:
@@ -565,7 +570,7 @@ class Pipeline:
         return d, nr
 
     def stage_times(self, enable: Optional[bool] = None):
-        ms = np.zeros(6, dtype=np.float64)
+        ms = np.zeros(7, dtype=np.float64)
         check(self.ctx._lib.bipp_pipeline_stage_times(self.handle, -1 if enable is None else int(enable), _ptr(ms)))
         return ms
 

@@ -1,5 +1,6 @@
 // C-ABI: context, error reporting, domain partition, dataset-driven image synthesis.
 #include <algorithm>
+#include <atomic>
 #include <complex>
 #include <cstring>
 #include <memory>
@@ -19,6 +20,9 @@ template <> __device__ __forceinline__ double fmul_rn_t<double>(double a, double
 namespace bippb200 {
 
 static thread_local std::string g_lastError;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_last_error(const std::string& msg) { g_lastError = msg; }
 
@@ -137,13 +141,19 @@ static void partition_host(bipp_ctx_s* ctx, const size_t* dims, size_t n, const 
   for (int d = 0; d < 3; ++d) h2d(ctx, dc.get<T>() + d * n, c[d], n * sizeof(T));
   counts.zero();
   const int blocks = (int)std::min<long long>(((long long)n + 255) / 256, 4096);
+  count_launch();
   part_group_kernel<T><<<blocks, 256, 0, ctx->stream>>>((long long)n, dc.get<T>(), dc.get<T>() + n, dc.get<T>() + 2 * n,
                                                         mn[0], mn[1], mn[2], inv[0], inv[1], inv[2], dims[0], dims[1],
                                                         dims[2], deg[0], deg[1], deg[2], dg.get<unsigned long long>());
+  count_launch();
   part_count_kernel<<<blocks, 256, 0, ctx->stream>>>((long long)n, dg.get<unsigned long long>(), nChunks, counts.get<int>());
+  count_launch();
   scan_partial_kernel<<<nb, kScanThreads, 0, ctx->stream>>>(counts.get<int>(), offs.get<int>(), nc, bs.get<int>());
+  count_launch();
   scan_blocksums_kernel<<<1, 1024, 0, ctx->stream>>>(bs.get<int>(), nb, offs.get<int>() + nc);
+  count_launch();
   scan_add_kernel<<<nb, 1024, 0, ctx->stream>>>(offs.get<int>(), nc, bs.get<int>(), cursor.get<int>());
+  count_launch();
   part_scatter_kernel<<<(int)nChunks, 32, 0, ctx->stream>>>((long long)n, dg.get<unsigned long long>(), nChunks,
                                                            cursor.get<int>(), dp.get<unsigned long long>());
   B2_CHECK_LAUNCH();
@@ -165,6 +175,8 @@ using namespace bippb200;
 extern "C" {
 
 const char* bipp_last_error(void) { return g_lastError.c_str(); }
+
+unsigned long long bipp_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 BippError bipp_ctx_create_on_device(BippProcessingUnit pu, int device, bipp_ctx_t* out) {
   return guard([&] {
@@ -318,6 +330,7 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
         g.n = dn.get<int>(); g.outMode = 0; g.levels = 1;
         g.kscale = dK.get(); g.kbeg = dn.get<int>() + 1; g.kend = dn.get<int>() + 2;
         const int tiles = ((int)nAnt + kGemmBM - 1) / kGemmBM;
+        count_launch();
         gemm_kernel<float2, float><<<dim3(tiles, tiles, 1), kGemmThreads, 0, ctx->stream>>>(g);
         B2_CHECK_LAUNCH();
         d2h(ctx, vvAll.data() + im * nB, dVV.get(), nB * sizeof(float2));

@@ -29,6 +29,10 @@ struct Error : std::runtime_error {
 
 #define B2_CHECK_LAUNCH() B2_CUDA(cudaGetLastError())
 
+// Count of kernel launches issued by this library (read by bipp_kernel_launch_count);
+// every launch site calls count_launch() right before its <<<>>>.
+void count_launch();
+
 inline void require(bool ok, const char* msg, BippError code = BIPP_INVALID_PARAMETER_ERROR) {
   if (!ok) throw Error(code, msg);
 }

@@ -184,6 +184,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     const size_t smem = 2 * (size_t)Nmax * sizeof(int);
     auto k = prep_kernel<T>;
     smem_optin(k, smem);
+    count_launch();
     k<<<nb, kPrepThreads, smem, st>>>(L.nBeam, L.S, L.sStride, L.lds, L.xyz, L.xyzStride, L.ldxyz, L.wl, L.mode,
                                       L.eps, L.gram && L.identityW, Nmax, L.idx, L.nred, L.nvis, A, G, L.status,
                                       L.doFlag, 1, L.batchOffset);
@@ -195,8 +196,11 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     DevBuf gant(ctx, (size_t)L.nAnt * L.nAnt * sizeof(double));
     DevBuf tmp(ctx, (size_t)L.nAnt * Nmax * sizeof(double2));
     const int nred0 = L.hostNred;
+    count_launch();
     gram_antenna_kernel<<<256, 256, 0, st>>>(L.nAnt, L.xyz, L.ldxyz, L.hostWl, gant.get<double>());
+    count_launch();
     gram_gw_kernel<C><<<256, 256, 0, st>>>(L.nAnt, nred0, gant.get<double>(), L.W, L.ldw, L.idx, tmp.get<double2>());
+    count_launch();
     gram_whgw_kernel<C><<<256, 256, 0, st>>>(L.nAnt, nred0, L.W, L.ldw, L.idx, tmp.get<double2>(), G, Nmax);
     B2_CHECK_LAUNCH();
   }
@@ -204,10 +208,12 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   if (L.gram) {
     mark(1);
     smem_optin(cholesky_kernel, kCholSmem);
+    count_launch();
     cholesky_kernel<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset);
     B2_CHECK_LAUNCH();
     mark(2);
     smem_optin(trinv_kernel<C>, kTrinvSmem);
+    count_launch();
     trinv_kernel<C><<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax);
     B2_CHECK_LAUNCH();
     // T1 = Linv * A
@@ -217,6 +223,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g1.B = A; g1.strideB = n2; g1.ldb = Nmax; g1.opB = 0;
     g1.Cm = T1; g1.strideC = n2; g1.ldc = Nmax;
     g1.n = nred; g1.triA = 1; g1.triB = 0; g1.outMode = 0; g1.levels = 1;
+    count_launch();
     gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
     B2_CHECK_LAUNCH();
     // A = T1 * Linv^H (Hermitian: lower tiles + mirror)
@@ -225,6 +232,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g2.B = Linv; g2.strideB = n2; g2.ldb = Nmax; g2.opB = 1;
     g2.Cm = A; g2.strideC = n2; g2.ldc = Nmax;
     g2.n = nred; g2.triA = 0; g2.triB = 1; g2.outMode = 1; g2.levels = 1;
+    count_launch();
     gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
     B2_CHECK_LAUNCH();
   }
@@ -234,6 +242,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     const size_t smem = 12 * (size_t)Nmax * sizeof(C);
     auto k = hetrd_kernel<C, R>;
     smem_optin(k, smem);
+    count_launch();
     k<<<nb, kTrdThreads, smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
                                      w.tau.template get<C>());
     B2_CHECK_LAUNCH();
@@ -244,6 +253,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     const size_t smem = 4 * (size_t)Nmax * sizeof(double);
     auto k = tridiag_kernel<R>;
     smem_optin(k, smem);
+    count_launch();
     k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
                                      L.status + L.batchOffset);
@@ -256,11 +266,13 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     if (smem16 <= ctx->maxSmemOptin) {
       auto k = backtransform_kernel<C, R, 16>;
       smem_optin(k, smem16);
+      count_launch();
       k<<<dim3((Nmax + 15) / 16, nb), kBtThreads, smem16, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1);
     } else {
       const size_t smem4 = ((size_t)Nmax * 4 + Nmax + kBtThreads) * sizeof(C);
       auto k = backtransform_kernel<C, R, 4>;
       smem_optin(k, smem4);
+      count_launch();
       k<<<dim3((Nmax + 3) / 4, nb), kBtThreads, smem4, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1);
     }
     B2_CHECK_LAUNCH();
@@ -273,6 +285,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g3.B = T1; g3.strideB = n2; g3.ldb = Nmax; g3.opB = 0;
     g3.Cm = reinterpret_cast<C*>(G); g3.strideC = n2; g3.ldc = Nmax;
     g3.n = nred; g3.triA = 2; g3.triB = 0; g3.outMode = 0; g3.levels = 1;
+    count_launch();
     gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);
     B2_CHECK_LAUNCH();
   }
@@ -358,6 +371,7 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
     const size_t smem = 2 * (size_t)Nmax * sizeof(int);
     auto k = prep_kernel<T>;
     smem_optin(k, smem);
+    count_launch();
     k<<<1, kPrepThreads, smem, ctx->stream>>>(F.nBeam, F.S, F.sStride, F.lds, F.xyz, F.xyzStride, F.ldxyz, F.wl,
                                               F.mode, F.eps, 0, Nmax, F.idx, F.nred, F.nvis,
                                               work.A.template get<C>(), work.G.template get<double2>(), F.status, 1, 0, 0);
@@ -379,6 +393,7 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   DevBuf dOut;
   if (v) {
     dOut.alloc(ctx, nAntenna * nBeam * sizeof(C));
+    count_launch();
     unbeam_kernel<C><<<256, 256, 0, ctx->stream>>>((int)nAntenna, (int)nBeam, nred > 0 ? nred : 0,
                                                    work.X(gram), Nmax, dIdx.get<int>(), dW.get<C>(), (int)nAntenna,
                                                    identity ? 1 : 0, dOut.get<C>());
@@ -441,12 +456,14 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     d2h(ctx, nr.data(), dNred.get<int>() + b0, nb * sizeof(int));
     sync(ctx);
     for (size_t b = 0; b < nb; ++b) {
+      count_launch();
       unbeam_kernel<C><<<128, 256, 0, ctx->stream>>>((int)nAnt, (int)nAnt, nr[b],
                                                      work.X(true) + (long long)b * Nmax * Nmax, Nmax,
                                                      dIdx.get<int>() + (b0 + b) * Nmax, nullptr, 0, 1,
                                                      dOut.get<C>() + b * n2);
     }
     B2_CHECK_LAUNCH();
+    count_launch();
     pad_eigenvalues_kernel<<<64, 256, 0, ctx->stream>>>((int)nb, (int)nAnt, dNred.get<int>() + b0,
                                                         dLam.get<double>() + b0 * Nmax, Nmax, dLamPad.get<double>());
     B2_CHECK_LAUNCH();
@@ -491,10 +508,13 @@ static void gram_host(bipp_ctx_s* ctx, size_t nAnt, size_t nBeam, const void* w,
   h2d(ctx, dX.get(), xyzh.data(), xyzh.size() * sizeof(double));
   h2d(ctx, dW.get(), wh.data(), wh.size() * sizeof(C));
   h2d(ctx, dIdx.get(), idx.data(), idx.size() * sizeof(int));
+  count_launch();
   gram_antenna_kernel<<<256, 256, 0, ctx->stream>>>((int)nAnt, dX.get<double>(), (int)nAnt, (double)wl, gant.get<double>());
+  count_launch();
   gram_gw_kernel<C><<<256, 256, 0, ctx->stream>>>((int)nAnt, (int)nBeam, gant.get<double>(), dW.get<C>(), (int)nAnt,
                                                   dIdx.get<int>(), tmp.get<double2>());
   dG.zero();
+  count_launch();
   gram_whgw_kernel<C><<<256, 256, 0, ctx->stream>>>((int)nAnt, (int)nBeam, dW.get<C>(), (int)nAnt, dIdx.get<int>(),
                                                     tmp.get<double2>(), dG.get<double2>(), (int)nBeam);
   B2_CHECK_LAUNCH();
@@ -531,6 +551,7 @@ static void virtual_vis_host(bipp_ctx_s* ctx, T scale, size_t nAnt, size_t nBeam
   g.n = dn.get<int>(); g.outMode = 0; g.levels = 1;
   g.kscale = dK.get(); g.kbeg = dn.get<int>() + 1; g.kend = dn.get<int>() + 2;
   const int tiles = ((int)nAnt + kGemmBM - 1) / kGemmBM;
+  count_launch();
   gemm_kernel<C, T><<<dim3(tiles, tiles, 1), kGemmThreads, 0, ctx->stream>>>(g);
   B2_CHECK_LAUNCH();
   d2h(ctx, vv, dVV.get(), nAnt * nAnt * sizeof(C));

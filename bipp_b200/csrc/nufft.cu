@@ -181,6 +181,7 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   h2d(ctx, qz_.get(), qx.data(), qx.size() * sizeof(double));
   h2d(ctx, qw_.get(), qwt.data(), qwt.size() * sizeof(double));
   decon_.alloc(ctx, P * sizeof(double));
+  count_launch();
   decon_kernel<<<std::min<long long>(4096, (P + 255) / 256), 256, 0, ctx->stream>>>(
       g_, nTilde_.get<double>(), qz_.get<double>(), qw_.get<double>(), (int)qx.size(), decon_.get<double>());
   B2_CHECK_LAUNCH();
@@ -221,9 +222,12 @@ void NufftCore::end_count(long long nPoints) {
   const long long per = (long long)kScanThreads * kScanItems;
   const int nb = (int)((n + per - 1) / per);
   blockSums_.ensure(ctx_, (nb + 1) * sizeof(int));
+  count_launch();
   scan_partial_kernel<<<nb, kScanThreads, 0, ctx_->stream>>>(counts_.get<int>(), offsets_.get<int>(), n,
                                                              blockSums_.get<int>());
+  count_launch();
   scan_blocksums_kernel<<<1, 1024, 0, ctx_->stream>>>(blockSums_.get<int>(), nb, offsets_.get<int>() + n);
+  count_launch();
   scan_add_kernel<<<nb, 1024, 0, ctx_->stream>>>(offsets_.get<int>(), n, blockSums_.get<int>(), cursor_.get<int>());
   B2_CHECK_LAUNCH();
   valStride_ = std::max<long long>(nPoints, 1);
@@ -237,6 +241,7 @@ static void launch_spread_w(const NufftGeom& g, int nItems, size_t smem, cudaStr
                             int tw0, int slabPlanes, float2* out) {
   auto k = spread_warp_kernel<CH, W>;
   smem_optin(k, smem);
+  count_launch();
   k<<<nItems, kSpreadThreads, smem, st>>>(g, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out);
 }
 
@@ -279,6 +284,7 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   // per-tile loads -> work items (non-empty tiles, heavy tiles split), grouped by slab
   const int ntiles = g_.ntx * g_.nty * g_.ntw;
   load_.ensure(ctx_, (size_t)ntiles * sizeof(int));
+  count_launch();
   tile_load_kernel<<<std::min(4096, (ntiles + 255) / 256), 256, 0, ctx_->stream>>>(g_, offsets_.get<int>(),
                                                                                    load_.get<int>());
   B2_CHECK_LAUNCH();
@@ -312,16 +318,17 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   items_.ensure(ctx_, std::max<size_t>(1, items.size()) * sizeof(SpreadItem));
   h2d(ctx_, items_.get(), items.data(), items.size() * sizeof(SpreadItem));
   const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[5];
   if (stageMs)
     for (auto& e : ev) B2_CUDA(cudaEventCreate(&e));
-  float tSpread = 0, tFft = 0, tW = 0;
+  float tSpread = 0, tFft = 0, tW = 0, tClear = 0;
   for (int sl = 0; sl < nslab; ++sl) {
     const int tw0 = sl * slabTiles;
     const int tiles = std::min(slabTiles, g_.ntw - tw0);
     const int nItems = slabBegin[sl + 1] - slabBegin[sl];
-    if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
+    if (stageMs) B2_CUDA(cudaEventRecord(ev[4], ctx_->stream));
     B2_CUDA(cudaMemsetAsync(grid_.get(), 0, (size_t)nch_ * slabPlanes * planeBytes, ctx_->stream));
+    if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
     if (nItems > 0) {
       const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];
       if (nch_ <= 4)
@@ -338,20 +345,23 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
                           CUFFT_INVERSE));
     if (stageMs) B2_CUDA(cudaEventRecord(ev[2], ctx_->stream));
     const int blocks = (int)std::min<long long>((P + 255) / 256, 65535);
+    count_launch();
     wsum_kernel<<<blocks, 256, 0, ctx_->stream>>>(g_, grid_.get<float2>(), nch_, slabPlanes, tw0 * kTW,
                                                   tiles * kTW, nTilde_.get<double>(), acc_.get<float2>(), P);
     B2_CHECK_LAUNCH();
     if (stageMs) {
       B2_CUDA(cudaEventRecord(ev[3], ctx_->stream));
       B2_CUDA(cudaEventSynchronize(ev[3]));
-      float a, b, c;
+      float a, b, c, z;
       cudaEventElapsedTime(&a, ev[0], ev[1]);
       cudaEventElapsedTime(&b, ev[1], ev[2]);
       cudaEventElapsedTime(&c, ev[2], ev[3]);
-      tSpread += a; tFft += b; tW += c;
+      cudaEventElapsedTime(&z, ev[4], ev[0]);
+      tSpread += a; tFft += b; tW += c; tClear += z;
     }
   }
   const int blocks = (int)std::min<long long>((P + 255) / 256, 65535);
+  count_launch();
   finalize_kernel<<<blocks, 256, 0, ctx_->stream>>>(P, levels_, acc_.get<float2>(), P, decon_.get<double>(),
                                                     nTilde_.get<double>(), g_.wc, corrTerms_ ? 1 : 0,
                                                     dl_.get<double>(), dm_.get<double>(), su_, sv_, image, ldImage,
@@ -361,6 +371,7 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     stageMs[0] += tSpread;
     stageMs[1] += tFft;
     stageMs[2] += tW;
+    stageMs[3] += tClear;
     for (auto& e : ev) cudaEventDestroy(e);
   }
 }
@@ -427,14 +438,17 @@ static void nufft_transform(bipp_nufft_s* p) {
     DevBuf u64(ctx, 3 * n * sizeof(double));
     DevBuf v64(ctx, n * sizeof(double2));
     for (int c = 0; c < 3; ++c) {
+      count_launch();
       f2d_kernel<<<256, 256, 0, ctx->stream>>>(p->uvw.get<float>() + c * ld, n, u64.get<double>() + c * n);
     }
     B2_CHECK_LAUNCH();
     const double* ud = u64.get<double>();
     const int blocks = (int)((p->nPixel + kDirectThreads - 1) / kDirectThreads);
     for (size_t im = 0; im < p->nImages; ++im) {
+      count_launch();
       f2d_kernel<<<256, 256, 0, ctx->stream>>>(reinterpret_cast<const float*>(p->values.get<float2>() + im * ld), 2 * n,
                                                v64.get<double>());
+      count_launch();
       direct_sum_kernel<double, double2, double, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
           1.0, n, v64.get<double2>(), n, ud, ud + n, ud + 2 * n, (long long)p->nPixel, lx, lx + p->nPixel,
           lx + 2 * p->nPixel, p->imagesD.get<double>() + im * p->nPixel, (long long)p->nPixel, 1, 1);
@@ -447,6 +461,7 @@ static void nufft_transform(bipp_nufft_s* p) {
 static void host_minmax(bipp_ctx_s* ctx, const float* x, long long n, DevBuf& scratch, double& lo, double& hi) {
   const int blocks = 256;
   scratch.ensure(ctx, 2 * blocks * sizeof(double));
+  count_launch();
   minmax_kernel<<<blocks, 256, 0, ctx->stream>>>(x, n, 1.0, scratch.get<double>());
   B2_CHECK_LAUNCH();
   std::vector<double> mm(2 * blocks);
@@ -486,9 +501,11 @@ static void nufft_transform_lattice(bipp_nufft_s* p, long long n, long long ld) 
   bp.levels = (int)p->nImages;
   const NufftGeom& g = p->core.geom();
   const int gb = (int)std::min<long long>((n + 255) / 256, 8192);
+  count_launch();
   baseline_count_kernel<<<gb, 256, 0, ctx->stream>>>(g, bp, p->core.counts());
   B2_CHECK_LAUNCH();
   p->core.end_count(n);
+  count_launch();
   baseline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(g, bp, p->core.cursor(), p->core.records(), p->core.values(),
                                                        p->core.value_stride(), p->core.sincos64() ? 1 : 0,
                                                        p->core.corr_terms() ? 1 : 0, p->core.su(), p->core.sv(),
@@ -618,6 +635,7 @@ BippError bipp_nufft_get_image(bipp_nufft_t plan, size_t imgIdx, float* image) {
     bipp_ctx_s* ctx = p->ctx;
     if (!p->lattice) {
       // fold the FP64 direct-sum accumulator into the float images
+      count_launch();
       add_double_to_float_kernel<<<256, 256, 0, ctx->stream>>>(p->imagesD.get<double>(), (long long)(p->nImages * p->nPixel),
                                                               p->images.get<float>());
       B2_CHECK_LAUNCH();
@@ -653,6 +671,7 @@ BippError bipp_nuft_sum_s(bipp_ctx_t ctx, float alpha, size_t nIn, const void* i
     h2d(ctx, dX.get<float>() + 2 * nOut, z, nOut * sizeof(float));
     h2d(ctx, dO.get(), out, nOut * sizeof(float));
     const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
+    count_launch();
     direct_sum_kernel<float, float2, float, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         (double)alpha, (long long)nIn, dIn.get<float2>(), (long long)nIn, dU.get<float>(), dU.get<float>() + nIn,
         dU.get<float>() + 2 * nIn, (long long)nOut, dX.get<float>(), dX.get<float>() + nOut, dX.get<float>() + 2 * nOut,
@@ -679,6 +698,7 @@ BippError bipp_nuft_sum_d(bipp_ctx_t ctx, double alpha, size_t nIn, const void* 
     h2d(ctx, dX.get<double>() + 2 * nOut, z, nOut * sizeof(double));
     h2d(ctx, dO.get(), out, nOut * sizeof(double));
     const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
+    count_launch();
     direct_sum_kernel<double, double2, double, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         alpha, (long long)nIn, dIn.get<double2>(), (long long)nIn, dU.get<double>(), dU.get<double>() + nIn,
         dU.get<double>() + 2 * nIn, (long long)nOut, dX.get<double>(), dX.get<double>() + nOut,
@@ -699,6 +719,7 @@ BippError bipp_nuft_sum_multi_device(bipp_ctx_t ctx, double alpha, size_t nIn, s
     const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
     for (size_t c0 = 0; c0 < nch; c0 += 4) {
       const int n = (int)std::min<size_t>(4, nch - c0);
+      count_launch();
       direct_sum_kernel<double, float2, double, 4><<<blocks, kDirectThreads, 0, ctx->stream>>>(
           alpha, (long long)nIn, static_cast<const float2*>(values) + c0 * ldIn, (long long)ldIn, u, v, w,
           (long long)nOut, x, y, z, out + c0 * ldOut, (long long)ldOut, n, fp64Trig);

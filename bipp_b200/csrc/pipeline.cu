@@ -125,7 +125,7 @@ struct bipp_pipeline_s {
   DevBuf images;
   long long stepsDone = 0;
   bool timing = false;
-  double stageMs[6] = {0, 0, 0, 0, 0, 0};
+  double stageMs[7] = {0, 0, 0, 0, 0, 0, 0};
   double eigMs[kEigTimers] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> lastLam;
   std::vector<int> lastNred;
@@ -179,6 +179,7 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     E.kernelMs = ms ? p->eigMs : nullptr;
     eig_launch<float>(ctx, E, p->eig);
     if (ms) cudaEventRecord(e1, ctx->stream);
+    count_launch();
     levels_kernel<<<nb, 128, 0, ctx->stream>>>(nb, N, L, p->intervalsD.get<double>(), p->filter, p->nred.get<int>() + s0,
                                                p->nvis.get<long long>() + s0, p->lam.get<double>() + (long long)s0 * N,
                                                p->kscale.get<float>() + (long long)s0 * N, p->kbeg.get<int>() + s0 * L,
@@ -193,10 +194,12 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     g.kscale = p->kscale.get<float>() + (long long)s0 * N; g.strideK = N;
     g.kbeg = p->kbeg.get<int>() + s0 * L; g.kend = p->kend.get<int>() + s0 * L;
     const int tiles = (N + kGemmBM - 1) / kGemmBM;
+    count_launch();
     gemm_kernel<float2, float><<<dim3(tiles, tiles, nb * L), kGemmThreads, 0, ctx->stream>>>(g);
     B2_CHECK_LAUNCH();
   }
   // zero baselines (r == s) of the levels in this transform
+  count_launch();
   vv_trace_kernel<<<nb * levelsInTransform, 128, 0, ctx->stream>>>(
       nb, levelsInTransform, p->nred.get<int>() + s0, p->vv.get<float2>() + (long long)levelOffset * n2, n2 * L, n2, N,
       p->core.zero_acc());
@@ -222,6 +225,7 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
   const long long total = rel[nb];
   if (total > 0) {
     const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
+    count_launch();
     pipeline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.cursor(), relD.get<long long>(),
                                                          p->core.records(), p->core.values(), p->core.value_stride(),
                                                          p->core.sincos64() ? 1 : 0);
@@ -263,6 +267,7 @@ static void pipeline_count(bipp_pipeline_s* p, int s0, int nb, const std::vector
   const long long total = rel[nb];
   if (total > 0) {
     const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
+    count_launch();
     pipeline_count_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.counts(), relD.get<long long>());
     B2_CHECK_LAUNCH();
   }
@@ -285,9 +290,11 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   B2_CUDA(cudaMemcpyAsync(p->S.get(), s, (size_t)T * n2 * sizeof(float2), kind, ctx->stream));
   B2_CUDA(cudaMemcpyAsync(p->xyz.get(), xyz, (size_t)T * N * 3 * sizeof(double), kind, ctx->stream));
   B2_CUDA(cudaMemcpyAsync(p->wl.get(), wl, (size_t)T * sizeof(double), kind, ctx->stream));
+  count_launch();
   antenna_uvw_kernel<<<T, 256, 0, ctx->stream>>>(T, N, p->xyz.get<double>(), p->wl.get<double>(), p->basis.get<double>(),
                                                  p->antUVW.get<double>(), p->uvwScale.get<double>(),
                                                  p->wrange.get<double>());
+  count_launch();
   xyz_transpose_kernel<<<1024, 256, 0, ctx->stream>>>((long long)T * 3 * N, N, p->xyz.get<double>(), p->xyzT.get<double>());
   p->status.zero();
   // flags for every step
@@ -295,6 +302,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     const size_t smem = 2 * (size_t)N * sizeof(int);
     auto k = prep_kernel<float>;
     smem_optin(k, smem);
+    count_launch();
     k<<<T, kPrepThreads, smem, ctx->stream>>>(N, p->S.get<float2>(), n2, N, p->xyzT.get<double>(), 3ll * N, N,
                                               p->wl.get<double>(), 0, std::numeric_limits<float>::epsilon(), 1, N,
                                               p->idx.get<int>(), p->nred.get<int>(), p->nvis.get<long long>(),
@@ -328,11 +336,12 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
     p->core.end_count(pairOff[T]);
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_chunk(p, s0, std::min(chunk, T - s0), pairOff, L, 0, false, ms);
-    double nm[3] = {0, 0, 0};
+    double nm[4] = {0, 0, 0, 0};
     p->core.execute(p->images.get<float>(), p->P, p->timing ? nm : nullptr);
     p->stageMs[3] += nm[0];
     p->stageMs[4] += nm[1];
     p->stageMs[5] += nm[2];
+    p->stageMs[6] += nm[3];
   } else {
     // plain: one step at a time, one NUFFT per step and level
     for (int b = 0; b < T; ++b) {
@@ -341,11 +350,12 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
         pipeline_count(p, b, 1, pairOff);
         p->core.end_count(pairOff[b + 1] - pairOff[b]);
         pipeline_chunk(p, b, 1, pairOff, 1, l, l > 0, ms);
-        double nm[3] = {0, 0, 0};
+        double nm[4] = {0, 0, 0, 0};
         p->core.execute(p->images.get<float>() + (long long)l * p->P, p->P, p->timing ? nm : nullptr);
         p->stageMs[3] += nm[0];
         p->stageMs[4] += nm[1];
         p->stageMs[5] += nm[2];
+        p->stageMs[6] += nm[3];
       }
     }
   }
@@ -419,6 +429,7 @@ BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize,
     if (normalize && pl->stepsDone > 0) {
       const float s = 1.0f / (float)pl->stepsDone;
       if (onDevice) {
+        count_launch();
         scale_images_kernel<<<1024, 256, 0, ctx->stream>>>(images, n, s);
         B2_CHECK_LAUNCH();
         sync(ctx);
@@ -461,7 +472,7 @@ BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms) 
     require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
     if (enable >= 0) pl->timing = enable != 0;
     if (ms)
-      for (int i = 0; i < 6; ++i) ms[i] = pl->stageMs[i];
+      for (int i = 0; i < 7; ++i) ms[i] = pl->stageMs[i];
   });
 }
 

@@ -38,6 +38,11 @@ typedef struct bipp_pipeline_s* bipp_pipeline_t;
 /* Message of the last failed call on this thread (empty if none). */
 BIPP_B200_EXPORT const char* bipp_last_error(void);
 
+/* Number of this library's own CUDA kernels launched by this process so far (all
+ * threads and devices; cuFFT's kernels are not counted). No reference counterpart:
+ * an instrumentation hook for benchmarks (launches between two reads = difference). */
+BIPP_B200_EXPORT unsigned long long bipp_kernel_launch_count(void);
+
 /* ---- context ------------------------------------------------------------------- */
 
 /* Create a context on the current CUDA device (replaces Context(BippProcessingUnit),
@@ -247,9 +252,10 @@ BIPP_B200_EXPORT BippError bipp_pipeline_images(bipp_pipeline_t pl, float* image
 BIPP_B200_EXPORT BippError bipp_pipeline_reset(bipp_pipeline_t pl);
 /* Eigenvalues [maxSteps][nAntenna] and nBeamReduced of the last process() call (host). */
 BIPP_B200_EXPORT BippError bipp_pipeline_last_eigenvalues(bipp_pipeline_t pl, double* d, int* nReduced);
-/* Accumulated device time (ms) per stage since the last reset: [0] eigensolver,
- * [1] virtual visibilities, [2] NUFFT point preparation and sort, [3] spreading, [4] FFT,
- * [5] w-sum and finalisation. Only filled when timing is enabled. */
+/* Accumulated device time (ms) per stage since the last reset (7 values): [0] eigensolver,
+ * [1] virtual visibilities, [2] NUFFT point preparation and sort, [3] spreading kernel,
+ * [4] FFT, [5] w-sum, [6] clearing of the fine-grid slabs. Only filled when timing is
+ * enabled. */
 BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int enable, double* ms);
 /* Accumulated device time (ms) of the eigensolver kernels since the last reset, when
  * timing is enabled: [0] flagging/compaction/Gram, [1] FP64 Cholesky, [2] triangular
