@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--antennas", type=int, default=512)
     ap.add_argument("--image", type=int, default=1024)
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--chunk-steps", type=int, default=1024, help="time steps per eigensolver/VV chunk")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -202,14 +203,15 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-def profiled_traffic_per_point():
-    """DRAM bytes per spread point, from the committed ncu summary of the spreading
-    kernel (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its points)."""
+def profiled_traffic_per_grid_byte():
+    """DRAM bytes per grid byte of one spreading launch, from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one launch / that launch's slab
+    bytes); writes of the slab are ~90% of it and the reads follow the slab's points."""
     path = os.path.join(ROOT, "profiles", "spread_warp_kernel_c2.md")
     try:
         with open(path) as f:
             for ln in f:
-                if ln.startswith("traffic_bytes_per_point:"):
+                if ln.startswith("traffic_bytes_per_grid_byte:"):
                     return float(ln.split(":", 1)[1].split()[0])
     except OSError:
         pass
@@ -230,8 +232,8 @@ def spread_roofline(stats, spread_ms, n_levels):
     peaks, label = measured_peaks()
     achieved = per_launch / dur_s / 1e9
     flops = stats["points"] * n_levels * 4 * stats["W"] ** 3 / slabs  # real weight x complex value: 4 flops
-    tpp = profiled_traffic_per_point()
-    traffic = tpp * stats["points"] / slabs if tpp else None
+    tpg = profiled_traffic_per_grid_byte()
+    traffic = int(tpg * stats["grid_bytes"] / slabs) if tpg else None
     return {"kernel": "spread_warp_kernel", "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 5),
             "peak_source": label, "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch),
@@ -307,7 +309,8 @@ def main():
     intervals = calibrate_levels(ctx, cfg, S, xyz)
     n = cfg.image_size
     pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
-                       tolerance=cfg.eps, chunk_steps=256, max_steps=cfg.n_steps, mode=args.mode)
+                       tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, cfg.n_steps), max_steps=cfg.n_steps,
+                       mode=args.mode)
     T = cfg.n_steps
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
 

@@ -239,7 +239,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   // 3. tridiagonalisation
   mark(4);
   {
-    const size_t smem = 12 * (size_t)Nmax * sizeof(C);
+    const size_t smem = hetrd_smem_bytes(Nmax, sizeof(C));
     auto k = hetrd_kernel<C, R>;
     smem_optin(k, smem);
     count_launch();

@@ -544,6 +544,120 @@ __device__ __forceinline__ void householder(C* __restrict__ col, int m, C* __res
   betaOut = beta;
 }
 
+// Reduce G per-lane values over the 32 lanes of a warp so that column k's total ends in
+// the lanes whose id has top log2(G) bits == k (recursive halving: G-1 exchanges instead
+// of G full reductions).
+template <int G, typename C>
+__device__ __forceinline__ C warp_reduce_scatter(C (&v)[G], int lane) {
+  constexpr int LG = G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 0;
+#pragma unroll
+  for (int s = 0; s < LG; ++s) {
+    const int bit = 4 - s;
+    const bool hi = (lane >> bit) & 1;
+    constexpr int kHalfMax = G / 2;
+    const int half = G >> (s + 1);
+#pragma unroll
+    for (int k = 0; k < kHalfMax; ++k) {
+      if (k < half) {
+        const C send = hi ? v[k] : v[k + half];
+        const C keep = hi ? v[k + half] : v[k];
+        C recv;
+        recv.x = __shfl_xor_sync(0xffffffffu, send.x, 1 << bit);
+        recv.y = __shfl_xor_sync(0xffffffffu, send.y, 1 << bit);
+        v[k] = keep + recv;
+      }
+    }
+  }
+  C r = v[0];
+#pragma unroll
+  for (int o = 1; o < (32 >> LG); o <<= 1) {
+    r.x += __shfl_xor_sync(0xffffffffu, r.x, o);
+    r.y += __shfl_xor_sync(0xffffffffu, r.y, o);
+  }
+  return r;
+}
+
+// One pass over the lower triangle of the mm x mm Hermitian block A0 (column-major, ld):
+// optionally the rank-2 update A -= vU wU^H + wU vU^H (UPD), and y += A x with the upper
+// triangle taken as the conjugate transpose of the lower one. Work unit: a 32 x 32 tile
+// per warp, lanes over rows; row sums stay in a register, column sums are reduced across
+// lanes G columns at a time; y (shared) is accumulated with shared-memory atomics.
+template <typename C, typename R, bool UPD>
+__device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int mm, const C* __restrict__ vU,
+                                               const C* __restrict__ wU, const C* __restrict__ x,
+                                               C* __restrict__ y) {
+  constexpr int G = sizeof(C) == 8 ? 4 : 2;  // loads in flight per lane within 64 registers
+  constexpr int LG = G == 8 ? 3 : G == 4 ? 2 : 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int nT = (mm + 31) >> 5;
+  const int nTiles = nT * (nT + 1) / 2;
+  const C zero = mk(R(0), R(0));
+  for (int t = warp; t < nTiles; t += nwarp) {
+    int I = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    const int J = t - I * (I + 1) / 2;
+    const int r = I * 32 + lane;
+    const bool rv = r < mm;
+    C vr = zero, wr = zero, xr = zero;
+    if (rv) {
+      xr = x[r];
+      if (UPD) { vr = vU[r]; wr = wU[r]; }
+    }
+    C ry = zero;
+    C* rowp = A0 + (rv ? r : 0);
+    const int cEnd = min(mm, J * 32 + 32);
+    // loads of the next G columns are issued before the current ones are used
+    C an[G];
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int c = J * 32 + u;
+      an[u] = (rv && c < mm && c <= r) ? rowp[(long long)c * ld] : zero;
+    }
+    for (int c0 = J * 32; c0 < cEnd; c0 += G) {
+      C a[G];
+#pragma unroll
+      for (int u = 0; u < G; ++u) a[u] = an[u];
+      if (c0 + G < cEnd) {
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+          const int c = c0 + G + u;
+          an[u] = (rv && c < mm && c <= r) ? rowp[(long long)c * ld] : zero;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        const int c = c0 + u;
+        const bool ok = rv && c < mm && c <= r;
+        if (UPD && ok) {
+          a[u] = a[u] - cmulc(vr, wU[c]) - cmulc(wr, vU[c]);
+          rowp[(long long)c * ld] = a[u];
+        }
+        const C xc = (c < mm) ? x[c] : zero;
+        if (ok) cfma(ry, a[u], xc);
+        // a[u] becomes this lane's contribution conj(a) x_r to y_c (strictly lower part)
+        C cp = zero;
+        if (ok && c < r) cfma_cj(cp, a[u], xr);
+        a[u] = cp;
+      }
+      const C s = warp_reduce_scatter<G>(a, lane);
+      const int cc = c0 + (lane >> (5 - LG));
+      if ((lane & ((32 >> LG) - 1)) == 0 && cc < mm) {
+        atomicAdd(&y[cc].x, s.x);
+        atomicAdd(&y[cc].y, s.y);
+      }
+    }
+    if (rv) {
+      atomicAdd(&y[r].x, ry.x);
+      atomicAdd(&y[r].y, ry.y);
+    }
+  }
+}
+
+// shared memory of hetrd_kernel: v, w, p, vn, y
+constexpr size_t hetrd_smem_bytes(int Nmax, size_t complexBytes) { return 5 * (size_t)Nmax * complexBytes; }
+
+// Only the lower triangle of A is read or written (the upper one is never touched).
 template <typename C, typename R>
 __global__ void __launch_bounds__(kTrdThreads)
 hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
@@ -557,9 +671,9 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
   extern __shared__ unsigned char smem_raw[];
   C* v = reinterpret_cast<C*>(smem_raw);        // [Nmax] current reflector (relative to row i+1)
   C* w = v + Nmax;                              // [Nmax] w vector
-  C* p = w + Nmax;                              // [Nmax] accumulated tau*A*v for the next step
+  C* p = w + Nmax;                              // [Nmax] tau*A*v for the next step
   C* vn = p + Nmax;                             // [Nmax] next reflector
-  C* ppart = vn + Nmax;                         // [8][Nmax] partial mat-vec sums
+  C* y = vn + Nmax;                             // [Nmax] mat-vec accumulator
   __shared__ R red[32];
   __shared__ C s_tau, s_taun;
   __shared__ R s_beta;
@@ -570,35 +684,16 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
     return;
   }
 
-  // ---- step 0 set-up: reflector of column 0, p = tau A22 v (plain mat-vec) ----
+  // ---- step 0 set-up: reflector of column 0, p = tau A22 v ----
   {
     C t; R be;
+    for (int r = tid; r < n; r += blockDim.x) y[r] = mk(R(0), R(0));
     householder<C, R>(Ab + 1, n - 1, v, red, t, be);
     if (tid == 0) { s_tau = t; s_beta = be; }
     __syncthreads();
-    const int m = n - 1;
-    // p[r] = tau * sum_c A22[r,c] v[c]; rows split over threads, columns over groups
-    const int groups = kTrdThreads / 128;  // 8 groups of 128 threads
-    const int g = tid / 128, lt = tid % 128;
-    for (int r = lt; r < m; r += 128) {
-      C acc = mk(R(0), R(0));
-      int c = g;
-      for (; c + 7 * groups < m; c += 8 * groups) {
-        C a[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) a[u] = Ab[(1 + r) + (long long)(1 + c + u * groups) * Nmax];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) cfma(acc, a[u], v[c + u * groups]);
-      }
-      for (; c < m; c += groups) cfma(acc, Ab[(1 + r) + (long long)(1 + c) * Nmax], v[c]);
-      ppart[g * Nmax + r] = acc;
-    }
+    trd_lower_pass<C, R, false>(Ab + 1 + Nmax, Nmax, n - 1, nullptr, nullptr, v, y);
     __syncthreads();
-    for (int r = tid; r < m; r += blockDim.x) {
-      C acc = mk(R(0), R(0));
-      for (int gg = 0; gg < groups; ++gg) acc = acc + ppart[gg * Nmax + r];
-      p[r] = cmul(s_tau, acc);
-    }
+    for (int r = tid; r < n - 1; r += blockDim.x) p[r] = cmul(s_tau, y[r]);
     __syncthreads();
   }
 
@@ -625,7 +720,10 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
     pi = block_sum(pi, red);
     const C pHv = mk(pr, pi);
     const C alph = cscale(cmul(tau, pHv), R(-0.5));
-    for (int r = tid; r < m; r += blockDim.x) w[r] = p[r] + cmul(alph, v[r]);
+    for (int r = tid; r < m; r += blockDim.x) {
+      w[r] = p[r] + cmul(alph, v[r]);
+      y[r] = mk(R(0), R(0));
+    }
     __syncthreads();
     if (m == 1) {
       // last 1x1 trailing block
@@ -653,46 +751,14 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
       if (tid == 0) { s_taun = t; s_beta = be; }
     }
     __syncthreads();
-    // fused pass over A33 = A[i+2:, i+2:] (size m-1): rank-2 update with (v[1:], w[1:]),
-    // accumulate pn = A33_new * vn
+    // fused pass over the lower triangle of A33 = A[i+2:, i+2:] (size m-1): rank-2 update
+    // with (v[1:], w[1:]) and y = A33_new vn
     const int mm = m - 1;
-    const int groups = kTrdThreads / 128;
-    const int g = tid / 128, lt = tid % 128;
-    for (int r = lt; r < mm; r += 128) {
-      const C vr = v[1 + r], wr = w[1 + r];
-      C acc = mk(R(0), R(0));
-      C* rowp = Ab + (i + 2 + r) + (long long)(i + 2) * Nmax;
-      int c = g;
-      // eight independent loads in flight per thread before the updates
-      constexpr int U = sizeof(C) == 8 ? 8 : 4;  // FP64 complex keeps 4 to stay within 64 registers
-      for (; c + (U - 1) * groups < mm; c += U * groups) {
-        C a[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) a[u] = rowp[(long long)(c + u * groups) * Nmax];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int cc = c + u * groups;
-          a[u] = a[u] - cmulc(vr, w[1 + cc]) - cmulc(wr, v[1 + cc]);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) rowp[(long long)(c + u * groups) * Nmax] = a[u];
-#pragma unroll
-        for (int u = 0; u < U; ++u) cfma(acc, a[u], vn[c + u * groups]);
-      }
-      for (; c < mm; c += groups) {
-        C a = rowp[(long long)c * Nmax];
-        a = a - cmulc(vr, w[1 + c]) - cmulc(wr, v[1 + c]);
-        rowp[(long long)c * Nmax] = a;
-        cfma(acc, a, vn[c]);
-      }
-      ppart[g * Nmax + r] = acc;
-    }
+    trd_lower_pass<C, R, true>(Ab + (i + 2) + (long long)(i + 2) * Nmax, Nmax, mm, v + 1, w + 1, vn, y);
     __syncthreads();
     const C taun = s_taun;
     for (int r = tid; r < mm; r += blockDim.x) {
-      C acc = mk(R(0), R(0));
-      for (int gg = 0; gg < groups; ++gg) acc = acc + ppart[gg * Nmax + r];
-      p[r] = cmul(taun, acc);
+      p[r] = cmul(taun, y[r]);
       v[r] = vn[r];
     }
     if (tid == 0) s_tau = taun;

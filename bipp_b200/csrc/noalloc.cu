@@ -167,7 +167,7 @@ extern "C" BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl
     gemm_kernel<float2, float><<<dim3(tiles, tiles, 1), kGemmThreads, 0, st>>>(g2);
     B2_CHECK_LAUNCH();
     {
-      const size_t smem = 12 * (size_t)N * sizeof(float2);
+      const size_t smem = hetrd_smem_bytes(N, sizeof(float2));
       smem_optin(hetrd_kernel<float2, float>, smem);
       hetrd_kernel<float2, float><<<1, kTrdThreads, smem, st>>>(w.A, nred, N, w.d, w.e, w.tau);
     }
