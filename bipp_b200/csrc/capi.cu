@@ -19,17 +19,24 @@ template <> __device__ __forceinline__ double fmul_rn_t<double>(double a, double
 
 namespace bippb200 {
 
-static thread_local std::string g_lastError;
+// Message of the last failure on this thread. A plain character array: a thread_local
+// std::string would be destroyed before objects with static storage duration, and a
+// caller's static context released at exit still goes through guard().
+static thread_local char g_lastError[1024];
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-void set_last_error(const std::string& msg) { g_lastError = msg; }
+void set_last_error(const std::string& msg) {
+  const size_t n = std::min(msg.size(), sizeof(g_lastError) - 1);
+  std::memcpy(g_lastError, msg.data(), n);
+  g_lastError[n] = '\0';
+}
 
 BippError guard(const std::function<void()>& body) {
   try {
     body();
-    g_lastError.clear();
+    g_lastError[0] = '\0';
     return BIPP_SUCCESS;
   } catch (const Error& e) {
     set_last_error(e.what());
@@ -174,7 +181,7 @@ using namespace bippb200;
 
 extern "C" {
 
-const char* bipp_last_error(void) { return g_lastError.c_str(); }
+const char* bipp_last_error(void) { return g_lastError; }
 
 unsigned long long bipp_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
