@@ -219,7 +219,7 @@ def profiled_traffic_per_grid_byte():
 
 
 def spread_roofline(stats, spread_ms, n_levels):
-    """Roofline of the dominant kernel, the NUFFT spreader (one launch per w-slab).
+    """Roofline of the dominant NUFFT kernel, the spreader (one launch per w-slab).
 
     Algorithmic bytes of one batch: every point read once (3 FP32 coordinates + one
     complex FP32 value per level) and every fine-grid cell written once per level:
@@ -234,12 +234,13 @@ def spread_roofline(stats, spread_ms, n_levels):
     flops = stats["points"] * n_levels * 4 * stats["W"] ** 3 / slabs  # real weight x complex value: 4 flops
     tpg = profiled_traffic_per_grid_byte()
     traffic = int(tpg * stats["grid_bytes"] / slabs) if tpg else None
-    return {"kernel": "spread_warp_kernel", "bound": "hbm", "achieved": round(achieved, 2),
+    return {"kernel": "spread_tc_kernel", "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 5),
             "peak_source": label, "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch),
             "launches_per_step": slabs, "launch_ms": round(dur_s * 1000.0, 3),
             "flops_per_launch": int(flops), "achieved_tflops": round(flops / dur_s / 1e12, 3),
-            "note": "spreading is shared-memory-atomic/issue bound; the HBM fraction is its floor"}
+            "note": "tcgen05 3xTF32 spreading; bound by building the dense operands (issue), "
+                    "the HBM fraction is its floor"}
 
 
 def run_reference(args):

@@ -6,10 +6,12 @@
 #include <cstdlib>
 #include <limits>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "context.hpp"
 #include "nufft.hpp"
+#include "spread_tc.cuh"
 
 namespace bippb200 {
 
@@ -252,11 +254,31 @@ static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStrea
   switch (g.W) {
 #define B2_W(w) \
   case w: launch_spread_w<CH, w>(g, nItems, smem, st, offs, rec, vals, vs, nch, items, tw0, slabPlanes, out); break;
-    B2_W(2) B2_W(3) B2_W(4) B2_W(5) B2_W(6) B2_W(7) B2_W(8) B2_W(9) B2_W(10) B2_W(11) B2_W(12) B2_W(13) B2_W(14)
-    B2_W(15) B2_W(16)
+    B2_W(2) B2_W(3) B2_W(4) B2_W(5) B2_W(6) B2_W(7) B2_W(8) B2_W(9)
 #undef B2_W
     default: throw Error(BIPP_INTERNAL_ERROR, "unsupported NUFFT kernel width");
   }
+}
+
+// tensor-core spreading (up to 4 channels): persistent CTAs, 4 per SM
+static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, const int* offs, const PtRec* rec,
+                             const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
+                             int slabPlanes, float2* out, int* errFlag) {
+  int dev = 0, sms = 148;
+  B2_CUDA(cudaGetDevice(&dev));
+  B2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  smem_optin(spread_tc_kernel, kTcSmem);
+  const int grid = std::max(1, std::min(nItems, sms * kTcMinBlocks));
+  count_launch();
+  spread_tc_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0, slabPlanes,
+                                                       out, errFlag);
+}
+
+// BIPP_B200_SPREAD=warp selects the shared-memory-atomic spreader for every channel count
+static bool use_tensor_core_spread(int nch) {
+  const char* e = std::getenv("BIPP_B200_SPREAD");
+  if (e && std::string(e) == "warp") return false;
+  return nch <= kTcChan;
 }
 
 // points per spreading part: heavier tiles are split so that no CTA serialises the
@@ -318,6 +340,9 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   items_.ensure(ctx_, std::max<size_t>(1, items.size()) * sizeof(SpreadItem));
   h2d(ctx_, items_.get(), items.data(), items.size() * sizeof(SpreadItem));
   const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);
+  const bool tc = use_tensor_core_spread(nch_);
+  errFlag_.ensure(ctx_, sizeof(int));
+  B2_CUDA(cudaMemsetAsync(errFlag_.get(), 0, sizeof(int), ctx_->stream));
   cudaEvent_t ev[5];
   if (stageMs)
     for (auto& e : ev) B2_CUDA(cudaEventCreate(&e));
@@ -329,7 +354,12 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     if (stageMs) B2_CUDA(cudaEventRecord(ev[4], ctx_->stream));
     B2_CUDA(cudaMemsetAsync(grid_.get(), 0, (size_t)nch_ * slabPlanes * planeBytes, ctx_->stream));
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
-    if (nItems > 0) {
+    if (nItems > 0 && tc) {
+      launch_spread_tc(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),
+                       valStride_, nch_, items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes,
+                       grid_.get<float2>(), errFlag_.get<int>());
+      B2_CHECK_LAUNCH();
+    } else if (nItems > 0) {
       const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];
       if (nch_ <= 4)
         launch_spread<4>(g_, nItems, smem, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),
@@ -367,6 +397,12 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
                                                     dl_.get<double>(), dm_.get<double>(), su_, sv_, image, ldImage,
                                                     zeroAcc_.get<double>());
   B2_CHECK_LAUNCH();
+  if (tc) {
+    int err = 0;
+    d2h(ctx_, &err, errFlag_.get(), sizeof(int));
+    sync(ctx_);
+    if (err) throw Error(BIPP_GPU_ERROR, "tensor-core spreading: MMA completion wait timed out");
+  }
   if (stageMs) {
     stageMs[0] += tSpread;
     stageMs[1] += tFft;

@@ -16,8 +16,8 @@
 
 namespace bippb200 {
 
-constexpr int kTX = 16, kTY = 16, kTW = 8;       // output tile (cells)
-constexpr int kMaxW = 16;                         // max kernel width
+constexpr int kTX = 16, kTY = 8, kTW = 8;        // output tile (cells): 128 (x, y) cells x 8 w-planes
+constexpr int kMaxW = 9;                          // max kernel width: a support crosses at most one tile edge (W - 1 <= kTY)
 constexpr int kMaxChan = 12;                      // max channels (levels x correction terms)
 
 struct NufftGeom {
@@ -379,6 +379,8 @@ static __global__ void scan_add_kernel(int* __restrict__ out, long long n, const
 // ---------------------------------------------------------------------------------------
 constexpr int kSpreadThreads = 256;
 constexpr int kTileCells = kTX * kTY * kTW;
+
+static_assert(kMaxW - 1 <= kTX && kMaxW - 1 <= kTY && kMaxW - 1 <= kTW, "tile smaller than a kernel support");
 
 struct SpreadItem {
   int tile;    // tile index (tw * nty + ty) * ntx + tx

@@ -1,0 +1,384 @@
+// NUFFT spreading on the 5th-generation tensor cores (sm_100a, tcgen05).
+//
+// For one output tile of 16 x 8 (x, y) cells and 8 w-planes, the spread grid is a sum of
+// separable outer products over the points ("visits") that reach the tile:
+//     G[(x,y), (w,c)] = sum_p  phi_x,p(x) phi_y,p(y)  *  phi_w,p(w) v_p,c
+// i.e. the product of A (128 cells x K visits) and B (K visits x 64 columns: 8 planes x
+// 4 channels x re/im). Threads write A and B for 32 visits at a time into shared memory
+// (canonical K-major, no swizzle), one thread issues tcgen05.mma (kind::tf32) into a
+// 128 x 64 FP32 accumulator in tensor memory, and the epilogue reads it back with
+// tcgen05.ld and writes the tile once. FP32 accuracy comes from the 3xTF32 split
+// a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi (a_hi = tf32(a), a_lo = tf32(a - a_hi)).
+// Every wait on the MMA completion barrier is bounded; a timeout sets an error flag
+// that the host turns into an error, and the CTA still frees its tensor memory.
+#pragma once
+
+#include <cstdint>
+
+#include "nufft_kernels.cuh"
+
+namespace bippb200 {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcVisits = 32;                 // visits per phase
+constexpr int kTcSteps = kTcVisits / 8;       // MMA K-steps per phase (K = 8 for tf32)
+constexpr int kTcM = kTX * kTY;               // 128 accumulator rows (cells)
+constexpr int kTcN = kTW * 8;                 // 64 accumulator columns (plane x channel x re/im)
+constexpr int kTcChan = 4;                    // channels handled by the tensor-core kernel
+constexpr int kTcCols = 64;                   // tensor-memory columns allocated per CTA
+constexpr int kTcMinBlocks = 4;               // CTAs per SM (shared memory and TMEM allow 4)
+// shared-memory layout (bytes); one K-step of A is 128 rows x 8 tf32, of B 64 rows x 8
+constexpr int kTcAStep = kTcM * 8 * 4;
+constexpr int kTcBStep = kTcN * 8 * 4;
+constexpr int kTcOffAhi = 0;
+constexpr int kTcOffAlo = kTcOffAhi + kTcSteps * kTcAStep;
+constexpr int kTcOffBhi = kTcOffAlo + kTcSteps * kTcAStep;
+constexpr int kTcOffBlo = kTcOffBhi + kTcSteps * kTcBStep;
+// per-visit kernel values at every tile position (zero outside the support) and values
+constexpr int kTcOffEx = kTcOffBlo + kTcSteps * kTcBStep;  // float [32][16]
+constexpr int kTcOffEy = kTcOffEx + kTcVisits * kTX * 4;   // float [32][8]
+constexpr int kTcOffEw = kTcOffEy + kTcVisits * kTY * 4;   // float [32][8]
+constexpr int kTcOffVal = kTcOffEw + kTcVisits * kTW * 4;  // float [32][8]
+constexpr int kTcSmem = kTcOffVal + kTcVisits * 8 * 4;
+static_assert(kTcM == 128 && kTcN == 64, "tile shape fixed by the MMA shape");
+static_assert(kTcOffEx % 1024 == 0, "operand blocks 1 KB aligned");
+static_assert(kTX == 16 && kTY == 8 && kTW == 8, "prep mapping assumes 16 x 8 x 8 tiles");
+
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 64, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                              ((uint32_t)(kTcM >> 4) << 24);
+// spin limit of one wait on the MMA barrier (each try_wait suspends for a bounded time)
+constexpr int kTcSpin = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor, canonical K-major layout without swizzle: 8-row core
+// matrices of 16 bytes per row (128 B contiguous), `sbo` between 8-row groups, `lbo`
+// between the two 16-byte K halves of a K-step; version 1 (sm_100)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// bounded wait for the completion of phase `parity` of the barrier
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < kTcSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// x = hi + lo with hi rounded to the 11 significant bits of tf32 (integer rounding of
+// the bit pattern, no conversion instruction) and lo = x - hi exact (|lo| <= 2^-11 |x|);
+// the tensor core reads lo's top 11 bits, so the split keeps ~22 significant bits
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  hi = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+  lo = x - hi;
+}
+
+// The 27 (source direction d, crossing bits) pairs whose key ranges reach a tile, in
+// the order tile_ranges() visits them: d in 0..7, bits a superset of d.
+__device__ __forceinline__ int tc_range_pair(int j) {
+  int n = 0;
+  for (int d = 0; d < 8; ++d)
+    for (int bits = 0; bits < 8; ++bits)
+      if ((bits & d) == d) {
+        if (n == j) return d | (bits << 3);
+        ++n;
+      }
+  return -1;
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, float a, float b, float c, float d) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&r)[16]) {
+  uint32_t u[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]), "=r"(u[8]),
+        "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) r[i] = __uint_as_float(u[i]);
+}
+
+// Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ...
+static __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks)
+spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
+                 const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
+                 int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmemSlot;
+  __shared__ int rBeg[27], rPre[28];
+  __shared__ int sOk;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t sbase = smem_u32(sm);
+  const uint32_t bar = smem_u32(&mbar);
+  float* ex = reinterpret_cast<float*>(sm + kTcOffEx);
+  float* ey = reinterpret_cast<float*>(sm + kTcOffEy);
+  float* ew = reinterpret_cast<float*>(sm + kTcOffEw);
+  float* val = reinterpret_cast<float*>(sm + kTcOffVal);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    sOk = 1;
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmemSlot)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmemSlot;
+  const uint32_t tmemWarp = tmem + ((uint32_t)(warp * 32) << 16);
+  const float invHalf = 2.0f / (float)g.W;
+  const int W = g.W;
+  const int xm = tid % kTX, ym = tid / kTX;   // cell of accumulator row tid
+  const int lane = tid & 31;
+  const int myPair = (lane < 27) ? tc_range_pair(lane) : -1;
+  uint32_t parity = 0;
+  bool pending = false;                       // a commit not yet waited for
+  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
+    const SpreadItem it = items[item];
+    const int tx = it.tile % g.ntx, ty = (it.tile / g.ntx) % g.nty, tw = it.tile / (g.ntx * g.nty);
+    const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
+    if (warp == 0) {
+      // lane j < 27: key range of pair j (empty when the source tile lies below w = 0)
+      int beg = 0, len = 0;
+      if (myPair >= 0) {
+        const int d = myPair & 7, bits = myPair >> 3;
+        const int stw = tw - ((d >> 2) & 1);
+        if (stw >= 0) {
+          const int stx = (tx - (d & 1) + g.ntx) % g.ntx;
+          const int sty = (ty - ((d >> 1) & 1) + g.nty) % g.nty;
+          const int key = ((stw * g.nty + sty) * g.ntx + stx) * 8 + bits;
+          beg = offsets[key];
+          len = offsets[key + 1] - beg;
+        }
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane < 27) {
+        rBeg[lane] = beg;
+        rPre[lane] = incl - len;
+      }
+      if (lane == 26) rPre[27] = incl;
+    }
+    __syncthreads();
+    const int lo = (int)((long long)it.load * it.part / it.nparts);
+    const int hi = (int)((long long)it.load * (it.part + 1) / it.nparts);
+    const int nvis = hi - lo;
+    int ri = 0;
+    for (int v0 = 0; v0 < nvis; v0 += kTcVisits) {
+      const int nk = min(kTcVisits, nvis - v0);
+      const int steps = (nk + 7) >> 3;
+      // the operands of the previous phase must have been consumed
+      if (tid == 0 && pending) {
+        if (mbar_wait(bar, parity)) {
+          parity ^= 1u;
+          pending = false;
+        } else {
+          sOk = 0;
+        }
+      }
+      // per-visit tables, thread (visit v, role a): a = 0/1: x positions 0-7 / 8-15,
+      // a = 2: y positions 0-7, a = 3: w planes 0-7 and the channel values
+      {
+        const int v = tid & 31, a = tid >> 5;
+        float* row = (a < 2) ? ex + v * kTX + a * 8 : (a == 2) ? ey + v * kTY : ew + v * kTW;
+        if (v < nk) {
+          const int q = lo + v0 + v;
+          while (q >= rPre[ri + 1]) ++ri;
+          const int p = rBeg[ri] + (q - rPre[ri]);
+          const PtRec pr = rec[p];
+          int l, first;
+          float d;
+          if (a < 2) {
+            l = pr.ix0 - x0;
+            l = ((l % g.nx) + g.nx) % g.nx;
+            if (l > g.nx / 2) l -= g.nx;
+            d = pr.dx;
+            first = a * 8;
+          } else if (a == 2) {
+            l = pr.iy0 - y0;
+            l = ((l % g.ny) + g.ny) % g.ny;
+            if (l > g.ny / 2) l -= g.ny;
+            d = pr.dy;
+            first = 0;
+          } else {
+            l = pr.iw0 - w0;
+            d = pr.dw;
+            first = 0;
+          }
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int j = first + i - l;   // support index of tile position first + i
+            row[i] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - d) * invHalf, g.beta) : 0.f;
+          }
+          if (a == 3) {
+#pragma unroll
+            for (int c = 0; c < kTcChan; ++c) {
+              const float2 x = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+              val[v * 8 + 2 * c] = x.x;
+              val[v * 8 + 2 * c + 1] = x.y;
+            }
+          }
+        } else if (v < steps * 8) {
+          // padding visits of the last K-step contribute nothing (values too: 0 x stale
+          // shared memory could be 0 x NaN)
+#pragma unroll
+          for (int i = 0; i < 8; ++i) row[i] = 0.f;
+          if (a == 3)
+            for (int c = 0; c < 8; ++c) val[v * 8 + c] = 0.f;
+        }
+      }
+      __syncthreads();
+      if (!sOk) break;
+      // A: row tid (cell xm, ym), 8 visits per K-step
+      for (int s = 0; s < steps; ++s) {
+        float h[8], l[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int v = s * 8 + k;
+          split_tf32(ex[v * kTX + xm] * ey[v * kTY + ym], h[k], l[k]);
+        }
+        const uint32_t ah = sbase + kTcOffAhi + s * kTcAStep + tid * 16;
+        const uint32_t al = sbase + kTcOffAlo + s * kTcAStep + tid * 16;
+        st_shared_v4(ah, h[0], h[1], h[2], h[3]);
+        st_shared_v4(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
+        st_shared_v4(al, l[0], l[1], l[2], l[3]);
+        st_shared_v4(al + kTcAStep / 2, l[4], l[5], l[6], l[7]);
+      }
+      // B: row n = plane * 8 + channel * 2 + (re|im), this thread's half of the K-step
+      {
+        const int n = tid & 63, kh = tid >> 6;
+        const int plane = n >> 3, cc = n & 7;
+        for (int s = 0; s < steps; ++s) {
+          float h[4], l[4];
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const int v = s * 8 + kh * 4 + kk;
+            split_tf32(ew[v * kTW + plane] * val[v * 8 + cc], h[kk], l[kk]);
+          }
+          const uint32_t bh = sbase + kTcOffBhi + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
+          const uint32_t bl = sbase + kTcOffBlo + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
+          st_shared_v4(bh, h[0], h[1], h[2], h[3]);
+          st_shared_v4(bl, l[0], l[1], l[2], l[3]);
+        }
+      }
+      // make the operand writes visible to the tensor core, then one thread issues
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        for (int s = 0; s < steps; ++s) {
+          const uint64_t dAh = tc_desc(sbase + kTcOffAhi + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dAl = tc_desc(sbase + kTcOffAlo + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dBh = tc_desc(sbase + kTcOffBhi + s * kTcBStep, kTcBStep / 2, 128);
+          const uint64_t dBl = tc_desc(sbase + kTcOffBlo + s * kTcBStep, kTcBStep / 2, 128);
+          tc_mma(tmem, dAh, dBh, (v0 > 0 || s > 0) ? 1u : 0u);
+          tc_mma(tmem, dAh, dBl, 1u);
+          tc_mma(tmem, dAl, dBh, 1u);
+        }
+        tc_commit(bar);
+        pending = true;
+      }
+    }
+    // accumulator complete
+    if (tid == 0 && pending) {
+      if (mbar_wait(bar, parity)) {
+        parity ^= 1u;
+        pending = false;
+      } else {
+        sOk = 0;
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!sOk) break;
+    if (nvis > 0) {
+      const int twl = tw - tw0;
+      const long long rowOff = (long long)(y0 + ym) * g.nx + (x0 + xm);
+      const long long planeStride = (long long)g.ny * g.nx;
+#pragma unroll
+      for (int q = 0; q < kTcN / 16; ++q) {
+        float r[16];
+        tmem_ld16(tmemWarp + (uint32_t)(q * 16), r);
+#pragma unroll
+        for (int pl = 0; pl < 2; ++pl) {
+          const int plane = twl * kTW + q * 2 + pl;
+#pragma unroll
+          for (int c = 0; c < kTcChan; ++c) {
+            if (c < nch) {
+              const float2 v = make_float2(r[pl * 8 + 2 * c], r[pl * 8 + 2 * c + 1]);
+              float2* dst = grid + ((long long)c * slabPlanes + plane) * planeStride + rowOff;
+              if (it.nparts == 1) {
+                *dst = v;
+              } else {
+                atomicAdd(&dst->x, v.x);
+                atomicAdd(&dst->y, v.y);
+              }
+            }
+          }
+        }
+      }
+    }
+    // tensor-memory reads done before the next tile's first MMA overwrites it
+    tc_fence_before();
+    __syncthreads();
+  }
+  // after a timeout: wait once more (bounded) for MMAs still in flight, then release
+  if (tid == 0) {
+    if (pending) mbar_wait(bar, parity);
+    if (!sOk) atomicOr(errFlag, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+  }
+}
+
+}  // namespace bippb200
