@@ -261,7 +261,30 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   }
   // 5. back-transform Y = Q Z -> T1
   mark(6);
-  {
+  if (Nmax <= kBtMaxRows) {
+    // blocked: T of each 16-reflector block into G's storage (free between the triangular
+    // inverse and the final GEMM), then one pass over Y per 16-column slice
+    C* Tblk = reinterpret_cast<C*>(G);
+    const long long tStride = n2 * (long long)(sizeof(double2) / sizeof(C));
+    const int nblk = (Nmax - 1 + kBtNB - 1) / kBtNB;
+    count_launch();
+    bt_larft_kernel<C, R><<<dim3(std::max(1, nblk), nb), 256, 0, st>>>(A, w.tau.template get<C>(), nred, Nmax, Tblk,
+                                                                       tStride);
+    B2_CHECK_LAUNCH();
+    const size_t smem = bt_apply_smem(Nmax, sizeof(C));
+    const dim3 grid((Nmax + kBtCB - 1) / kBtCB, nb);
+#define B2_BT(KR)                                                                            \
+  {                                                                                          \
+    auto k = bt_apply_kernel<C, R, KR>;                                                      \
+    smem_optin(k, smem);                                                                     \
+    count_launch();                                                                          \
+    k<<<grid, kBtApplyThreads, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1);             \
+  }
+    const int kr = (Nmax + kBtRG - 1) / kBtRG;
+    if (kr <= 2) B2_BT(2) else if (kr <= 4) B2_BT(4) else if (kr <= 6) B2_BT(6) else B2_BT(8)
+#undef B2_BT
+    B2_CHECK_LAUNCH();
+  } else {
     size_t smem16 = ((size_t)Nmax * 16 + Nmax + kBtThreads) * sizeof(C);
     if (smem16 <= ctx->maxSmemOptin) {
       auto k = backtransform_kernel<C, R, 16>;

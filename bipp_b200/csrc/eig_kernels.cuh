@@ -1023,4 +1023,225 @@ backtransform_kernel(const C* __restrict__ A, const C* __restrict__ taus, const 
   }
 }
 
+// ------------------------------------------------------------------------------------
+// blocked back-transform Y = Q Z (compact WY, LAPACK ?larft forward/columnwise + ?larfb)
+// ------------------------------------------------------------------------------------
+// Reflectors are applied 16 at a time: Q_k = H_i0 ... H_i0+15 = I - V T V^H, so
+// Y <- Y - V (T (V^H Y)) for the blocks k = last .. 0. bt_larft_kernel forms T per block
+// (one CTA per block and matrix); bt_apply_kernel keeps a 16-column slice of Y in
+// registers (thread: one column, every 16th row) for all blocks.
+constexpr int kBtNB = 16;             // reflectors per block
+constexpr int kBtCB = 16;             // columns of Y per CTA
+constexpr int kBtApplyThreads = 256;  // 16 row groups x 16 columns
+constexpr int kBtMaxRows = 512;       // Nmax limit of the register-resident kernel
+
+// element r of reflector i (v(i+1) = 1, stored below the subdiagonal of column i)
+template <typename C, typename R>
+__device__ __forceinline__ C bt_v(const C* __restrict__ Ab, int Nmax, int i, int r) {
+  if (r <= i) return mk(R(0), R(0));
+  if (r == i + 1) return mk(R(1), R(0));
+  return Ab[r + (long long)i * Nmax];
+}
+
+// T of every block of every matrix: Tout[b][k] is 16 x 16 (row-major, upper triangular)
+template <typename C, typename R>
+__global__ void __launch_bounds__(256)
+bt_larft_kernel(const C* __restrict__ A, const C* __restrict__ taus, const int* __restrict__ nred, int Nmax,
+                C* __restrict__ Tout, long long tStride) {
+  const int b = blockIdx.y, k = blockIdx.x;
+  const int n = nred[b];
+  const int i0 = k * kBtNB;
+  if (i0 >= n - 1) return;
+  const int nbk = min(kBtNB, n - 1 - i0);
+  const C* Ab = A + (long long)b * Nmax * Nmax;
+  const C* tb = taus + (long long)b * Nmax;
+  __shared__ C gv[kBtNB][kBtNB];   // gv[l][j] = v_l^H v_j (l < j)
+  __shared__ C T[kBtNB][kBtNB];
+  __shared__ C t[kBtNB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int e = tid; e < kBtNB * kBtNB; e += blockDim.x) {
+    T[e / kBtNB][e % kBtNB] = mk(R(0), R(0));
+    gv[e / kBtNB][e % kBtNB] = mk(R(0), R(0));
+  }
+  __syncthreads();
+  // pairs (l, j), l < j < nbk, one warp per pair; rows from the start of v_j
+  for (int pr = warp; pr < nbk * nbk; pr += nwarp) {
+    const int l = pr / nbk, j = pr % nbk;
+    if (l >= j) continue;
+    C acc = mk(R(0), R(0));
+    for (int r = i0 + j + 1 + lane; r < n; r += 32)
+      cfma_cj(acc, bt_v<C, R>(Ab, Nmax, i0 + l, r), bt_v<C, R>(Ab, Nmax, i0 + j, r));
+    acc.x = warp_sum(acc.x);
+    acc.y = warp_sum(acc.y);
+    if (lane == 0) gv[l][j] = acc;
+  }
+  __syncthreads();
+  for (int j = 0; j < nbk; ++j) {
+    const C tauj = tb[i0 + j];
+    if (tid < j) t[tid] = cmul(mk(-tauj.x, -tauj.y), gv[tid][j]);
+    __syncthreads();
+    if (tid < j) {
+      C acc = mk(R(0), R(0));
+      for (int q = tid; q < j; ++q) cfma(acc, T[tid][q], t[q]);
+      T[tid][j] = acc;
+    }
+    if (tid == 0) T[j][j] = tauj;
+    __syncthreads();
+  }
+  C* To = Tout + (long long)b * tStride + (long long)k * kBtNB * kBtNB;
+  for (int e = tid; e < kBtNB * kBtNB; e += blockDim.x) To[e] = T[e / kBtNB][e % kBtNB];
+}
+
+// Thread (row group rg = tid / 4, column group cg = tid % 4) holds Y rows rg + 64 q and
+// columns 4 cg .. 4 cg + 3 of the CTA's 16-column slice: every V element loaded from
+// shared memory feeds 4 columns. V^H Y partial sums are reduced over the 8 row groups
+// of a warp with shuffles, then over the 8 warps in shared memory.
+constexpr int kBtRG = kBtApplyThreads / 4;   // 64 row groups
+constexpr int kBtVS = kBtNB + 2;             // padded row stride of the V block (16-byte aligned rows)
+constexpr int kBtJC = 2;                     // reflectors per register chunk
+
+template <typename C, typename R, int KR>
+__global__ void __launch_bounds__(kBtApplyThreads, sizeof(C) == 8 ? 2 : 1)
+bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tStride, const R* __restrict__ Z,
+                const int* __restrict__ nred, int Nmax, C* __restrict__ Y) {
+  const int b = blockIdx.y;
+  const int n = nred[b];
+  const int c0 = blockIdx.x * kBtCB;
+  if (c0 >= n) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* Vs = reinterpret_cast<C*>(smem_raw);              // [Nmax][kBtVS] block of reflectors (row-major)
+  C* red = Vs + (long long)Nmax * kBtVS;               // [8 warps][16 j][16 c]
+  C* Ts = red + 8 * kBtNB * kBtCB;                     // [16][16]
+  C* Wt = Ts + kBtNB * kBtNB;                          // [16 j][16 c]
+  const C* Ab = A + (long long)b * Nmax * Nmax;
+  const R* Zb = Z + (long long)b * Nmax * Nmax;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cg = tid & 3, rg = tid >> 2;
+  C y[KR][4];
+#pragma unroll
+  for (int q = 0; q < KR; ++q) {
+    const int r = rg + kBtRG * q;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int col = c0 + 4 * cg + u;
+      // Z (tridiagonal eigenvectors) is row-major: Z(r, col) at r * Nmax + col
+      y[q][u] = mk((r < n && col < n) ? Zb[(long long)r * Nmax + col] : R(0), R(0));
+    }
+  }
+  const int nblk = (n - 1 + kBtNB - 1) / kBtNB;
+  for (int k = nblk - 1; k >= 0; --k) {
+    const int i0 = k * kBtNB;
+    const int nbk = min(kBtNB, n - 1 - i0);
+    const int m = n - i0 - 1;
+    for (int e = tid; e < m * kBtNB; e += blockDim.x) {
+      const int r = i0 + 1 + e % m, j = e / m;
+      Vs[r * kBtVS + j] = (j < nbk) ? bt_v<C, R>(Ab, Nmax, i0 + j, r) : mk(R(0), R(0));
+    }
+    const C* Tk = Tin + (long long)b * tStride + (long long)k * kBtNB * kBtNB;
+    for (int e = tid; e < kBtNB * kBtNB; e += blockDim.x) {
+      const int row = e / kBtNB, cc = e % kBtNB;
+      Ts[e] = (row < nbk && cc < nbk) ? Tk[e] : mk(R(0), R(0));
+    }
+    __syncthreads();
+    // W = V^H Y, kBtJC reflectors at a time
+#pragma unroll
+    for (int jc = 0; jc < kBtNB / kBtJC; ++jc) {
+      C w[kBtJC][4];
+#pragma unroll
+      for (int a = 0; a < kBtJC; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) w[a][u] = mk(R(0), R(0));
+#pragma unroll
+      for (int q = 0; q < KR; ++q) {
+        const int r = rg + kBtRG * q;
+        if (r > i0 && r < n) {
+          C v[kBtJC];
+#pragma unroll
+          for (int a = 0; a < kBtJC; ++a) v[a] = Vs[r * kBtVS + kBtJC * jc + a];
+#pragma unroll
+          for (int a = 0; a < kBtJC; ++a)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cfma_cj(w[a][u], v[a], y[q][u]);
+        }
+      }
+      // sum over the 8 row groups of the warp (lane bits 2..4)
+#pragma unroll
+      for (int a = 0; a < kBtJC; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+          for (int o = 4; o < 32; o <<= 1) {
+            w[a][u].x += __shfl_xor_sync(0xffffffffu, w[a][u].x, o);
+            w[a][u].y += __shfl_xor_sync(0xffffffffu, w[a][u].y, o);
+          }
+        }
+      if (lane < 4) {
+#pragma unroll
+        for (int a = 0; a < kBtJC; ++a)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) red[(warp * kBtNB + kBtJC * jc + a) * kBtCB + 4 * cg + u] = w[a][u];
+      }
+    }
+    __syncthreads();
+    // W[j][c] over the 8 warps, then Wt = T W (thread = (j, c))
+    {
+      const int j = tid / kBtCB, c = tid % kBtCB;
+      C s0 = mk(R(0), R(0));
+#pragma unroll
+      for (int g = 0; g < 8; ++g) s0 = s0 + red[(g * kBtNB + j) * kBtCB + c];
+      __syncthreads();
+      red[j * kBtCB + c] = s0;
+      __syncthreads();
+      C t = mk(R(0), R(0));
+      for (int l = j; l < kBtNB; ++l) cfma(t, Ts[j * kBtNB + l], red[l * kBtCB + c]);
+      Wt[j * kBtCB + c] = t;
+    }
+    __syncthreads();
+    // Y -= V Wt, kBtJC reflectors at a time
+#pragma unroll
+    for (int jc = 0; jc < kBtNB / kBtJC; ++jc) {
+      C wt[kBtJC][4];
+#pragma unroll
+      for (int a = 0; a < kBtJC; ++a)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) wt[a][u] = Wt[(kBtJC * jc + a) * kBtCB + 4 * cg + u];
+#pragma unroll
+      for (int q = 0; q < KR; ++q) {
+        const int r = rg + kBtRG * q;
+        if (r > i0 && r < n) {
+          C v[kBtJC];
+#pragma unroll
+          for (int a = 0; a < kBtJC; ++a) v[a] = Vs[r * kBtVS + kBtJC * jc + a];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            C acc = y[q][u];
+#pragma unroll
+            for (int a = 0; a < kBtJC; ++a) {
+              acc.x -= v[a].x * wt[a][u].x - v[a].y * wt[a][u].y;
+              acc.y -= v[a].x * wt[a][u].y + v[a].y * wt[a][u].x;
+            }
+            y[q][u] = acc;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  C* Yb = Y + (long long)b * Nmax * Nmax;
+#pragma unroll
+  for (int q = 0; q < KR; ++q) {
+    const int r = rg + kBtRG * q;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int col = c0 + 4 * cg + u;
+      if (r < n && col < n) Yb[r + (long long)col * Nmax] = y[q][u];
+    }
+  }
+}
+
+// shared memory of bt_apply_kernel
+constexpr size_t bt_apply_smem(int Nmax, size_t complexBytes) {
+  return ((size_t)Nmax * kBtVS + 8 * kBtNB * kBtCB + kBtNB * kBtNB + kBtNB * kBtCB) * complexBytes;
+}
+
 }  // namespace bippb200

@@ -285,6 +285,20 @@ static bool use_tensor_core_spread(int nch) {
 // dense core of the uv plane (short baselines)
 constexpr int kSpreadCap = 4096;
 
+// exclusive scan of n ints on the stream; out[n] = total
+void NufftCore::exclusive_scan(const int* in, int* out, long long n) {
+  const long long per = (long long)kScanThreads * kScanItems;
+  const int nb = (int)((n + per - 1) / per);
+  itemSums_.ensure(ctx_, (nb + 1) * sizeof(int));
+  count_launch();
+  scan_partial_kernel<<<nb, kScanThreads, 0, ctx_->stream>>>(in, out, n, itemSums_.get<int>());
+  count_launch();
+  scan_blocksums_kernel<<<1, 1024, 0, ctx_->stream>>>(itemSums_.get<int>(), nb, out + n);
+  count_launch();
+  scan_add_kernel<<<nb, 1024, 0, ctx_->stream>>>(out, n, itemSums_.get<int>(), nullptr);
+  B2_CHECK_LAUNCH();
+}
+
 void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const long long P = num_pixels();
   const size_t planeBytes = (size_t)g_.nx * g_.ny * sizeof(float2);
@@ -303,44 +317,59 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const int slabPlanes = slabTiles * kTW;
   grid_.ensure(ctx_, (size_t)nch_ * slabPlanes * planeBytes);
   B2_CUDA(cudaMemsetAsync(acc_.get(), 0, (size_t)nch_ * P * sizeof(float2), ctx_->stream));
-  // per-tile loads -> work items (non-empty tiles, heavy tiles split), grouped by slab
+  // per-tile loads -> work items (non-empty tiles, heavy tiles split in parts), built on
+  // the device: parts per tile, exclusive scan -> item offsets, fill; tiles are numbered
+  // slab by slab, so a slab's items are one contiguous range
   const int ntiles = g_.ntx * g_.nty * g_.ntw;
   load_.ensure(ctx_, (size_t)ntiles * sizeof(int));
+  parts_.ensure(ctx_, (size_t)ntiles * sizeof(int));
+  itemOff_.ensure(ctx_, (size_t)(ntiles + 1) * sizeof(int));
+  // the tensor-core spreader writes every tile it spreads in one part; the other tiles of a
+  // slab (empty, or split into parts that accumulate with atomics) are cleared first from
+  // a compact list; the warp spreader works on a cleared slab
+  const bool tc = use_tensor_core_spread(nch_);
+  const int tb = std::min(8192, (ntiles + 255) / 256);
+  clearFlag_.ensure(ctx_, (size_t)ntiles * sizeof(int));
+  clearOff_.ensure(ctx_, (size_t)(ntiles + 1) * sizeof(int));
+  clearList_.ensure(ctx_, (size_t)std::max(1, ntiles) * sizeof(int));
   count_launch();
-  tile_load_kernel<<<std::min(4096, (ntiles + 255) / 256), 256, 0, ctx_->stream>>>(g_, offsets_.get<int>(),
-                                                                                   load_.get<int>());
+  tile_load_kernel<<<tb, 256, 0, ctx_->stream>>>(g_, offsets_.get<int>(), load_.get<int>());
+  count_launch();
+  tile_parts_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), kSpreadCap, parts_.get<int>(),
+                                                  clearFlag_.get<int>());
   B2_CHECK_LAUNCH();
-  std::vector<int> loads(ntiles);
-  d2h(ctx_, loads.data(), load_.get(), (size_t)ntiles * sizeof(int));
-  sync(ctx_);
-  std::vector<SpreadItem> items;
-  std::vector<int> slabBegin(nslab + 1, 0);
-  const int tilesPerPlaneSet = g_.ntx * g_.nty;
-  for (int sl = 0; sl < nslab; ++sl) {
-    slabBegin[sl] = (int)items.size();
-    const int t0 = sl * slabTiles * tilesPerPlaneSet;
-    const int t1 = std::min(ntiles, (sl + 1) * slabTiles * tilesPerPlaneSet);
-    for (int t = t0; t < t1; ++t) {
-      const int ld = loads[t];
-      if (!ld) continue;
-      const int np = (ld + kSpreadCap - 1) / kSpreadCap;
-      for (int q = 0; q < np; ++q) items.push_back(SpreadItem{t, q, np, ld});
-    }
+  exclusive_scan(parts_.get<int>(), itemOff_.get<int>(), ntiles);
+  if (tc) {
+    exclusive_scan(clearFlag_.get<int>(), clearOff_.get<int>(), ntiles);
+    count_launch();
+    clear_list_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, clearFlag_.get<int>(), clearOff_.get<int>(),
+                                                    clearList_.get<int>());
+    B2_CHECK_LAUNCH();
   }
-  slabBegin[nslab] = (int)items.size();
+  const int tilesPerPlaneSet = g_.ntx * g_.nty;
+  std::vector<int> slabBegin(nslab + 1, 0), clearBegin(nslab + 1, 0);
+  for (int sl = 0; sl <= nslab; ++sl) {
+    const int t = std::min(ntiles, sl * slabTiles * tilesPerPlaneSet);
+    d2h(ctx_, &slabBegin[sl], itemOff_.get<int>() + t, sizeof(int));
+    if (tc) d2h(ctx_, &clearBegin[sl], clearOff_.get<int>() + t, sizeof(int));
+  }
+  sync(ctx_);
+  const int nItemsAll = slabBegin[nslab];
+  items_.ensure(ctx_, std::max<size_t>(1, (size_t)nItemsAll) * sizeof(SpreadItem));
+  count_launch();
+  item_fill_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), parts_.get<int>(), itemOff_.get<int>(),
+                                                 items_.get<SpreadItem>());
+  B2_CHECK_LAUNCH();
   {
     int total = 0;
     d2h(ctx_, &total, offsets_.get<int>() + nkeys_, sizeof(int));
     sync(ctx_);
     lastPoints = total;
     lastSlabs = nslab;
-    lastItems = (long long)items.size();
+    lastItems = nItemsAll;
     lastGridBytes = (long long)g_.ntw * kTW * (long long)planeBytes * nch_;
   }
-  items_.ensure(ctx_, std::max<size_t>(1, items.size()) * sizeof(SpreadItem));
-  h2d(ctx_, items_.get(), items.data(), items.size() * sizeof(SpreadItem));
   const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);
-  const bool tc = use_tensor_core_spread(nch_);
   errFlag_.ensure(ctx_, sizeof(int));
   B2_CUDA(cudaMemsetAsync(errFlag_.get(), 0, sizeof(int), ctx_->stream));
   cudaEvent_t ev[5];
@@ -352,7 +381,14 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     const int tiles = std::min(slabTiles, g_.ntw - tw0);
     const int nItems = slabBegin[sl + 1] - slabBegin[sl];
     if (stageMs) B2_CUDA(cudaEventRecord(ev[4], ctx_->stream));
-    B2_CUDA(cudaMemsetAsync(grid_.get(), 0, (size_t)nch_ * slabPlanes * planeBytes, ctx_->stream));
+    if (!tc) {
+      B2_CUDA(cudaMemsetAsync(grid_.get(), 0, (size_t)nch_ * slabPlanes * planeBytes, ctx_->stream));
+    } else if (clearBegin[sl + 1] > clearBegin[sl]) {
+      count_launch();
+      clear_tiles_kernel<<<clearBegin[sl + 1] - clearBegin[sl], kTcThreads, 0, ctx_->stream>>>(
+          g_, clearList_.get<int>() + clearBegin[sl], tw0, slabPlanes, nch_, grid_.get<float2>());
+      B2_CHECK_LAUNCH();
+    }
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
     if (nItems > 0 && tc) {
       launch_spread_tc(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),

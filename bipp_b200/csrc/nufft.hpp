@@ -72,10 +72,11 @@ private:
   double su_ = 1, sv_ = 1;
   long long nkeys_ = 0, valStride_ = 0;
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
-  DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_;
+  DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
   std::map<int, cufftHandle> plans_;
   int slabTiles_ = 1;
   cufftHandle plan_for(int batch);
+  void exclusive_scan(const int* in, int* out, long long n);
 
 public:
   ~NufftCore();

@@ -427,6 +427,33 @@ static __global__ void tile_load_kernel(NufftGeom g, const int* __restrict__ off
   }
 }
 
+// spreading parts of each tile (ceil(load / cap), 0 when empty) and whether the tile has
+// to be cleared before spreading (empty, or spread in several parts that accumulate)
+static __global__ void tile_parts_kernel(int ntiles, const int* __restrict__ load, int cap, int* __restrict__ parts,
+                                         int* __restrict__ clearFlag) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int np = (load[t] + cap - 1) / cap;
+    parts[t] = np;
+    clearFlag[t] = (np != 1) ? 1 : 0;
+  }
+}
+
+// tiles to clear, compacted in tile order (offsets from an exclusive scan of the flags)
+static __global__ void clear_list_kernel(int ntiles, const int* __restrict__ clearFlag, const int* __restrict__ off,
+                                         int* __restrict__ list) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x)
+    if (clearFlag[t]) list[off[t]] = t;
+}
+
+// work items of every tile at its exclusive-scan offset
+static __global__ void item_fill_kernel(int ntiles, const int* __restrict__ load, const int* __restrict__ parts,
+                                        const int* __restrict__ itemOff, SpreadItem* __restrict__ items) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int np = parts[t];
+    for (int q = 0; q < np; ++q) items[itemOff[t] + q] = SpreadItem{t, q, np, load[t]};
+  }
+}
+
 // swizzled cell index inside the tile: x is rotated by W * (y / 2) so that the W x W
 // footprint of a point covers distinct banks
 __device__ __forceinline__ int tile_cell(int x, int y, int w, int W) {

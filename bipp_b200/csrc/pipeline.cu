@@ -121,6 +121,7 @@ struct bipp_pipeline_s {
   EigWork<float> eig;
   DevBuf basis, intervalsD;
   DevBuf S, xyz, xyzT, wl, antUVW, uvwScale, wrange;
+  const float2* Sin = nullptr;   // visibilities of the current call (caller's device memory or S)
   DevBuf idx, nred, nvis, status, lam, kscale, kbeg, kend, vv, pairOff;
   DevBuf images;
   long long stepsDone = 0;
@@ -170,7 +171,7 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
   if (!scatterOnly) {
     EigLaunch<float> E{};
     E.nBatch = nb; E.nBeam = N; E.nAnt = N; E.Nmax = N;
-    E.S = p->S.get<float2>() + (long long)s0 * n2; E.sStride = n2; E.lds = N;
+    E.S = p->Sin + (long long)s0 * n2; E.sStride = n2; E.lds = N;
     E.xyz = p->xyzT.get<double>(); E.xyzStride = 3ll * N; E.ldxyz = N; E.wl = p->wl.get<double>();
     E.mode = 0; E.eps = std::numeric_limits<float>::epsilon(); E.gram = true; E.identityW = true;
     E.idx = p->idx.get<int>(); E.nred = p->nred.get<int>(); E.nvis = p->nvis.get<long long>();
@@ -287,7 +288,13 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   if (p->timing) { cudaEventCreate(&ev0); cudaEventCreate(&ev1); cudaEventRecord(ev0, ctx->stream); }
   // inputs
   const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  B2_CUDA(cudaMemcpyAsync(p->S.get(), s, (size_t)T * n2 * sizeof(float2), kind, ctx->stream));
+  // device inputs are read in place; host inputs are staged in S
+  if (onDevice) {
+    p->Sin = static_cast<const float2*>(s);
+  } else {
+    B2_CUDA(cudaMemcpyAsync(p->S.get(), s, (size_t)T * n2 * sizeof(float2), kind, ctx->stream));
+    p->Sin = p->S.get<float2>();
+  }
   B2_CUDA(cudaMemcpyAsync(p->xyz.get(), xyz, (size_t)T * N * 3 * sizeof(double), kind, ctx->stream));
   B2_CUDA(cudaMemcpyAsync(p->wl.get(), wl, (size_t)T * sizeof(double), kind, ctx->stream));
   count_launch();
@@ -303,7 +310,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     auto k = prep_kernel<float>;
     smem_optin(k, smem);
     count_launch();
-    k<<<T, kPrepThreads, smem, ctx->stream>>>(N, p->S.get<float2>(), n2, N, p->xyzT.get<double>(), 3ll * N, N,
+    k<<<T, kPrepThreads, smem, ctx->stream>>>(N, p->Sin, n2, N, p->xyzT.get<double>(), 3ll * N, N,
                                               p->wl.get<double>(), 0, std::numeric_limits<float>::epsilon(), 1, N,
                                               p->idx.get<int>(), p->nred.get<int>(), p->nvis.get<long long>(),
                                               nullptr, nullptr, p->status.get<int>(), 1, 0, 0);

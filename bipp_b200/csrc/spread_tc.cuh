@@ -4,7 +4,7 @@
 // separable outer products over the points ("visits") that reach the tile:
 //     G[(x,y), (w,c)] = sum_p  phi_x,p(x) phi_y,p(y)  *  phi_w,p(w) v_p,c
 // i.e. the product of A (128 cells x K visits) and B (K visits x 64 columns: 8 planes x
-// 4 channels x re/im). Threads write A and B for 32 visits at a time into shared memory
+// 4 channels x re/im). Threads write A and B for 16 visits at a time into shared memory
 // (canonical K-major, no swizzle), one thread issues tcgen05.mma (kind::tf32) into a
 // 128 x 64 FP32 accumulator in tensor memory, and the epilogue reads it back with
 // tcgen05.ld and writes the tile once. FP32 accuracy comes from the 3xTF32 split
@@ -20,13 +20,13 @@
 namespace bippb200 {
 
 constexpr int kTcThreads = 128;
-constexpr int kTcVisits = 32;                 // visits per phase
+constexpr int kTcVisits = 16;                 // visits per phase
 constexpr int kTcSteps = kTcVisits / 8;       // MMA K-steps per phase (K = 8 for tf32)
 constexpr int kTcM = kTX * kTY;               // 128 accumulator rows (cells)
 constexpr int kTcN = kTW * 8;                 // 64 accumulator columns (plane x channel x re/im)
 constexpr int kTcChan = 4;                    // channels handled by the tensor-core kernel
 constexpr int kTcCols = 64;                   // tensor-memory columns allocated per CTA
-constexpr int kTcMinBlocks = 4;               // CTAs per SM (shared memory and TMEM allow 4)
+constexpr int kTcMinBlocks = 8;               // CTAs per SM (8 x 64 TMEM columns = all 512)
 // shared-memory layout (bytes); one K-step of A is 128 rows x 8 tf32, of B 64 rows x 8
 constexpr int kTcAStep = kTcM * 8 * 4;
 constexpr int kTcBStep = kTcN * 8 * 4;
@@ -34,15 +34,20 @@ constexpr int kTcOffAhi = 0;
 constexpr int kTcOffAlo = kTcOffAhi + kTcSteps * kTcAStep;
 constexpr int kTcOffBhi = kTcOffAlo + kTcSteps * kTcAStep;
 constexpr int kTcOffBlo = kTcOffBhi + kTcSteps * kTcBStep;
-// per-visit kernel values at every tile position (zero outside the support) and values
-constexpr int kTcOffEx = kTcOffBlo + kTcSteps * kTcBStep;  // float [32][16]
-constexpr int kTcOffEy = kTcOffEx + kTcVisits * kTX * 4;   // float [32][8]
-constexpr int kTcOffEw = kTcOffEy + kTcVisits * kTY * 4;   // float [32][8]
-constexpr int kTcOffVal = kTcOffEw + kTcVisits * kTW * 4;  // float [32][8]
-constexpr int kTcSmem = kTcOffVal + kTcVisits * 8 * 4;
+// per-visit kernel values at every tile position (zero outside the support) and the
+// channel values, stored position-major with a padded visit stride (conflict-free both
+// when a thread per visit writes them and when a thread per cell reads them)
+constexpr int kTcVS = kTcVisits + 1;
+constexpr int kTcOffEx = kTcOffBlo + kTcSteps * kTcBStep;  // float [16 x][kTcVS]
+constexpr int kTcOffEy = kTcOffEx + kTX * kTcVS * 4;       // float [8 y][kTcVS]
+constexpr int kTcOffEw = kTcOffEy + kTY * kTcVS * 4;       // float [8 w][kTcVS]
+constexpr int kTcOffVal = kTcOffEw + kTW * kTcVS * 4;      // float [8 (channel, re/im)][kTcVS]
+constexpr int kTcSmem = kTcOffVal + 8 * kTcVS * 4;
 static_assert(kTcM == 128 && kTcN == 64, "tile shape fixed by the MMA shape");
 static_assert(kTcOffEx % 1024 == 0, "operand blocks 1 KB aligned");
-static_assert(kTX == 16 && kTY == 8 && kTW == 8, "prep mapping assumes 16 x 8 x 8 tiles");
+static_assert(kTcMinBlocks * (kTcSmem + 512 + 1024) <= 233472, "shared memory (dynamic + static <= 512 B + 1 KB reserved) for kTcMinBlocks CTAs per SM");
+static_assert(kTcMinBlocks * kTcCols <= 512, "tensor memory for kTcMinBlocks CTAs per SM");
+static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mapping assumes 16 x 8 x 8 tiles, 16 visits");
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 64, M = 128
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
@@ -139,7 +144,7 @@ static __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                  int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+  extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmemSlot;
   __shared__ int rBeg[27], rPre[28];
@@ -221,11 +226,11 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           sOk = 0;
         }
       }
-      // per-visit tables, thread (visit v, role a): a = 0/1: x positions 0-7 / 8-15,
-      // a = 2: y positions 0-7, a = 3: w planes 0-7 and the channel values
+      // per-visit tables, thread (visit v, role a): a = 0..3: x positions 4a..4a+3,
+      // a = 4, 5: y positions, a = 6, 7: w planes 4(a-6)..+3 and channels 2(a-6), 2(a-6)+1
       {
-        const int v = tid & 31, a = tid >> 5;
-        float* row = (a < 2) ? ex + v * kTX + a * 8 : (a == 2) ? ey + v * kTY : ew + v * kTW;
+        const int v = tid & 15, a = tid >> 4;
+        float* tab = (a < 4) ? ex + (4 * a) * kTcVS : (a < 6) ? ey + (4 * (a - 4)) * kTcVS : ew + (4 * (a - 6)) * kTcVS;
         if (v < nk) {
           const int q = lo + v0 + v;
           while (q >= rPre[ri + 1]) ++ri;
@@ -233,43 +238,44 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           const PtRec pr = rec[p];
           int l, first;
           float d;
-          if (a < 2) {
+          if (a < 4) {
             l = pr.ix0 - x0;
             l = ((l % g.nx) + g.nx) % g.nx;
             if (l > g.nx / 2) l -= g.nx;
             d = pr.dx;
-            first = a * 8;
-          } else if (a == 2) {
+            first = 4 * a;
+          } else if (a < 6) {
             l = pr.iy0 - y0;
             l = ((l % g.ny) + g.ny) % g.ny;
             if (l > g.ny / 2) l -= g.ny;
             d = pr.dy;
-            first = 0;
+            first = 4 * (a - 4);
           } else {
             l = pr.iw0 - w0;
             d = pr.dw;
-            first = 0;
+            first = 4 * (a - 6);
           }
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
+          for (int i = 0; i < 4; ++i) {
             const int j = first + i - l;   // support index of tile position first + i
-            row[i] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - d) * invHalf, g.beta) : 0.f;
+            tab[i * kTcVS + v] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - d) * invHalf, g.beta) : 0.f;
           }
-          if (a == 3) {
+          if (a >= 6) {
 #pragma unroll
-            for (int c = 0; c < kTcChan; ++c) {
+            for (int cc = 0; cc < 2; ++cc) {
+              const int c = 2 * (a - 6) + cc;
               const float2 x = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
-              val[v * 8 + 2 * c] = x.x;
-              val[v * 8 + 2 * c + 1] = x.y;
+              val[(2 * c) * kTcVS + v] = x.x;
+              val[(2 * c + 1) * kTcVS + v] = x.y;
             }
           }
         } else if (v < steps * 8) {
           // padding visits of the last K-step contribute nothing (values too: 0 x stale
           // shared memory could be 0 x NaN)
 #pragma unroll
-          for (int i = 0; i < 8; ++i) row[i] = 0.f;
-          if (a == 3)
-            for (int c = 0; c < 8; ++c) val[v * 8 + c] = 0.f;
+          for (int i = 0; i < 4; ++i) tab[i * kTcVS + v] = 0.f;
+          if (a >= 6)
+            for (int c = 4 * (a - 6); c < 4 * (a - 6) + 4; ++c) val[c * kTcVS + v] = 0.f;
         }
       }
       __syncthreads();
@@ -280,7 +286,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int v = s * 8 + k;
-          split_tf32(ex[v * kTX + xm] * ey[v * kTY + ym], h[k], l[k]);
+          split_tf32(ex[xm * kTcVS + v] * ey[ym * kTcVS + v], h[k], l[k]);
         }
         const uint32_t ah = sbase + kTcOffAhi + s * kTcAStep + tid * 16;
         const uint32_t al = sbase + kTcOffAlo + s * kTcAStep + tid * 16;
@@ -298,7 +304,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
             const int v = s * 8 + kh * 4 + kk;
-            split_tf32(ew[v * kTW + plane] * val[v * 8 + cc], h[kk], l[kk]);
+            split_tf32(ew[plane * kTcVS + v] * val[cc * kTcVS + v], h[kk], l[kk]);
           }
           const uint32_t bh = sbase + kTcOffBhi + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
           const uint32_t bl = sbase + kTcOffBlo + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
@@ -379,6 +385,21 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
   }
+}
+
+// Clear the listed tiles of one slab (empty tiles and tiles spread in several parts):
+// one CTA per listed tile, thread = cell, a 128-byte row of the tile per warp store
+static __global__ void __launch_bounds__(kTcThreads)
+clear_tiles_kernel(NufftGeom g, const int* __restrict__ list, int tw0, int slabPlanes, int nch,
+                   float2* __restrict__ grid) {
+  const int t = list[blockIdx.x];
+  const int tx = t % g.ntx, ty = (t / g.ntx) % g.nty, tw = t / (g.ntx * g.nty);
+  const int xm = threadIdx.x % kTX, ym = threadIdx.x / kTX;
+  const long long planeStride = (long long)g.ny * g.nx;
+  float2* p = grid + (long long)(tw - tw0) * kTW * planeStride + (long long)(ty * kTY + ym) * g.nx + (tx * kTX + xm);
+  for (int c = 0; c < nch; ++c)
+#pragma unroll
+    for (int pl = 0; pl < kTW; ++pl) p[((long long)c * slabPlanes + pl) * planeStride] = make_float2(0.f, 0.f);
 }
 
 }  // namespace bippb200

@@ -242,8 +242,9 @@ BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipel
                                                 bipp_pipeline_t* pipeline);
 /* Process nSteps time steps: s [nSteps][nAntenna x nAntenna] complex float (lower triangle
  * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. onDevice != 0: the
- * three pointers are device pointers, else host pointers (copied in by the call). The
- * steps' contributions are accumulated into the images. */
+ * three pointers are device pointers (s is read in place, not modified), else host
+ * pointers (copied in by the call). The steps' contributions are accumulated into the
+ * images. */
 BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s,
                                                  const double* xyz, const double* wl, int onDevice);
 /* Images [nLevels][nPixel] (normalised by the number of processed steps if normalize),
