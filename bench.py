@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stages", action="store_true", help="report per-stage device times")
+    ap.add_argument("--plain-steps", type=int, default=16,
+                    help="time steps of the plain-GPU comparison (one NUFFT per step and level); 0 skips it")
     return ap.parse_args()
 
 
@@ -362,6 +364,26 @@ def main():
                                           "tridiag_fp64", "backtransform", "x_gemm"], [round(float(x), 3) for x in kt]))
         roof = spread_roofline(pl.nufft_stats(), float(st[3]), cfg.n_levels)
 
+    # the plain GPU form of the metric on a bounded sample: the same kernels, one step at a
+    # time and one NUFFT per step and level (no batching across steps or levels)
+    plain = None
+    if rank == 0 and args.plain_steps > 0 and args.mode == "batched":
+        ns = min(args.plain_steps, T)
+        pp = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
+                           tolerance=cfg.eps, chunk_steps=1, max_steps=ns, mode="plain")
+        pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())  # warm-up
+        pp.reset()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pv = ns / (p0.elapsed_time(p1) / 1000.0)
+        plain = {"value": pv, "unit": UNIT, "sample": f"first {ns} time steps of the batch",
+                 "chosen_over_plain": value / pv}
+        pp.close()
+
     # end to end through the public API: pinned host inputs copied in every step,
     # images read back every step
     e2e = None
@@ -411,7 +433,7 @@ def main():
                            "time_steps_per_batch": T, "mode": args.mode, "parallelism": f"dp{world} (steps)",
                            "l2": "inputs (4.3 GB/batch) larger than L2; no flush"},
                 "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,
-                "cpu_baseline": cpu, "roofline": roof}
+                "cpu_baseline": cpu, "roofline": roof, "plain_gpu": plain}
         print(json.dumps(line))
     pl.close()
     ctx.close()
