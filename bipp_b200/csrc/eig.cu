@@ -185,9 +185,10 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     auto k = prep_kernel<T>;
     smem_optin(k, smem);
     count_launch();
+    // W = I: the Gram matrix is real symmetric, stored as FP64 reals (withGram 2)
     k<<<nb, kPrepThreads, smem, st>>>(L.nBeam, L.S, L.sStride, L.lds, L.xyz, L.xyzStride, L.ldxyz, L.wl, L.mode,
-                                      L.eps, L.gram && L.identityW, Nmax, L.idx, L.nred, L.nvis, A, G, L.status,
-                                      L.doFlag, 1, L.batchOffset);
+                                      L.eps, (L.gram && L.identityW) ? 2 : 0, Nmax, L.idx, L.nred, L.nvis, A, G,
+                                      L.status, L.doFlag, 1, L.batchOffset);
     B2_CHECK_LAUNCH();
   }
   if (L.gram && !L.identityW) {
@@ -205,18 +206,37 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     B2_CHECK_LAUNCH();
   }
   const int tiles = (Nmax + kGemmBM - 1) / kGemmBM;
+  const bool realG = L.gram && L.identityW;
   if (L.gram) {
     mark(1);
-    smem_optin(cholesky_kernel, kCholSmem);
-    count_launch();
-    cholesky_kernel<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset);
+    if (realG) {
+      auto k = cholesky_kernel<double>;
+      smem_optin(k, chol_smem<double>());
+      count_launch();
+      k<<<nb, kCholThreads, chol_smem<double>(), st>>>(reinterpret_cast<double*>(G), nred, Nmax,
+                                                        L.status + L.batchOffset);
+    } else {
+      auto k = cholesky_kernel<double2>;
+      smem_optin(k, kCholSmem);
+      count_launch();
+      k<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset);
+    }
     B2_CHECK_LAUNCH();
     mark(2);
-    smem_optin(trinv_kernel<C>, kTrinvSmem);
-    count_launch();
-    trinv_kernel<C><<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax);
+    if (realG) {
+      auto k = trinv_kernel<double, R>;
+      smem_optin(k, trinv_smem<double>());
+      count_launch();
+      k<<<nb, 256, trinv_smem<double>(), st>>>(reinterpret_cast<const double*>(G), reinterpret_cast<double*>(W64),
+                                               reinterpret_cast<R*>(Linv), nred, Nmax);
+    } else {
+      auto k = trinv_kernel<double2, C>;
+      smem_optin(k, kTrinvSmem);
+      count_launch();
+      k<<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax);
+    }
     B2_CHECK_LAUNCH();
-    // T1 = Linv * A
+    // T1 = Linv * A (Linv real for W = I)
     mark(3);
     GemmArgs<C> g1{};
     g1.A = Linv; g1.strideA = n2; g1.lda = Nmax; g1.opA = 0;
@@ -224,7 +244,10 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g1.Cm = T1; g1.strideC = n2; g1.ldc = Nmax;
     g1.n = nred; g1.triA = 1; g1.triB = 0; g1.outMode = 0; g1.levels = 1;
     count_launch();
-    gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
+    if (realG)
+      gemm_kernel<C, R, R, C><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
+    else
+      gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
     B2_CHECK_LAUNCH();
     // A = T1 * Linv^H (Hermitian: lower tiles + mirror)
     GemmArgs<C> g2{};
@@ -233,7 +256,10 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g2.Cm = A; g2.strideC = n2; g2.ldc = Nmax;
     g2.n = nred; g2.triA = 0; g2.triB = 1; g2.outMode = 1; g2.levels = 1;
     count_launch();
-    gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
+    if (realG)
+      gemm_kernel<C, R, C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
+    else
+      gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
     B2_CHECK_LAUNCH();
   }
   // 3. tridiagonalisation
@@ -309,7 +335,10 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g3.Cm = reinterpret_cast<C*>(G); g3.strideC = n2; g3.ldc = Nmax;
     g3.n = nred; g3.triA = 2; g3.triB = 0; g3.outMode = 0; g3.levels = 1;
     count_launch();
-    gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);
+    if (realG)
+      gemm_kernel<C, R, R, C><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);
+    else
+      gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);
     B2_CHECK_LAUNCH();
   }
   tm.finish(order, no);

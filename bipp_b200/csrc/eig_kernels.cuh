@@ -127,7 +127,10 @@ prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long s
         const double x = 2.0 * sqrt(dx * dx + dy * dy + dz * dz) / w;
         g = (x != 0.0) ? sinpi(x) / (3.14159265358979323846 * x) : 1.0;
       }
-      Gb[r + (long long)c * Nmax] = make_double2(g, 0.0);
+      if (withGram == 2)
+        reinterpret_cast<double*>(G)[(long long)b * Nmax * Nmax + r + (long long)c * Nmax] = g;
+      else
+        Gb[r + (long long)c * Nmax] = make_double2(g, 0.0);
     }
   }
 }
@@ -137,51 +140,95 @@ prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long s
 // ------------------------------------------------------------------------------------
 constexpr int kCholNB = 32;
 constexpr int kCholThreads = 256;
-constexpr size_t kCholSmem = (size_t)(kCholNB + 128) * (kCholNB + 1) * sizeof(double2);
+template <typename E>
+constexpr size_t chol_smem() { return (size_t)(kCholNB + 128) * (kCholNB + 1) * sizeof(E); }
+constexpr size_t kCholSmem = chol_smem<double2>();
 
-static __global__ void __launch_bounds__(kCholThreads)
-cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status) {
+// FP64 element helpers: E = double2 (complex Hermitian G) or double (real symmetric G,
+// identity beamforming)
+template <typename E> __device__ __forceinline__ E e_zero();
+template <> __device__ __forceinline__ double2 e_zero<double2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ double e_zero<double>() { return 0.0; }
+__device__ __forceinline__ double e_re(double2 a) { return a.x; }
+__device__ __forceinline__ double e_re(double a) { return a; }
+__device__ __forceinline__ double2 e_real(double2, double v) { return make_double2(v, 0.0); }
+__device__ __forceinline__ double e_real(double, double v) { return v; }
+__device__ __forceinline__ double2 e_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double e_scale(double a, double s) { return a * s; }
+__device__ __forceinline__ double2 e_neg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double e_neg(double a) { return -a; }
+// acc -= a conj(b)
+__device__ __forceinline__ void e_sub_mulc(double2& acc, double2 a, double2 b) {
+  acc.x -= a.x * b.x + a.y * b.y;
+  acc.y -= a.y * b.x - a.x * b.y;
+}
+__device__ __forceinline__ void e_sub_mulc(double& acc, double a, double b) { acc -= a * b; }
+// acc -= a b
+__device__ __forceinline__ void e_sub_mul(double2& acc, double2 a, double2 b) {
+  acc.x -= a.x * b.x - a.y * b.y;
+  acc.y -= a.x * b.y + a.y * b.x;
+}
+__device__ __forceinline__ void e_sub_mul(double& acc, double a, double b) { acc -= a * b; }
+// acc += a conj(b)
+__device__ __forceinline__ void e_add_mulc(double2& acc, double2 a, double2 b) {
+  acc.x += a.x * b.x + a.y * b.y;
+  acc.y += a.y * b.x - a.x * b.y;
+}
+__device__ __forceinline__ void e_add_mulc(double& acc, double a, double b) { acc += a * b; }
+// acc += a b
+__device__ __forceinline__ void e_add_mul(double2& acc, double2 a, double2 b) { cfma(acc, a, b); }
+__device__ __forceinline__ void e_add_mul(double& acc, double a, double b) { acc += a * b; }
+// a / d
+__device__ __forceinline__ double2 e_div(double2 a, double2 d) {
+  const double den = d.x * d.x + d.y * d.y;
+  return make_double2((a.x * d.x + a.y * d.y) / den, (a.y * d.x - a.x * d.y) / den);
+}
+__device__ __forceinline__ double e_div(double a, double d) { return a / d; }
+
+template <typename E>
+__global__ void __launch_bounds__(kCholThreads)
+cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status) {
   const int b = blockIdx.x;
   const int n = nred[b];
-  double2* Gb = G + (long long)b * Nmax * Nmax;
-  extern __shared__ double2 chol_smem[];
-  double2 (*D)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem);
-  double2 (*Pi)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem + kCholNB * (kCholNB + 1));
-  double2 (*Pj)[kCholNB + 1] = reinterpret_cast<double2 (*)[kCholNB + 1]>(chol_smem + (kCholNB + 64) * (kCholNB + 1));
+  E* Gb = G + (long long)b * Nmax * Nmax;
+  extern __shared__ __align__(16) unsigned char chol_raw[];
+  E* chol_smem = reinterpret_cast<E*>(chol_raw);
+  E (*D)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem);
+  E (*Pi)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + kCholNB * (kCholNB + 1));
+  E (*Pj)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + (kCholNB + 64) * (kCholNB + 1));
   __shared__ int s_bad;
   if (threadIdx.x == 0) s_bad = 0;
   const int tid = threadIdx.x;
+  const E zero = e_zero<E>();
   for (int k0 = 0; k0 < n; k0 += kCholNB) {
     const int kb = min(kCholNB, n - k0);
     // 1. load diagonal block (lower)
     __syncthreads();
     for (int e = tid; e < kCholNB * kCholNB; e += blockDim.x) {
       const int r = e % kCholNB, c = e / kCholNB;
-      D[r][c] = (r < kb && c < kb && r >= c) ? Gb[(k0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+      D[r][c] = (r < kb && c < kb && r >= c) ? Gb[(k0 + r) + (long long)(k0 + c) * Nmax] : zero;
     }
     __syncthreads();
     // 2. unblocked factorisation in smem
     for (int j = 0; j < kb; ++j) {
       if (tid == 0) {
-        double djj = D[j][j].x;
+        double djj = e_re(D[j][j]);
         if (!(djj > 0.0)) {
           s_bad = 1;
           djj = 1e-300;
         }
-        D[j][j] = make_double2(sqrt(djj), 0.0);
+        D[j][j] = e_real(zero, sqrt(djj));
       }
       __syncthreads();
-      const double inv = 1.0 / D[j][j].x;
-      for (int r = j + 1 + tid; r < kb; r += blockDim.x) D[r][j] = cscale(D[r][j], inv);
+      const double inv = 1.0 / e_re(D[j][j]);
+      for (int r = j + 1 + tid; r < kb; r += blockDim.x) D[r][j] = e_scale(D[r][j], inv);
       __syncthreads();
       // trailing update inside the block: D[r][c] -= D[r][j] conj(D[c][j]), j < c <= r
       for (int e = tid; e < kb * kb; e += blockDim.x) {
         const int r = e % kb, c = e / kb;
         if (c > j && r >= c) {
-          double2 t = D[r][c];
-          double2 a = D[r][j], bb = D[c][j];
-          t.x -= a.x * bb.x + a.y * bb.y;
-          t.y -= a.y * bb.x - a.x * bb.y;
+          E t = D[r][c];
+          e_sub_mulc(t, D[r][j], D[c][j]);
           D[r][c] = t;
         }
       }
@@ -194,20 +241,15 @@ cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax,
     }
     // 4. panel: rows i >= k0+kb: x L_kk^H = a  (row-wise forward substitution)
     for (int i = k0 + kb + tid; i < n; i += blockDim.x) {
-      double2 x[kCholNB];
+      E x[kCholNB];
 #pragma unroll
-      for (int c = 0; c < kCholNB; ++c) x[c] = (c < kb) ? Gb[i + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+      for (int c = 0; c < kCholNB; ++c) x[c] = (c < kb) ? Gb[i + (long long)(k0 + c) * Nmax] : zero;
 #pragma unroll
       for (int c = 0; c < kCholNB; ++c) {
         if (c < kb) {
-          double2 acc = x[c];
-          for (int m = 0; m < c; ++m) {
-            // acc -= x[m] * conj(L[c][m])
-            const double2 l = D[c][m];
-            acc.x -= x[m].x * l.x + x[m].y * l.y;
-            acc.y -= x[m].y * l.x - x[m].x * l.y;
-          }
-          x[c] = cscale(acc, 1.0 / D[c][c].x);
+          E acc = x[c];
+          for (int m = 0; m < c; ++m) e_sub_mulc(acc, x[m], D[c][m]);
+          x[c] = e_scale(acc, 1.0 / e_re(D[c][c]));
         }
       }
 #pragma unroll
@@ -226,19 +268,19 @@ cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax,
         __syncthreads();
         for (int e = tid; e < 64 * kCholNB; e += blockDim.x) {
           const int r = e % 64, c = e / 64;
-          Pi[r][c] = (i0 + r < n && c < kb) ? Gb[(i0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
-          Pj[r][c] = (j0 + r < n && c < kb) ? Gb[(j0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+          Pi[r][c] = (i0 + r < n && c < kb) ? Gb[(i0 + r) + (long long)(k0 + c) * Nmax] : zero;
+          Pj[r][c] = (j0 + r < n && c < kb) ? Gb[(j0 + r) + (long long)(k0 + c) * Nmax] : zero;
         }
         __syncthreads();
         // each thread: 4x4 outputs; thread (tr, tc) in 16x16 grid
         const int tr = tid % 16, tc = tid / 16;
-        double2 acc[4][4];
+        E acc[4][4];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int c = 0; c < 4; ++c) acc[a][c] = make_double2(0, 0);
+          for (int c = 0; c < 4; ++c) acc[a][c] = zero;
         for (int m = 0; m < kb; ++m) {
-          double2 pa[4], pb[4];
+          E pa[4], pb[4];
 #pragma unroll
           for (int a = 0; a < 4; ++a) pa[a] = Pi[tr + 16 * a][m];
 #pragma unroll
@@ -246,10 +288,7 @@ cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax,
 #pragma unroll
           for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              acc[a][c].x += pa[a].x * pb[c].x + pa[a].y * pb[c].y;
-              acc[a][c].y += pa[a].y * pb[c].x - pa[a].x * pb[c].y;
-            }
+            for (int c = 0; c < 4; ++c) e_add_mulc(acc[a][c], pa[a], pb[c]);
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a)
@@ -257,10 +296,9 @@ cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax,
           for (int c = 0; c < 4; ++c) {
             const int i = i0 + tr + 16 * a, j = j0 + tc + 16 * c;
             if (i < n && j < n && j <= i) {
-              double2* p = Gb + i + (long long)j * Nmax;
-              double2 v = *p;
-              v.x -= acc[a][c].x;
-              v.y -= acc[a][c].y;
+              E* p = Gb + i + (long long)j * Nmax;
+              E v = *p;
+              e_sub_mul(v, acc[a][c], e_real(zero, 1.0));
               *p = v;
             }
           }
@@ -274,33 +312,37 @@ cholesky_kernel(double2* __restrict__ G, const int* __restrict__ nred, int Nmax,
 // ------------------------------------------------------------------------------------
 // triangular inverse of the lower Cholesky factor (FP64), output in working precision
 // ------------------------------------------------------------------------------------
-template <typename C>
-__device__ __forceinline__ void store_conv(C* p, double2 v);
-template <> __device__ __forceinline__ void store_conv<float2>(float2* p, double2 v) { *p = to_f(v); }
-template <> __device__ __forceinline__ void store_conv<double2>(double2* p, double2 v) { *p = v; }
+// FP64 value -> output element of Linv (complex or real, working precision)
+__device__ __forceinline__ void store_conv(float2* p, double2 v) { *p = to_f(v); }
+__device__ __forceinline__ void store_conv(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void store_conv(float* p, double v) { *p = (float)v; }
+__device__ __forceinline__ void store_conv(double* p, double v) { *p = v; }
 
 // Linv is computed block row by block row: Linv[I,I] = inv(L[I,I]);
-// Linv[I,J] = -Linv[I,I] sum_{K=J}^{I-1} L[I,K] Linv[K,J].
-// The FP64 inverse is kept in the (now unused) upper part of G's storage? No: G's
-// strictly upper triangle holds no data, so Linv^T is not needed; Linv is written to
-// a separate FP64 buffer W64 and rounded into LinvOut.
-constexpr size_t kTrinvSmem = 3 * 32 * 33 * sizeof(double2);
+// Linv[I,J] = -Linv[I,I] sum_{K=J}^{I-1} L[I,K] Linv[K,J]. The FP64 inverse goes to W64
+// (read back for the later block rows) and, rounded, to LinvOut. E = double2 (complex)
+// or double (real symmetric G); O = the matching working-precision output element.
+template <typename E>
+constexpr size_t trinv_smem() { return 3 * 32 * 33 * sizeof(E); }
+constexpr size_t kTrinvSmem = trinv_smem<double2>();
 
-template <typename C>
+template <typename E, typename O>
 __global__ void __launch_bounds__(256)
-trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __restrict__ LinvOut,
-             const int* __restrict__ nred, int Nmax) {
+trinv_kernel(const E* __restrict__ L, E* __restrict__ W64, O* __restrict__ LinvOut, const int* __restrict__ nred,
+             int Nmax) {
   constexpr int NB = 32;
   const int b = blockIdx.x;
   const int n = nred[b];
-  const double2* Lb = L + (long long)b * Nmax * Nmax;
-  double2* Wb = W64 + (long long)b * Nmax * Nmax;
-  C* Ob = LinvOut + (long long)b * Nmax * Nmax;
-  extern __shared__ double2 trinv_smem[];
-  double2 (*Dinv)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem);
-  double2 (*Ta)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem + NB * (NB + 1));
-  double2 (*Tb)[NB + 1] = reinterpret_cast<double2 (*)[NB + 1]>(trinv_smem + 2 * NB * (NB + 1));
+  const E* Lb = L + (long long)b * Nmax * Nmax;
+  E* Wb = W64 + (long long)b * Nmax * Nmax;
+  O* Ob = LinvOut + (long long)b * Nmax * Nmax;
+  extern __shared__ __align__(16) unsigned char trinv_raw[];
+  E* trinv_smem_p = reinterpret_cast<E*>(trinv_raw);
+  E (*Dinv)[NB + 1] = reinterpret_cast<E (*)[NB + 1]>(trinv_smem_p);
+  E (*Ta)[NB + 1] = reinterpret_cast<E (*)[NB + 1]>(trinv_smem_p + NB * (NB + 1));
+  E (*Tb)[NB + 1] = reinterpret_cast<E (*)[NB + 1]>(trinv_smem_p + 2 * NB * (NB + 1));
   const int tid = threadIdx.x;
+  const E zero = e_zero<E>();
   const int nblk = (n + NB - 1) / NB;
   for (int I = 0; I < nblk; ++I) {
     const int i0 = I * NB, ib = min(NB, n - i0);
@@ -308,26 +350,18 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
     // load L_II into Ta (lower) and invert into Dinv by column forward substitution
     for (int e = tid; e < NB * NB; e += blockDim.x) {
       const int r = e % NB, c = e / NB;
-      Ta[r][c] = (r < ib && c < ib && r >= c) ? Lb[(i0 + r) + (long long)(i0 + c) * Nmax] : make_double2(0, 0);
+      Ta[r][c] = (r < ib && c < ib && r >= c) ? Lb[(i0 + r) + (long long)(i0 + c) * Nmax] : zero;
     }
     __syncthreads();
     if (tid < NB) {
       const int c = tid;  // column c of the inverse
       for (int r = 0; r < NB; ++r) {
-        double2 acc = make_double2(r == c ? 1.0 : 0.0, 0.0);
+        E acc = e_real(zero, r == c ? 1.0 : 0.0);
         if (r < ib && c < ib && r >= c) {
-          for (int m = c; m < r; ++m) {
-            // acc -= L[r][m] * X[m]
-            const double2 l = Ta[r][m], x = Dinv[m][c];
-            acc.x -= l.x * x.x - l.y * x.y;
-            acc.y -= l.x * x.y + l.y * x.x;
-          }
-          const double2 d = Ta[r][r];
-          // divide by complex diagonal (real for a Cholesky factor)
-          const double den = d.x * d.x + d.y * d.y;
-          Dinv[r][c] = make_double2((acc.x * d.x + acc.y * d.y) / den, (acc.y * d.x - acc.x * d.y) / den);
+          for (int m = c; m < r; ++m) e_sub_mul(acc, Ta[r][m], Dinv[m][c]);
+          Dinv[r][c] = e_div(acc, Ta[r][r]);
         } else {
-          Dinv[r][c] = make_double2(0, 0);
+          Dinv[r][c] = zero;
         }
       }
     }
@@ -335,28 +369,28 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
     for (int e = tid; e < NB * NB; e += blockDim.x) {
       const int r = e % NB, c = e / NB;
       if (r < ib && c < ib) {
-        const double2 v = (r >= c) ? Dinv[r][c] : make_double2(0, 0);
+        const E v = (r >= c) ? Dinv[r][c] : zero;
         Wb[(i0 + r) + (long long)(i0 + c) * Nmax] = v;
-        store_conv<C>(Ob + (i0 + r) + (long long)(i0 + c) * Nmax, v);
+        store_conv(Ob + (i0 + r) + (long long)(i0 + c) * Nmax, v);
       }
     }
     // strictly upper blocks J > I are zero (the GEMMs read whole tiles of Linv)
     for (long long e = tid; e < (long long)ib * (n - i0 - ib); e += blockDim.x) {
       const int r = (int)(e % ib), c = i0 + ib + (int)(e / ib);
-      Wb[(i0 + r) + (long long)c * Nmax] = make_double2(0, 0);
-      store_conv<C>(Ob + (i0 + r) + (long long)c * Nmax, make_double2(0, 0));
+      Wb[(i0 + r) + (long long)c * Nmax] = zero;
+      store_conv(Ob + (i0 + r) + (long long)c * Nmax, zero);
     }
     // off-diagonal blocks J < I
     for (int J = 0; J < I; ++J) {
       const int j0 = J * NB;
       const int tr = tid % 16, tc = tid / 16;  // 16x16 threads, 2x2 outputs each
-      double2 acc[2][2] = {{make_double2(0, 0), make_double2(0, 0)}, {make_double2(0, 0), make_double2(0, 0)}};
+      E acc[2][2] = {{zero, zero}, {zero, zero}};
       for (int K = J; K < I; ++K) {
         const int k0 = K * NB;
         __syncthreads();
         for (int e = tid; e < NB * NB; e += blockDim.x) {
           const int r = e % NB, c = e / NB;
-          Ta[r][c] = (r < ib) ? Lb[(i0 + r) + (long long)(k0 + c) * Nmax] : make_double2(0, 0);
+          Ta[r][c] = (r < ib) ? Lb[(i0 + r) + (long long)(k0 + c) * Nmax] : zero;
           Tb[r][c] = Wb[(k0 + r) + (long long)(j0 + c) * Nmax];
         }
         __syncthreads();
@@ -365,7 +399,7 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
 #pragma unroll
           for (int a = 0; a < 2; ++a)
 #pragma unroll
-            for (int c = 0; c < 2; ++c) cfma(acc[a][c], Ta[tr + 16 * a][m], Tb[m][tc + 16 * c]);
+            for (int c = 0; c < 2; ++c) e_add_mul(acc[a][c], Ta[tr + 16 * a][m], Tb[m][tc + 16 * c]);
         }
       }
       __syncthreads();
@@ -376,12 +410,12 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
         for (int c = 0; c < 2; ++c) Tb[tr + 16 * a][tc + 16 * c] = acc[a][c];
       __syncthreads();
       // out = -Dinv * Tb
-      double2 o[2][2] = {{make_double2(0, 0), make_double2(0, 0)}, {make_double2(0, 0), make_double2(0, 0)}};
+      E o[2][2] = {{zero, zero}, {zero, zero}};
       for (int m = 0; m < NB; ++m) {
 #pragma unroll
         for (int a = 0; a < 2; ++a)
 #pragma unroll
-          for (int c = 0; c < 2; ++c) cfma(o[a][c], Dinv[tr + 16 * a][m], Tb[m][tc + 16 * c]);
+          for (int c = 0; c < 2; ++c) e_add_mul(o[a][c], Dinv[tr + 16 * a][m], Tb[m][tc + 16 * c]);
       }
 #pragma unroll
       for (int a = 0; a < 2; ++a)
@@ -389,9 +423,9 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
         for (int c = 0; c < 2; ++c) {
           const int r = tr + 16 * a, cc = tc + 16 * c;
           if (r < ib && j0 + cc < n) {
-            const double2 v = make_double2(-o[a][c].x, -o[a][c].y);
+            const E v = e_neg(o[a][c]);
             Wb[(i0 + r) + (long long)(j0 + cc) * Nmax] = v;
-            store_conv<C>(Ob + (i0 + r) + (long long)(j0 + cc) * Nmax, v);
+            store_conv(Ob + (i0 + r) + (long long)(j0 + cc) * Nmax, v);
           }
         }
     }
@@ -403,8 +437,9 @@ trinv_kernel(const double2* __restrict__ L, double2* __restrict__ W64, C* __rest
 // ------------------------------------------------------------------------------------
 template <typename C>
 struct GemmArgs {
-  const C* A; long long strideA; int lda; int opA;   // opA 0: A[i,k]; 1: conj(A[k,i])
-  const C* B; long long strideB; int ldb; int opB;   // opB 0: B[k,j]; 1: conj(B[j,k])
+  // A and B are complex C or, for the real-operand instantiations, real R (element strides)
+  const void* A; long long strideA; int lda; int opA;   // opA 0: A[i,k]; 1: conj(A[k,i])
+  const void* B; long long strideB; int ldb; int opB;   // opB 0: B[k,j]; 1: conj(B[j,k])
   C* Cm; long long strideC; int ldc;
   const int* n;           // per-matrix size
   int triA;               // 0 none; 1 opA(i,k)=0 for k>i; 2 opA(i,k)=0 for k<i
@@ -418,7 +453,29 @@ struct GemmArgs {
 
 constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 8, kGemmThreads = 256;
 
-template <typename C, typename R>
+// operand helpers: conj of a real value is itself; the product of a complex accumulator
+// with real / complex operands
+__device__ __forceinline__ float opconj(float a) { return a; }
+__device__ __forceinline__ double opconj(double a) { return a; }
+__device__ __forceinline__ float2 opconj(float2 a) { return cconj(a); }
+__device__ __forceinline__ double2 opconj(double2 a) { return cconj(a); }
+__device__ __forceinline__ float opscale(float a, float s) { return a * s; }
+__device__ __forceinline__ double opscale(double a, double s) { return a * s; }
+__device__ __forceinline__ float2 opscale(float2 a, float s) { return cscale(a, s); }
+__device__ __forceinline__ double2 opscale(double2 a, double s) { return cscale(a, s); }
+template <typename E> __device__ __forceinline__ E opzero();
+template <> __device__ __forceinline__ float opzero<float>() { return 0.f; }
+template <> __device__ __forceinline__ double opzero<double>() { return 0.0; }
+template <> __device__ __forceinline__ float2 opzero<float2>() { return make_float2(0.f, 0.f); }
+template <> __device__ __forceinline__ double2 opzero<double2>() { return make_double2(0.0, 0.0); }
+template <typename C> __device__ __forceinline__ void opfma(C& acc, C a, C b) { cfma(acc, a, b); }
+__device__ __forceinline__ void opfma(float2& acc, float a, float2 b) { acc.x = fmaf(a, b.x, acc.x); acc.y = fmaf(a, b.y, acc.y); }
+__device__ __forceinline__ void opfma(float2& acc, float2 a, float b) { acc.x = fmaf(a.x, b, acc.x); acc.y = fmaf(a.y, b, acc.y); }
+__device__ __forceinline__ void opfma(double2& acc, double a, double2 b) { acc.x = fma(a, b.x, acc.x); acc.y = fma(a, b.y, acc.y); }
+__device__ __forceinline__ void opfma(double2& acc, double2 a, double b) { acc.x = fma(a.x, b, acc.x); acc.y = fma(a.y, b, acc.y); }
+
+// EA / EB: element types of A / B (C complex, or R real: Linv of a real Gram matrix)
+template <typename C, typename R, typename EA = C, typename EB = C>
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   const int z = blockIdx.z;
   const int b = z / g.levels, lvl = z % g.levels;
@@ -436,13 +493,13 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   if (g.triA == 2) kb = max(kb, i0);
   if (g.triB == 1) ke = min(ke, j0 + kGemmBN);
   if (g.triB == 2) kb = max(kb, j0);
-  const C* A = g.A + b * g.strideA;
-  const C* B = g.B + b * g.strideB;
+  const EA* A = static_cast<const EA*>(g.A) + b * g.strideA;
+  const EB* B = static_cast<const EB*>(g.B) + b * g.strideB;
   C* Cm = g.Cm + b * g.strideC + lvl * g.strideCLevel;
   const R* ks = g.kscale ? reinterpret_cast<const R*>(g.kscale) + b * g.strideK : nullptr;
 
-  __shared__ C As[kGemmBK][kGemmBM + 1];
-  __shared__ C Bs[kGemmBK][kGemmBN + 1];
+  __shared__ EA As[kGemmBK][kGemmBM + 1];
+  __shared__ EB Bs[kGemmBK][kGemmBN + 1];
   const int tid = threadIdx.x;
   const int tr = tid % 16, tc = tid / 16;
   C acc[4][4];
@@ -459,10 +516,10 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
       int r, kk;
       if (g.opA == 0) { r = e % kGemmBM; kk = e / kGemmBM; } else { kk = e % kGemmBK; r = e / kGemmBK; }
       const int i = i0 + r, k = k0 + kk;
-      C v = mk(R(0), R(0));
+      EA v = opzero<EA>();
       if (i < n && k < ke) {
-        v = (g.opA == 0) ? A[i + (long long)k * g.lda] : cconj(A[k + (long long)i * g.lda]);
-        if (ks) v = cscale(v, ks[k]);
+        v = (g.opA == 0) ? A[i + (long long)k * g.lda] : opconj(A[k + (long long)i * g.lda]);
+        if (ks) v = opscale(v, ks[k]);
       }
       As[kk][r] = v;
     }
@@ -472,14 +529,15 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
       int cidx, kk;
       if (g.opB == 0) { kk = e % kGemmBK; cidx = e / kGemmBK; } else { cidx = e % kGemmBN; kk = e / kGemmBN; }
       const int j = j0 + cidx, k = k0 + kk;
-      C v = mk(R(0), R(0));
-      if (j < n && k < ke) v = (g.opB == 0) ? B[k + (long long)j * g.ldb] : cconj(B[j + (long long)k * g.ldb]);
+      EB v = opzero<EB>();
+      if (j < n && k < ke) v = (g.opB == 0) ? B[k + (long long)j * g.ldb] : opconj(B[j + (long long)k * g.ldb]);
       Bs[kk][cidx] = v;
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < kGemmBK; ++kk) {
-      C av[4], bv[4];
+      EA av[4];
+      EB bv[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) av[a] = As[kk][tr + 16 * a];
 #pragma unroll
@@ -487,7 +545,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) cfma(acc[a][c], av[a], bv[c]);
+        for (int c = 0; c < 4; ++c) opfma(acc[a][c], av[a], bv[c]);
     }
     __syncthreads();
   }

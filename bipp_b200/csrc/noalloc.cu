@@ -149,10 +149,10 @@ extern "C" BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl
     prep_kernel<float><<<1, kPrepThreads, 2 * (size_t)N * sizeof(int), st>>>(
         N, static_cast<const float2*>(s), 0, (int)lds, xyz, 0, (int)ldxyz, wlD, 0, FLT_EPSILON, 1, N, idx, nred, nvis,
         w.A, w.G, status, 1, 1, 0);
-    smem_optin(cholesky_kernel, kCholSmem);
-    cholesky_kernel<<<1, kCholThreads, kCholSmem, st>>>(w.G, nred, N, status);
-    smem_optin(trinv_kernel<float2>, kTrinvSmem);
-    trinv_kernel<float2><<<1, 256, kTrinvSmem, st>>>(w.G, w.W64, w.Linv, nred, N);
+    smem_optin(cholesky_kernel<double2>, kCholSmem);
+    cholesky_kernel<double2><<<1, kCholThreads, kCholSmem, st>>>(w.G, nred, N, status);
+    smem_optin(trinv_kernel<double2, float2>, kTrinvSmem);
+    trinv_kernel<double2, float2><<<1, 256, kTrinvSmem, st>>>(w.G, w.W64, w.Linv, nred, N);
     GemmArgs<float2> g1{};
     g1.A = w.Linv; g1.strideA = n2; g1.lda = N; g1.opA = 0;
     g1.B = w.A; g1.strideB = n2; g1.ldb = N; g1.opB = 0;

@@ -54,13 +54,24 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
   }
 }
 
-void es_params(double eps, int& W, float& beta) {
-  W = (int)std::ceil(std::log10(1.0 / std::max(eps, 1e-15))) + 1;
+// Exponential-of-semicircle kernel parameters for tolerance eps at oversampling sigma
+// (the published FINUFFT rules): sigma = 2: W = ceil(log10(1/eps)) + 1, beta/W = 2.30
+// (2.20, 2.26, 2.38 for W = 2, 3, 4); otherwise W = ceil(ln(1/eps) / (pi sqrt(1 - 1/sigma)))
+// and beta/W = 0.97 pi (1 - 1/(2 sigma)).
+void es_params(double eps, double sigma, int& W, float& beta) {
+  const double e = std::max(eps, 1e-15);
+  double bw;
+  if (sigma == 2.0) {
+    W = (int)std::ceil(std::log10(1.0 / e)) + 1;
+    bw = 2.30;
+    if (W == 2) bw = 2.20;
+    else if (W == 3) bw = 2.26;
+    else if (W == 4) bw = 2.38;
+  } else {
+    W = (int)std::ceil(std::log(1.0 / e) / (M_PI * std::sqrt(1.0 - 1.0 / sigma)));
+    bw = 0.97 * M_PI * (1.0 - 0.5 / sigma);
+  }
   W = std::max(2, std::min(W, kMaxW));
-  double bw = 2.30;
-  if (W == 2) bw = 2.20;
-  else if (W == 3) bw = 2.26;
-  else if (W == 4) bw = 2.38;
   beta = (float)(bw * W);
 }
 
@@ -148,8 +159,10 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   g_ = NufftGeom{};
   g_.l0 = lat.l0; g_.m0 = lat.m0; g_.Al = lat.Al; g_.Bl = lat.Bl; g_.Am = lat.Am; g_.Bm = lat.Bm;
   g_.Na = lat.Na; g_.Nb = lat.Nb;
-  es_params(eps, g_.W, g_.beta);
-  const double sigma = 2.0;
+  // oversampling 1.75: the same kernel width as 2 at the tolerances of interest
+  // (W = 6 at 1e-5) on (7/8)^3 of the fine grid
+  const double sigma = kNufftSigma;
+  es_params(eps, sigma, g_.W, g_.beta);
   g_.nx = next_smooth((int)std::ceil(sigma * g_.Nb));
   g_.ny = next_smooth((int)std::ceil(sigma * g_.Na));
   g_.nx = std::max(g_.nx, 2 * g_.W);
