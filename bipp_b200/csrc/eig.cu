@@ -157,6 +157,7 @@ void EigWork<T>::reserve(bipp_ctx_s* ctx, int nBatch, int nmax) {
   d.alloc(ctx, (size_t)nmax * sizeof(double) * nBatch);
   e.alloc(ctx, (size_t)nmax * sizeof(double) * nBatch);
   tau.alloc(ctx, (size_t)nmax * sizeof(C) * nBatch);
+  krange.alloc(ctx, (size_t)2 * sizeof(int) * nBatch);
 }
 
 template <typename T>
@@ -173,6 +174,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   C* T1 = w.T1.template get<C>();
   R* Z = w.Z.template get<R>();
   const int* nred = L.nred + L.batchOffset;
+  int* krange = w.krange.template get<int>();
   SeqTimer tm(st, L.kernelMs);
   int order[kEigTimers];
   int no = 0;
@@ -282,7 +284,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     count_launch();
     k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
-                                     L.status + L.batchOffset);
+                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange);
     B2_CHECK_LAUNCH();
   }
   // 5. back-transform Y = Q Z -> T1
@@ -304,7 +306,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     auto k = bt_apply_kernel<C, R, KR>;                                                      \
     smem_optin(k, smem);                                                                     \
     count_launch();                                                                          \
-    k<<<grid, kBtApplyThreads, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1);             \
+    k<<<grid, kBtApplyThreads, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange);     \
   }
     const int kr = (Nmax + kBtRG - 1) / kBtRG;
     if (kr <= 2) B2_BT(2) else if (kr <= 4) B2_BT(4) else if (kr <= 6) B2_BT(6) else B2_BT(8)
@@ -333,7 +335,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g3.A = Linv; g3.strideA = n2; g3.lda = Nmax; g3.opA = 1;
     g3.B = T1; g3.strideB = n2; g3.ldb = Nmax; g3.opB = 0;
     g3.Cm = reinterpret_cast<C*>(G); g3.strideC = n2; g3.ldc = Nmax;
-    g3.n = nred; g3.triA = 2; g3.triB = 0; g3.outMode = 0; g3.levels = 1;
+    g3.n = nred; g3.triA = 2; g3.triB = 0; g3.outMode = 0; g3.levels = 1; g3.colRange = krange;
     count_launch();
     if (realG)
       gemm_kernel<C, R, R, C><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g3);

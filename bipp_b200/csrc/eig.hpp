@@ -10,7 +10,7 @@ namespace bippb200 {
 template <typename T>
 struct EigWork {
   int capBatch = 0, Nmax = 0;
-  DevBuf A, G, W64, Linv, T1, Z, d, e, tau;
+  DevBuf A, G, W64, Linv, T1, Z, d, e, tau, krange;
   void reserve(bipp_ctx_s* ctx, int nBatch, int Nmax);
   // compacted eigenvectors (column c = eigenvector of eigenvalue c), ld Nmax
   typename Cplx<T>::type* X(bool gram);
@@ -45,6 +45,9 @@ struct EigLaunch {
   double* lam = nullptr;        // [batch][Nmax]
   int doFlag = 1;
   int batchOffset = 0;
+  // eigenvectors are needed only for eigenvalues in [vecLo, vecHi] (the synthesis uses
+  // those inside its energy levels); the others are returned as zero columns
+  double vecLo = -1.0 / 0.0, vecHi = 1.0 / 0.0;
   // optional per-kernel device time accumulation (ms): prep, cholesky, trinv, reduction
   // GEMMs, hetrd, tridiagonal eigenpairs, back-transform, Linv^H Y GEMM
   double* kernelMs = nullptr;

@@ -448,6 +448,7 @@ struct GemmArgs {
   const void* kscale; long long strideK;   // optional real per-k scale on opA columns
   const int* kbeg; const int* kend;        // optional per-(matrix,level) k range
   int levels;             // grid.z = batch * levels (levels >= 1)
+  const int* colRange;    // optional [2 per matrix]: only output columns [lo, hi) are needed
   long long strideCLevel; // output stride per level
 };
 
@@ -483,6 +484,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   const int i0 = blockIdx.y * kGemmBM, j0 = blockIdx.x * kGemmBN;
   if (i0 >= n || j0 >= n) return;
   if (g.outMode != 0 && j0 > i0 + kGemmBM - 1) return;
+  if (g.colRange && (j0 + kGemmBN <= g.colRange[2 * b] || j0 >= g.colRange[2 * b + 1])) return;
   int kb = 0, ke = n;
   if (g.kbeg) {
     kb = g.kbeg[z];
@@ -846,11 +848,15 @@ __device__ __forceinline__ int sturm_count(const double* __restrict__ d, const d
 // work: [2][n][Nmax] FP64 per matrix (Lp and Um of every eigenvalue, interleaved by
 // eigenvalue index so that lanes access consecutive addresses). Z: real eigenvectors,
 // row-major Z[k*Nmax + i] = z_i[k], working precision R.
+// Eigenvectors are formed only for the eigenvalues in [vecLo, vecHi] (all of them with
+// the infinite defaults); their index range [kLo, kHi) goes to krange[2b], krange[2b+1]
+// when krange is given, and the other columns of Z are zero.
 template <typename R>
 __global__ void __launch_bounds__(kTriThreads)
 tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, const int* __restrict__ nred,
                int Nmax, double* __restrict__ lamOut, R* __restrict__ Z, double* __restrict__ work,
-               int* __restrict__ status) {
+               int* __restrict__ status, double vecLo = -INFINITY, double vecHi = INFINITY,
+               int* __restrict__ krange = nullptr) {
   const int b = blockIdx.x;
   const int n = nred[b];
   if (n <= 0) return;
@@ -900,12 +906,31 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
   }
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) lamOut[(long long)b * Nmax + i] = lam[i];
+  // eigenvalue index range of the requested eigenvectors (lam ascending)
+  __shared__ int s_klo, s_khi;
+  if (threadIdx.x == 0) {
+    int a = 0, c = n;
+    while (a < c && lam[a] < vecLo) ++a;
+    while (c > a && lam[c - 1] > vecHi) --c;
+    s_klo = a;
+    s_khi = c;
+    if (krange) {
+      krange[2 * b] = a;
+      krange[2 * b + 1] = c;
+    }
+  }
+  __syncthreads();
+  const int kLo = s_klo, kHi = s_khi;
 
   // twisted factorisation eigenvectors
   double* Lp = work + (long long)b * 2 * Nmax * Nmax;
   double* Um = Lp + (long long)Nmax * Nmax;
   R* Zb = Z + (long long)b * Nmax * Nmax;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (i >= kLo && i < kHi) continue;
+    for (int k = 0; k < n; ++k) Zb[(long long)k * Nmax + i] = R(0);
+  }
+  for (int i = kLo + threadIdx.x; i < kHi; i += blockDim.x) {
     const double l = lam[i];
     // top-down stationary factorisation T - l = L+ D+ L+^T
     double dp = d[0] - l;
@@ -988,16 +1013,16 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
   __shared__ int s_any;
   if (threadIdx.x == 0) {
     int any = 0;
-    for (int i = 1; i < n; ++i) any |= (lam[i] - lam[i - 1] < ctol);
+    for (int i = kLo + 1; i < kHi; ++i) any |= (lam[i] - lam[i - 1] < ctol);
     s_any = any;
   }
   __syncthreads();
   if (!s_any) return;
   if (threadIdx.x == 0) atomicOr(status + b, (int)kStatusClusterFix);
-  for (int i = 1; i < n; ++i) {
+  for (int i = kLo + 1; i < kHi; ++i) {
     if (!(lam[i] - lam[i - 1] < ctol)) continue;
     int j0 = i - 1;
-    while (j0 > 0 && lam[j0] - lam[j0 - 1] < ctol) --j0;
+    while (j0 > kLo && lam[j0] - lam[j0 - 1] < ctol) --j0;
     for (int j = j0; j < i; ++j) {
       double part = 0.0;
       for (int k = threadIdx.x; k < n; k += blockDim.x)
@@ -1161,11 +1186,14 @@ constexpr int kBtJC = 2;                     // reflectors per register chunk
 template <typename C, typename R, int KR>
 __global__ void __launch_bounds__(kBtApplyThreads, sizeof(C) == 8 ? 2 : 1)
 bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tStride, const R* __restrict__ Z,
-                const int* __restrict__ nred, int Nmax, C* __restrict__ Y) {
+                const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange) {
   const int b = blockIdx.y;
   const int n = nred[b];
   const int c0 = blockIdx.x * kBtCB;
   if (c0 >= n) return;
+  // only the eigenvector columns [cLo, cHi) are transformed
+  const int cLo = krange ? krange[2 * b] : 0, cHi = krange ? krange[2 * b + 1] : n;
+  if (c0 + kBtCB <= cLo || c0 >= cHi) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Vs = reinterpret_cast<C*>(smem_raw);              // [Nmax][kBtVS] block of reflectors (row-major)
   C* red = Vs + (long long)Nmax * kBtVS;               // [8 warps][16 j][16 c]
@@ -1183,7 +1211,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
     for (int u = 0; u < 4; ++u) {
       const int col = c0 + 4 * cg + u;
       // Z (tridiagonal eigenvectors) is row-major: Z(r, col) at r * Nmax + col
-      y[q][u] = mk((r < n && col < n) ? Zb[(long long)r * Nmax + col] : R(0), R(0));
+      y[q][u] = mk((r < n && col >= cLo && col < cHi) ? Zb[(long long)r * Nmax + col] : R(0), R(0));
     }
   }
   const int nblk = (n - 1 + kBtNB - 1) / kBtNB;

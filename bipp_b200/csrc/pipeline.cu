@@ -178,6 +178,13 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     E.status = p->status.get<int>(); E.lam = p->lam.get<double>();
     E.doFlag = 0; E.batchOffset = s0;
     E.kernelMs = ms ? p->eigMs : nullptr;
+    // only the eigenvectors inside the energy levels enter the virtual visibilities
+    E.vecLo = INFINITY;
+    E.vecHi = -INFINITY;
+    for (size_t l = 0; l < p->intervals.size() / 2; ++l) {
+      E.vecLo = std::min(E.vecLo, p->intervals[2 * l]);
+      E.vecHi = std::max(E.vecHi, p->intervals[2 * l + 1]);
+    }
     eig_launch<float>(ctx, E, p->eig);
     if (ms) cudaEventRecord(e1, ctx->stream);
     count_launch();
