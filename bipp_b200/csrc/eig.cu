@@ -284,7 +284,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     count_launch();
     k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
-                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange);
+                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues);
     B2_CHECK_LAUNCH();
   }
   // 5. back-transform Y = Q Z -> T1

@@ -48,6 +48,8 @@ struct EigLaunch {
   // eigenvectors are needed only for eigenvalues in [vecLo, vecHi] (the synthesis uses
   // those inside its energy levels); the others are returned as zero columns
   double vecLo = -1.0 / 0.0, vecHi = 1.0 / 0.0;
+  // 0: eigenvalues outside [vecLo, vecHi] are not computed either (returned as zero)
+  int allValues = 1;
   // optional per-kernel device time accumulation (ms): prep, cholesky, trinv, reduction
   // GEMMs, hetrd, tridiagonal eigenpairs, back-transform, Linv^H Y GEMM
   double* kernelMs = nullptr;

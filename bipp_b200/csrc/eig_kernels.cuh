@@ -850,13 +850,15 @@ __device__ __forceinline__ int sturm_count(const double* __restrict__ d, const d
 // row-major Z[k*Nmax + i] = z_i[k], working precision R.
 // Eigenvectors are formed only for the eigenvalues in [vecLo, vecHi] (all of them with
 // the infinite defaults); their index range [kLo, kHi) goes to krange[2b], krange[2b+1]
-// when krange is given, and the other columns of Z are zero.
+// when krange is given, and the other columns of Z are zero. With allValues == 0 only
+// the eigenvalues of that range are computed too (two Sturm counts bound it) and the
+// other entries of lamOut are zero.
 template <typename R>
 __global__ void __launch_bounds__(kTriThreads)
 tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, const int* __restrict__ nred,
                int Nmax, double* __restrict__ lamOut, R* __restrict__ Z, double* __restrict__ work,
                int* __restrict__ status, double vecLo = -INFINITY, double vecHi = INFINITY,
-               int* __restrict__ krange = nullptr) {
+               int* __restrict__ krange = nullptr, int allValues = 1) {
   const int b = blockIdx.x;
   const int n = nred[b];
   if (n <= 0) return;
@@ -893,8 +895,27 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
   const double pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
   lo -= 2.0 * eps * tnorm + 4.0 * pivmin;
   hi += 2.0 * eps * tnorm + 4.0 * pivmin;
+  // index range of the eigenvalues to compute
+  __shared__ int s_vlo, s_vhi;
+  if (threadIdx.x == 0) {
+    int a = 0, c = n;
+    if (!allValues) {
+      if (vecLo > lo) a = min(n, sturm_count(d, e2, n, vecLo, pivmin));
+      if (vecHi < hi) c = max(a, min(n, sturm_count(d, e2, n, vecHi, pivmin)));
+    }
+    s_vlo = a;
+    s_vhi = c;
+  }
+  __syncthreads();
+  const int vLo = s_vlo, vHi = s_vhi;
+  if (!allValues) {
+    if (vecLo > lo) lo = vecLo - (2.0 * eps * fabs(vecLo) + 4.0 * pivmin);
+    if (vecHi < hi) hi = vecHi + (2.0 * eps * fabs(vecHi) + 4.0 * pivmin);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      if (i < vLo || i >= vHi) lam[i] = 0.0;
+  }
   // bisection for each eigenvalue index
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = vLo + threadIdx.x; i < vHi; i += blockDim.x) {
     double a = lo, c = hi;
     for (int it = 0; it < 128; ++it) {
       const double mid = 0.5 * (a + c);
@@ -909,7 +930,7 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
   // eigenvalue index range of the requested eigenvectors (lam ascending)
   __shared__ int s_klo, s_khi;
   if (threadIdx.x == 0) {
-    int a = 0, c = n;
+    int a = vLo, c = vHi;
     while (a < c && lam[a] < vecLo) ++a;
     while (c > a && lam[c - 1] > vecHi) --c;
     s_klo = a;

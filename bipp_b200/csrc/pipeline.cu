@@ -78,10 +78,13 @@ __device__ __forceinline__ double filter_value(int f, double d) {
 
 // per step: kscale[b][c] = (1/nVis) filter(d_c); per (step, level) the contiguous range of
 // eigenvalue indices with lo <= d <= hi (eigenvalues are ascending)
+// Per step and level: the eigenvalue index range [kbeg, kend) of the level (eigenvalues
+// ascending) inside the computed range krange = [kLo, kHi) of the eigensolver, and the
+// column scales filter(d) / nVis.
 __global__ void levels_kernel(int nSteps, int Nmax, int nLevels, const double* __restrict__ intervals, int filt,
                               const int* __restrict__ nred, const long long* __restrict__ nvis,
-                              const double* __restrict__ lam, float* __restrict__ kscale, int* __restrict__ kbeg,
-                              int* __restrict__ kend) {
+                              const double* __restrict__ lam, const int* __restrict__ krange,
+                              float* __restrict__ kscale, int* __restrict__ kbeg, int* __restrict__ kend) {
   const int b = blockIdx.x;
   if (b >= nSteps) return;
   const int n = nred[b];
@@ -92,10 +95,11 @@ __global__ void levels_kernel(int nSteps, int Nmax, int nLevels, const double* _
   if (threadIdx.x < nLevels) {
     const int l = threadIdx.x;
     const double lo = intervals[2 * l], hi = intervals[2 * l + 1];
-    int a = 0;
-    while (a < n && d[a] < lo) ++a;
+    const int kLo = krange[2 * b], kHi = krange[2 * b + 1];
+    int a = kLo;
+    while (a < kHi && d[a] < lo) ++a;
     int e = a;
-    while (e < n && d[e] <= hi) ++e;
+    while (e < kHi && d[e] <= hi) ++e;
     kbeg[b * nLevels + l] = a;
     kend[b * nLevels + l] = e;
   }
@@ -185,12 +189,14 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
       E.vecLo = std::min(E.vecLo, p->intervals[2 * l]);
       E.vecHi = std::max(E.vecHi, p->intervals[2 * l + 1]);
     }
+    E.allValues = 0;
     eig_launch<float>(ctx, E, p->eig);
     if (ms) cudaEventRecord(e1, ctx->stream);
     count_launch();
     levels_kernel<<<nb, 128, 0, ctx->stream>>>(nb, N, L, p->intervalsD.get<double>(), p->filter, p->nred.get<int>() + s0,
                                                p->nvis.get<long long>() + s0, p->lam.get<double>() + (long long)s0 * N,
-                                               p->kscale.get<float>() + (long long)s0 * N, p->kbeg.get<int>() + s0 * L,
+                                               p->eig.krange.get<int>(), p->kscale.get<float>() + (long long)s0 * N,
+                                               p->kbeg.get<int>() + s0 * L,
                                                p->kend.get<int>() + s0 * L);
     B2_CHECK_LAUNCH();
     // VV[b][l] lower triangle = X diag(kscale) X^H over the level's eigenvalue range

@@ -251,7 +251,9 @@ BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSte
  * to host (onDevice == 0) or device memory. */
 BIPP_B200_EXPORT BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize, int onDevice);
 BIPP_B200_EXPORT BippError bipp_pipeline_reset(bipp_pipeline_t pl);
-/* Eigenvalues [maxSteps][nAntenna] and nBeamReduced of the last process() call (host). */
+/* Eigenvalues [maxSteps][nAntenna] and nBeamReduced of the last process() call (host).
+ * Only the eigenvalues inside [min lo, max hi] of the energy levels are computed by the
+ * pipeline (the others do not enter the images); the other entries are zero. */
 BIPP_B200_EXPORT BippError bipp_pipeline_last_eigenvalues(bipp_pipeline_t pl, double* d, int* nReduced);
 /* Accumulated device time (ms) per stage since the last reset (7 values): [0] eigensolver,
  * [1] virtual visibilities, [2] NUFFT point preparation and sort, [3] spreading kernel,
