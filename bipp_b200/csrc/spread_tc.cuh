@@ -213,7 +213,36 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     const int lo = (int)((long long)it.load * it.part / it.nparts);
     const int hi = (int)((long long)it.load * (it.part + 1) / it.nparts);
     const int nvis = hi - lo;
+    // thread (visit v, role a): a = 0..3: x positions 4a..4a+3, a = 4, 5: y positions,
+    // a = 6, 7: w planes 4(a-6)..+3 and channels 2(a-6), 2(a-6)+1. The point data of the
+    // next phase are loaded into registers while the current phase is built.
+    const int pv = tid & 15, pa = tid >> 4;
     int ri = 0;
+    int pfL = 0;
+    float pfD = 0.f;
+    float2 pfX0 = make_float2(0.f, 0.f), pfX1 = make_float2(0.f, 0.f);
+    auto fetch = [&](int vb) {
+      if (pv < min(kTcVisits, nvis - vb)) {
+        const int q = lo + vb + pv;
+        while (q >= rPre[ri + 1]) ++ri;
+        const int p = rBeg[ri] + (q - rPre[ri]);
+        const PtRec* pr = rec + p;
+        if (pa < 4) {
+          pfL = __ldg(&pr->ix0);
+          pfD = __ldg(&pr->dx);
+        } else if (pa < 6) {
+          pfL = __ldg(&pr->iy0);
+          pfD = __ldg(&pr->dy);
+        } else {
+          pfL = __ldg(&pr->iw0);
+          pfD = __ldg(&pr->dw);
+          const int c = 2 * (pa - 6);
+          pfX0 = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+          pfX1 = (c + 1 < nch) ? vals[(long long)(c + 1) * valStride + p] : make_float2(0.f, 0.f);
+        }
+      }
+    };
+    fetch(0);
     for (int v0 = 0; v0 < nvis; v0 += kTcVisits) {
       const int nk = min(kTcVisits, nvis - v0);
       const int steps = (nk + 7) >> 3;
@@ -226,60 +255,49 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           sOk = 0;
         }
       }
-      // per-visit tables, thread (visit v, role a): a = 0..3: x positions 4a..4a+3,
-      // a = 4, 5: y positions, a = 6, 7: w planes 4(a-6)..+3 and channels 2(a-6), 2(a-6)+1
+      // per-visit tables from the prefetched point data
       {
-        const int v = tid & 15, a = tid >> 4;
-        float* tab = (a < 4) ? ex + (4 * a) * kTcVS : (a < 6) ? ey + (4 * (a - 4)) * kTcVS : ew + (4 * (a - 6)) * kTcVS;
-        if (v < nk) {
-          const int q = lo + v0 + v;
-          while (q >= rPre[ri + 1]) ++ri;
-          const int p = rBeg[ri] + (q - rPre[ri]);
-          const PtRec pr = rec[p];
-          int l, first;
-          float d;
-          if (a < 4) {
-            l = pr.ix0 - x0;
+        float* tab = (pa < 4) ? ex + (4 * pa) * kTcVS : (pa < 6) ? ey + (4 * (pa - 4)) * kTcVS : ew + (4 * (pa - 6)) * kTcVS;
+        if (pv < nk) {
+          int l = pfL, first;
+          if (pa < 4) {
+            l -= x0;
             l = ((l % g.nx) + g.nx) % g.nx;
             if (l > g.nx / 2) l -= g.nx;
-            d = pr.dx;
-            first = 4 * a;
-          } else if (a < 6) {
-            l = pr.iy0 - y0;
+            first = 4 * pa;
+          } else if (pa < 6) {
+            l -= y0;
             l = ((l % g.ny) + g.ny) % g.ny;
             if (l > g.ny / 2) l -= g.ny;
-            d = pr.dy;
-            first = 4 * (a - 4);
+            first = 4 * (pa - 4);
           } else {
-            l = pr.iw0 - w0;
-            d = pr.dw;
-            first = 4 * (a - 6);
+            l -= w0;
+            first = 4 * (pa - 6);
           }
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int j = first + i - l;   // support index of tile position first + i
-            tab[i * kTcVS + v] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - d) * invHalf, g.beta) : 0.f;
+            tab[i * kTcVS + pv] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - pfD) * invHalf, g.beta) : 0.f;
           }
-          if (a >= 6) {
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-              const int c = 2 * (a - 6) + cc;
-              const float2 x = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
-              val[(2 * c) * kTcVS + v] = x.x;
-              val[(2 * c + 1) * kTcVS + v] = x.y;
-            }
+          if (pa >= 6) {
+            const int c = 2 * (pa - 6);
+            val[(2 * c) * kTcVS + pv] = pfX0.x;
+            val[(2 * c + 1) * kTcVS + pv] = pfX0.y;
+            val[(2 * c + 2) * kTcVS + pv] = pfX1.x;
+            val[(2 * c + 3) * kTcVS + pv] = pfX1.y;
           }
-        } else if (v < steps * 8) {
+        } else if (pv < steps * 8) {
           // padding visits of the last K-step contribute nothing (values too: 0 x stale
           // shared memory could be 0 x NaN)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) tab[i * kTcVS + v] = 0.f;
-          if (a >= 6)
-            for (int c = 4 * (a - 6); c < 4 * (a - 6) + 4; ++c) val[c * kTcVS + v] = 0.f;
+          for (int i = 0; i < 4; ++i) tab[i * kTcVS + pv] = 0.f;
+          if (pa >= 6)
+            for (int c = 4 * (pa - 6); c < 4 * (pa - 6) + 4; ++c) val[c * kTcVS + pv] = 0.f;
         }
       }
       __syncthreads();
       if (!sOk) break;
+      if (v0 + kTcVisits < nvis) fetch(v0 + kTcVisits);
       // A: row tid (cell xm, ym), 8 visits per K-step
       for (int s = 0; s < steps; ++s) {
         float h[8], l[8];
