@@ -208,8 +208,8 @@ def measured_peaks():
 def profiled_traffic_per_grid_byte():
     """DRAM bytes per grid byte of one spreading launch, from the committed ncu summary
     (dram__bytes_read.sum + dram__bytes_write.sum of one launch / that launch's slab
-    bytes); writes of the slab are ~90% of it and the reads follow the slab's points."""
-    path = os.path.join(ROOT, "profiles", "spread_warp_kernel_c2.md")
+    bytes): the slab is written once and the reads follow the slab's points."""
+    path = os.path.join(ROOT, "profiles", "spread_tc_kernel_c2.md")
     try:
         with open(path) as f:
             for ln in f:
