@@ -594,7 +594,7 @@ static void nufft_transform_lattice(bipp_nufft_s* p, long long n, long long ld) 
   baseline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(g, bp, p->core.cursor(), p->core.records(), p->core.values(),
                                                        p->core.value_stride(), p->core.sincos64() ? 1 : 0,
                                                        p->core.corr_terms() ? 1 : 0, p->core.su(), p->core.sv(),
-                                                       p->core.zero_acc());
+                                                       p->core.zero_acc(), p->core.channels());
   B2_CHECK_LAUNCH();
   p->core.execute(p->images.get<float>(), (long long)p->nPixel);
 }

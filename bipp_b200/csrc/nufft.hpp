@@ -45,7 +45,9 @@ public:
   void end_count(long long nPoints);
   int* cursor() { return cursor_.get<int>(); }
   PtRec* records() { return rec_.get<PtRec>(); }
+  // values of the sorted points, [point][channel] (channels() per point)
   float2* values() { return vals_.get<float2>(); }
+  // capacity in points of records() / values() (the scatter kernels' bounds guard)
   long long value_stride() const { return valStride_; }
   // per-channel accumulator of zero-baseline values (added to every pixel)
   double* zero_acc() { return zeroAcc_.get<double>(); }

@@ -177,7 +177,7 @@ static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long
 // pass 2: scatter records + values (channel-major: vals[ch][sortedIndex])
 static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
                                         const long long* __restrict__ chunkPairOffset, PtRec* __restrict__ rec,
-                                        float2* __restrict__ vals, long long valStride, int sincos64) {
+                                        float2* __restrict__ vals, long long valStride, int sincos64, int nchAll) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     int lo = 0, hi = P.nSteps;
@@ -213,7 +213,7 @@ static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, lo
     const float2* vvb = P.vv + (long long)st * P.vvStepStride + r + (long long)s * P.Nmax;
     for (int l = 0; l < P.levels; ++l) {
       const float2 a = vvb[(long long)l * P.vvLevelStride];
-      vals[(long long)l * valStride + pos] = make_float2(wgt * (a.x * cs - a.y * sn), wgt * (a.x * sn + a.y * cs));
+      vals[(long long)pos * nchAll + l] = make_float2(wgt * (a.x * cs - a.y * sn), wgt * (a.x * sn + a.y * cs));
     }
   }
 }
@@ -248,7 +248,7 @@ static __global__ void baseline_count_kernel(NufftGeom g, BaselinePoints P, int*
 static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ cursor,
                                         PtRec* __restrict__ rec, float2* __restrict__ vals, long long valStride,
                                         int sincos64, int corrTerms, double su, double sv,
-                                        double* __restrict__ zeroAcc) {
+                                        double* __restrict__ zeroAcc, int nchAll) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
     const double u = (double)P.uvw[t] * P.uvwScale;
     const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
@@ -273,11 +273,11 @@ static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, in
     for (int l = 0; l < P.levels; ++l) {
       const float2 a = P.values[(long long)l * P.ldv + t];
       const float2 q = make_float2(a.x * cs - a.y * sn, a.x * sn + a.y * cs);
-      vals[(long long)l * valStride + pos] = q;
+      vals[(long long)pos * nchAll + l] = q;
       if (corrTerms) {
         const float fu = (float)(u / su), fv = (float)(v / sv);
-        vals[(long long)(P.levels + l) * valStride + pos] = make_float2(q.x * fu, q.y * fu);
-        vals[(long long)(2 * P.levels + l) * valStride + pos] = make_float2(q.x * fv, q.y * fv);
+        vals[(long long)pos * nchAll + P.levels + l] = make_float2(q.x * fu, q.y * fu);
+        vals[(long long)pos * nchAll + 2 * P.levels + l] = make_float2(q.x * fv, q.y * fv);
       }
     }
   }
@@ -519,7 +519,7 @@ spread_warp_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __
     }
     float2 v[CH];
 #pragma unroll
-    for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
+    for (int c = 0; c < CH; ++c) v[c] = (c < nch) ? vals[(long long)p * nch + c] : make_float2(0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < nIter; ++i) {
       const unsigned o = cellOff[i];

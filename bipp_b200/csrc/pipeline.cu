@@ -242,7 +242,7 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
     count_launch();
     pipeline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.cursor(), relD.get<long long>(),
                                                          p->core.records(), p->core.values(), p->core.value_stride(),
-                                                         p->core.sincos64() ? 1 : 0);
+                                                         p->core.sincos64() ? 1 : 0, p->core.channels());
     B2_CHECK_LAUNCH();
   }
   if (ms) {

@@ -237,8 +237,9 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           pfL = __ldg(&pr->iw0);
           pfD = __ldg(&pr->dw);
           const int c = 2 * (pa - 6);
-          pfX0 = (c < nch) ? vals[(long long)c * valStride + p] : make_float2(0.f, 0.f);
-          pfX1 = (c + 1 < nch) ? vals[(long long)(c + 1) * valStride + p] : make_float2(0.f, 0.f);
+          // values of a point are contiguous ([point][channel])
+          pfX0 = (c < nch) ? vals[(long long)p * nch + c] : make_float2(0.f, 0.f);
+          pfX1 = (c + 1 < nch) ? vals[(long long)p * nch + c + 1] : make_float2(0.f, 0.f);
         }
       }
     };
