@@ -500,8 +500,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   C* Cm = g.Cm + b * g.strideC + lvl * g.strideCLevel;
   const R* ks = g.kscale ? reinterpret_cast<const R*>(g.kscale) + b * g.strideK : nullptr;
 
-  __shared__ EA As[kGemmBK][kGemmBM + 1];
-  __shared__ EB Bs[kGemmBK][kGemmBN + 1];
+  // k-tiles of BK, double-buffered in shared memory; the next tile's global loads are
+  // issued before the current tile is multiplied
+  constexpr int BK = sizeof(C) == 8 ? 2 * kGemmBK : kGemmBK;
+  constexpr int LPT = kGemmBM * BK / kGemmThreads;   // elements of A (and of B) per thread
+  __shared__ EA As[2][BK][kGemmBM + 1];
+  __shared__ EB Bs[2][BK][kGemmBN + 1];
   const int tid = threadIdx.x;
   const int tr = tid % 16, tc = tid / 16;
   C acc[4][4];
@@ -509,47 +513,74 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[a][c] = mk(R(0), R(0));
-
-  for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
-    // load A tile: opA(i0+r, k0+kk), r<64, kk<8 -> 512 elements, 2 per thread
+  EA ra[LPT];
+  EB rb[LPT];
+  auto load = [&](int k0) {
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
+    for (int t = 0; t < LPT; ++t) {
       const int e = tid + t * kGemmThreads;
       int r, kk;
-      if (g.opA == 0) { r = e % kGemmBM; kk = e / kGemmBM; } else { kk = e % kGemmBK; r = e / kGemmBK; }
+      if (g.opA == 0) { r = e % kGemmBM; kk = e / kGemmBM; } else { kk = e % BK; r = e / BK; }
       const int i = i0 + r, k = k0 + kk;
       EA v = opzero<EA>();
       if (i < n && k < ke) {
         v = (g.opA == 0) ? A[i + (long long)k * g.lda] : opconj(A[k + (long long)i * g.lda]);
         if (ks) v = opscale(v, ks[k]);
       }
-      As[kk][r] = v;
+      ra[t] = v;
     }
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
+    for (int t = 0; t < LPT; ++t) {
       const int e = tid + t * kGemmThreads;
       int cidx, kk;
-      if (g.opB == 0) { kk = e % kGemmBK; cidx = e / kGemmBK; } else { cidx = e % kGemmBN; kk = e / kGemmBN; }
+      if (g.opB == 0) { kk = e % BK; cidx = e / BK; } else { cidx = e % kGemmBN; kk = e / kGemmBN; }
       const int j = j0 + cidx, k = k0 + kk;
       EB v = opzero<EB>();
       if (j < n && k < ke) v = (g.opB == 0) ? B[k + (long long)j * g.ldb] : opconj(B[j + (long long)k * g.ldb]);
-      Bs[kk][cidx] = v;
+      rb[t] = v;
     }
-    __syncthreads();
+  };
+  auto store = [&](int buf) {
 #pragma unroll
-    for (int kk = 0; kk < kGemmBK; ++kk) {
+    for (int t = 0; t < LPT; ++t) {
+      const int e = tid + t * kGemmThreads;
+      int r, kk;
+      if (g.opA == 0) { r = e % kGemmBM; kk = e / kGemmBM; } else { kk = e % BK; r = e / BK; }
+      As[buf][kk][r] = ra[t];
+    }
+#pragma unroll
+    for (int t = 0; t < LPT; ++t) {
+      const int e = tid + t * kGemmThreads;
+      int cidx, kk;
+      if (g.opB == 0) { kk = e % BK; cidx = e / BK; } else { cidx = e % kGemmBN; kk = e / kGemmBN; }
+      Bs[buf][kk][cidx] = rb[t];
+    }
+  };
+  if (kb < ke) {
+    load(kb);
+    store(0);
+  }
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    const bool more = k0 + BK < ke;
+    if (more) load(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
       EA av[4];
       EB bv[4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) av[a] = As[kk][tr + 16 * a];
+      for (int a = 0; a < 4; ++a) av[a] = As[buf][kk][tr + 16 * a];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) bv[c] = Bs[kk][tc + 16 * c];
+      for (int c = 0; c < 4; ++c) bv[c] = Bs[buf][kk][tc + 16 * c];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int c = 0; c < 4; ++c) opfma(acc[a][c], av[a], bv[c]);
     }
+    if (more) store(buf ^ 1);
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
