@@ -273,25 +273,28 @@ static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStrea
   }
 }
 
-// tensor-core spreading (up to 4 channels): persistent CTAs, 4 per SM
+// tensor-core spreading (4 or 8 channels): persistent CTAs, as many per SM as tensor
+// memory allows
+template <int CH>
 static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, const int* offs, const PtRec* rec,
                              const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
                              int slabPlanes, float2* out, int* errFlag) {
+  using S = TcShape<CH>;
   int dev = 0, sms = 148;
   B2_CUDA(cudaGetDevice(&dev));
   B2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  smem_optin(spread_tc_kernel, kTcSmem);
-  const int grid = std::max(1, std::min(nItems, sms * kTcMinBlocks));
+  smem_optin(spread_tc_kernel<CH>, S::Smem);
+  const int grid = std::max(1, std::min(nItems, sms * S::MinBlocks));
   count_launch();
-  spread_tc_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0, slabPlanes,
-                                                       out, errFlag);
+  spread_tc_kernel<CH><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0,
+                                                           slabPlanes, out, errFlag);
 }
 
 // BIPP_B200_SPREAD=warp selects the shared-memory-atomic spreader for every channel count
 static bool use_tensor_core_spread(int nch) {
   const char* e = std::getenv("BIPP_B200_SPREAD");
   if (e && std::string(e) == "warp") return false;
-  return nch <= kTcChan;
+  return nch <= kTcMaxChan;
 }
 
 // points per spreading part: heavier tiles are split so that no CTA serialises the
@@ -404,9 +407,9 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     }
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
     if (nItems > 0 && tc) {
-      launch_spread_tc(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(),
-                       valStride_, nch_, items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes,
-                       grid_.get<float2>(), errFlag_.get<int>());
+      auto launch = nch_ <= 4 ? launch_spread_tc<4> : launch_spread_tc<8>;
+      launch(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(), valStride_, nch_,
+             items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes, grid_.get<float2>(), errFlag_.get<int>());
       B2_CHECK_LAUNCH();
     } else if (nItems > 0) {
       const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];

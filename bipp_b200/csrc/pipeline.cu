@@ -396,7 +396,7 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
   return guard([&] {
     require(ctx && cfg && out, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(cfg->nAntenna > 0 && cfg->nAntenna <= 4096, "nAntenna must be in [1, 4096]");
-    require(cfg->nLevels >= 1 && cfg->nLevels <= 4, "nLevels must be in [1, 4]");
+    require(cfg->nLevels >= 1 && cfg->nLevels <= (size_t)kMaxPipelineLevels, "nLevels must be in [1, 8]");
     require(cfg->intervals && cfg->pixelN && cfg->uvwBasis, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(cfg->gridA >= 2 && cfg->gridB >= 2, "pixel lattice must be at least 2 x 2");
     require(cfg->filter >= 0 && cfg->filter <= 4, "unknown filter");

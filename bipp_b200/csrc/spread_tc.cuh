@@ -3,8 +3,8 @@
 // For one output tile of 16 x 8 (x, y) cells and 8 w-planes, the spread grid is a sum of
 // separable outer products over the points ("visits") that reach the tile:
 //     G[(x,y), (w,c)] = sum_p  phi_x,p(x) phi_y,p(y)  *  phi_w,p(w) v_p,c
-// i.e. the product of A (128 cells x K visits) and B (K visits x 64 columns: 8 planes x
-// 4 channels x re/im). Threads write A and B for 16 visits at a time into shared memory
+// i.e. the product of A (128 cells x K visits) and B (K visits x 16 CH columns: 8 planes x
+// CH = 4 or 8 channels x re/im). Threads write A and B for 16 visits at a time into shared memory
 // (canonical K-major, no swizzle), one thread issues tcgen05.mma (kind::tf32) into a
 // 128 x 64 FP32 accumulator in tensor memory, and the epilogue reads it back with
 // tcgen05.ld and writes the tile once. FP32 accuracy comes from the 3xTF32 split
@@ -23,35 +23,42 @@ constexpr int kTcThreads = 128;
 constexpr int kTcVisits = 16;                 // visits per phase
 constexpr int kTcSteps = kTcVisits / 8;       // MMA K-steps per phase (K = 8 for tf32)
 constexpr int kTcM = kTX * kTY;               // 128 accumulator rows (cells)
-constexpr int kTcN = kTW * 8;                 // 64 accumulator columns (plane x channel x re/im)
-constexpr int kTcChan = 4;                    // channels handled by the tensor-core kernel
-constexpr int kTcCols = 64;                   // tensor-memory columns allocated per CTA
-constexpr int kTcMinBlocks = 8;               // CTAs per SM (8 x 64 TMEM columns = all 512)
-// shared-memory layout (bytes); one K-step of A is 128 rows x 8 tf32, of B 64 rows x 8
+constexpr int kTcMaxChan = 8;                 // channels handled by the tensor-core kernel
+// shared-memory layout (bytes); one K-step of A is 128 rows x 8 tf32
 constexpr int kTcAStep = kTcM * 8 * 4;
-constexpr int kTcBStep = kTcN * 8 * 4;
-constexpr int kTcOffAhi = 0;
-constexpr int kTcOffAlo = kTcOffAhi + kTcSteps * kTcAStep;
-constexpr int kTcOffBhi = kTcOffAlo + kTcSteps * kTcAStep;
-constexpr int kTcOffBlo = kTcOffBhi + kTcSteps * kTcBStep;
 // per-visit kernel values at every tile position (zero outside the support) and the
 // channel values, stored position-major with a padded visit stride (conflict-free both
 // when a thread per visit writes them and when a thread per cell reads them)
 constexpr int kTcVS = kTcVisits + 1;
-constexpr int kTcOffEx = kTcOffBlo + kTcSteps * kTcBStep;  // float [16 x][kTcVS]
-constexpr int kTcOffEy = kTcOffEx + kTX * kTcVS * 4;       // float [8 y][kTcVS]
-constexpr int kTcOffEw = kTcOffEy + kTY * kTcVS * 4;       // float [8 w][kTcVS]
-constexpr int kTcOffVal = kTcOffEw + kTW * kTcVS * 4;      // float [8 (channel, re/im)][kTcVS]
-constexpr int kTcSmem = kTcOffVal + 8 * kTcVS * 4;
-static_assert(kTcM == 128 && kTcN == 64, "tile shape fixed by the MMA shape");
-static_assert(kTcOffEx % 1024 == 0, "operand blocks 1 KB aligned");
-static_assert(kTcMinBlocks * (kTcSmem + 512 + 1024) <= 233472, "shared memory (dynamic + static <= 512 B + 1 KB reserved) for kTcMinBlocks CTAs per SM");
-static_assert(kTcMinBlocks * kTcCols <= 512, "tensor memory for kTcMinBlocks CTAs per SM");
 static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mapping assumes 16 x 8 x 8 tiles, 16 visits");
 
-// instruction descriptor: D f32, A/B tf32, both K-major, N = 64, M = 128
-constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                              ((uint32_t)(kTcM >> 4) << 24);
+// Shape of the kernel for CH channels (4 or 8): accumulator 128 x N, N = 8 planes x CH
+// channels x re/im; one K-step of B is N rows x 8 tf32; CTAs per SM bounded by TMEM.
+template <int CH>
+struct TcShape {
+  static constexpr int N = kTW * 2 * CH;
+  static constexpr int Cols = N;                  // tensor-memory columns per CTA
+  static constexpr int MinBlocks = 512 / Cols;    // CTAs per SM (all 512 TMEM columns)
+  static constexpr int BStep = N * 8 * 4;
+  static constexpr int OffAhi = 0;
+  static constexpr int OffAlo = OffAhi + kTcSteps * kTcAStep;
+  static constexpr int OffBhi = OffAlo + kTcSteps * kTcAStep;
+  static constexpr int OffBlo = OffBhi + kTcSteps * BStep;
+  static constexpr int OffEx = OffBlo + kTcSteps * BStep;  // float [16 x][kTcVS]
+  static constexpr int OffEy = OffEx + kTX * kTcVS * 4;    // float [8 y][kTcVS]
+  static constexpr int OffEw = OffEy + kTY * kTcVS * 4;    // float [8 w][kTcVS]
+  static constexpr int OffVal = OffEw + kTW * kTcVS * 4;   // float [2 CH (channel, re/im)][kTcVS]
+  static constexpr int Smem = OffVal + 2 * CH * kTcVS * 4;
+  // instruction descriptor: D f32, A/B tf32, both K-major, N, M = 128
+  static constexpr uint32_t Idesc =
+      (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+  static_assert(CH == 4 || CH == 8, "4 or 8 channels");
+  static_assert(N % 16 == 0 && N <= 256, "MMA N for M = 128");
+  static_assert(OffEx % 1024 == 0, "operand blocks 1 KB aligned");
+  static_assert(MinBlocks * (Smem + 512 + 1024) <= 233472,
+                "shared memory (dynamic + static <= 512 B + 1 KB reserved) for MinBlocks CTAs per SM");
+};
+
 // spin limit of one wait on the MMA barrier (each try_wait suspends for a bounded time)
 constexpr int kTcSpin = 1 << 22;
 
@@ -67,11 +74,12 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
@@ -140,10 +148,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&r)[16]) {
 }
 
 // Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ...
-static __global__ void __launch_bounds__(kTcThreads, kTcMinBlocks)
+template <int CH>
+static __global__ void __launch_bounds__(kTcThreads, TcShape<CH>::MinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                  int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag) {
+  using S = TcShape<CH>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmemSlot;
@@ -152,10 +162,10 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t sbase = smem_u32(sm);
   const uint32_t bar = smem_u32(&mbar);
-  float* ex = reinterpret_cast<float*>(sm + kTcOffEx);
-  float* ey = reinterpret_cast<float*>(sm + kTcOffEy);
-  float* ew = reinterpret_cast<float*>(sm + kTcOffEw);
-  float* val = reinterpret_cast<float*>(sm + kTcOffVal);
+  float* ex = reinterpret_cast<float*>(sm + S::OffEx);
+  float* ey = reinterpret_cast<float*>(sm + S::OffEy);
+  float* ew = reinterpret_cast<float*>(sm + S::OffEw);
+  float* val = reinterpret_cast<float*>(sm + S::OffVal);
   if (tid == 0) {
     mbar_init(bar, 1);
     sOk = 1;
@@ -163,7 +173,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   __syncwarp();
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmemSlot)),
-                 "r"(kTcCols)
+                 "r"(S::Cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -214,13 +224,16 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     const int hi = (int)((long long)it.load * (it.part + 1) / it.nparts);
     const int nvis = hi - lo;
     // thread (visit v, role a): a = 0..3: x positions 4a..4a+3, a = 4, 5: y positions,
-    // a = 6, 7: w planes 4(a-6)..+3 and channels 2(a-6), 2(a-6)+1. The point data of the
-    // next phase are loaded into registers while the current phase is built.
+    // a = 6, 7: w planes 4(a-6)..+3 and channels CH/2 (a-6) .. CH/2 (a-5) - 1. The point
+    // data of the next phase are loaded into registers while the current phase is built.
+    constexpr int CPR = CH / 2;   // channels per value role
     const int pv = tid & 15, pa = tid >> 4;
     int ri = 0;
     int pfL = 0;
     float pfD = 0.f;
-    float2 pfX0 = make_float2(0.f, 0.f), pfX1 = make_float2(0.f, 0.f);
+    float2 pfX[CPR];
+#pragma unroll
+    for (int c = 0; c < CPR; ++c) pfX[c] = make_float2(0.f, 0.f);
     auto fetch = [&](int vb) {
       if (pv < min(kTcVisits, nvis - vb)) {
         const int q = lo + vb + pv;
@@ -236,10 +249,12 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
         } else {
           pfL = __ldg(&pr->iw0);
           pfD = __ldg(&pr->dw);
-          const int c = 2 * (pa - 6);
           // values of a point are contiguous ([point][channel])
-          pfX0 = (c < nch) ? vals[(long long)p * nch + c] : make_float2(0.f, 0.f);
-          pfX1 = (c + 1 < nch) ? vals[(long long)p * nch + c + 1] : make_float2(0.f, 0.f);
+#pragma unroll
+          for (int cc = 0; cc < CPR; ++cc) {
+            const int c = CPR * (pa - 6) + cc;
+            pfX[cc] = (c < nch) ? vals[(long long)p * nch + c] : make_float2(0.f, 0.f);
+          }
         }
       }
     };
@@ -281,11 +296,12 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
             tab[i * kTcVS + pv] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - pfD) * invHalf, g.beta) : 0.f;
           }
           if (pa >= 6) {
-            const int c = 2 * (pa - 6);
-            val[(2 * c) * kTcVS + pv] = pfX0.x;
-            val[(2 * c + 1) * kTcVS + pv] = pfX0.y;
-            val[(2 * c + 2) * kTcVS + pv] = pfX1.x;
-            val[(2 * c + 3) * kTcVS + pv] = pfX1.y;
+#pragma unroll
+            for (int cc = 0; cc < CPR; ++cc) {
+              const int c = CPR * (pa - 6) + cc;
+              val[(2 * c) * kTcVS + pv] = pfX[cc].x;
+              val[(2 * c + 1) * kTcVS + pv] = pfX[cc].y;
+            }
           }
         } else if (pv < steps * 8) {
           // padding visits of the last K-step contribute nothing (values too: 0 x stale
@@ -293,7 +309,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
 #pragma unroll
           for (int i = 0; i < 4; ++i) tab[i * kTcVS + pv] = 0.f;
           if (pa >= 6)
-            for (int c = 4 * (pa - 6); c < 4 * (pa - 6) + 4; ++c) val[c * kTcVS + pv] = 0.f;
+            for (int c = 2 * CPR * (pa - 6); c < 2 * CPR * (pa - 5); ++c) val[c * kTcVS + pv] = 0.f;
         }
       }
       __syncthreads();
@@ -307,28 +323,34 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           const int v = s * 8 + k;
           split_tf32(ex[xm * kTcVS + v] * ey[ym * kTcVS + v], h[k], l[k]);
         }
-        const uint32_t ah = sbase + kTcOffAhi + s * kTcAStep + tid * 16;
-        const uint32_t al = sbase + kTcOffAlo + s * kTcAStep + tid * 16;
+        const uint32_t ah = sbase + S::OffAhi + s * kTcAStep + tid * 16;
+        const uint32_t al = sbase + S::OffAlo + s * kTcAStep + tid * 16;
         st_shared_v4(ah, h[0], h[1], h[2], h[3]);
         st_shared_v4(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
         st_shared_v4(al, l[0], l[1], l[2], l[3]);
         st_shared_v4(al + kTcAStep / 2, l[4], l[5], l[6], l[7]);
       }
-      // B: row n = plane * 8 + channel * 2 + (re|im), this thread's half of the K-step
+      // B: row n = plane * 2 CH + channel * 2 + (re|im); TPR threads per row, each with
+      // VPT visits of the K-step
       {
-        const int n = tid & 63, kh = tid >> 6;
-        const int plane = n >> 3, cc = n & 7;
+        constexpr int TPR = kTcThreads / S::N, VPT = 8 / TPR;
+        const int n = tid % S::N, kh = tid / S::N;
+        const int plane = n / (2 * CH), cc = n % (2 * CH);
         for (int s = 0; s < steps; ++s) {
-          float h[4], l[4];
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            const int v = s * 8 + kh * 4 + kk;
-            split_tf32(ew[plane * kTcVS + v] * val[cc * kTcVS + v], h[kk], l[kk]);
+          for (int q = 0; q < VPT / 4; ++q) {
+            const int k0 = kh * VPT + 4 * q;   // first visit of this 16-byte group
+            float h[4], l[4];
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+              const int v = s * 8 + k0 + kk;
+              split_tf32(ew[plane * kTcVS + v] * val[cc * kTcVS + v], h[kk], l[kk]);
+            }
+            const uint32_t bh = sbase + S::OffBhi + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
+            const uint32_t bl = sbase + S::OffBlo + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
+            st_shared_v4(bh, h[0], h[1], h[2], h[3]);
+            st_shared_v4(bl, l[0], l[1], l[2], l[3]);
           }
-          const uint32_t bh = sbase + kTcOffBhi + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
-          const uint32_t bl = sbase + kTcOffBlo + s * kTcBStep + kh * (kTcBStep / 2) + n * 16;
-          st_shared_v4(bh, h[0], h[1], h[2], h[3]);
-          st_shared_v4(bl, l[0], l[1], l[2], l[3]);
         }
       }
       // make the operand writes visible to the tensor core, then one thread issues
@@ -337,13 +359,13 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       if (tid == 0) {
         tc_fence_after();
         for (int s = 0; s < steps; ++s) {
-          const uint64_t dAh = tc_desc(sbase + kTcOffAhi + s * kTcAStep, kTcAStep / 2, 128);
-          const uint64_t dAl = tc_desc(sbase + kTcOffAlo + s * kTcAStep, kTcAStep / 2, 128);
-          const uint64_t dBh = tc_desc(sbase + kTcOffBhi + s * kTcBStep, kTcBStep / 2, 128);
-          const uint64_t dBl = tc_desc(sbase + kTcOffBlo + s * kTcBStep, kTcBStep / 2, 128);
-          tc_mma(tmem, dAh, dBh, (v0 > 0 || s > 0) ? 1u : 0u);
-          tc_mma(tmem, dAh, dBl, 1u);
-          tc_mma(tmem, dAl, dBh, 1u);
+          const uint64_t dAh = tc_desc(sbase + S::OffAhi + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dAl = tc_desc(sbase + S::OffAlo + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dBh = tc_desc(sbase + S::OffBhi + s * S::BStep, S::BStep / 2, 128);
+          const uint64_t dBl = tc_desc(sbase + S::OffBlo + s * S::BStep, S::BStep / 2, 128);
+          tc_mma(tmem, dAh, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
+          tc_mma(tmem, dAh, dBl, S::Idesc, 1u);
+          tc_mma(tmem, dAl, dBh, S::Idesc, 1u);
         }
         tc_commit(bar);
         pending = true;
@@ -366,17 +388,18 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       const int twl = tw - tw0;
       const long long rowOff = (long long)(y0 + ym) * g.nx + (x0 + xm);
       const long long planeStride = (long long)g.ny * g.nx;
+      constexpr int PPB = 16 / (2 * CH);   // planes per 16-column block
 #pragma unroll
-      for (int q = 0; q < kTcN / 16; ++q) {
+      for (int q = 0; q < S::N / 16; ++q) {
         float r[16];
         tmem_ld16(tmemWarp + (uint32_t)(q * 16), r);
 #pragma unroll
-        for (int pl = 0; pl < 2; ++pl) {
-          const int plane = twl * kTW + q * 2 + pl;
+        for (int pl = 0; pl < PPB; ++pl) {
+          const int plane = twl * kTW + q * PPB + pl;
 #pragma unroll
-          for (int c = 0; c < kTcChan; ++c) {
+          for (int c = 0; c < CH; ++c) {
             if (c < nch) {
-              const float2 v = make_float2(r[pl * 8 + 2 * c], r[pl * 8 + 2 * c + 1]);
+              const float2 v = make_float2(r[pl * 2 * CH + 2 * c], r[pl * 2 * CH + 2 * c + 1]);
               float2* dst = grid + ((long long)c * slabPlanes + plane) * planeStride + rowOff;
               if (it.nparts == 1) {
                 *dst = v;
@@ -402,7 +425,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::Cols) : "memory");
   }
 }
 

@@ -235,6 +235,25 @@ def test_pipeline_batched_vs_fp64_oracle(ctx, keep):
     pl.close()
 
 
+@pytest.mark.parametrize("n_levels", [6, 8])
+def test_pipeline_many_levels_vs_fp64_oracle(ctx, n_levels):
+    """More than 4 energy levels (the 8-channel tensor-core spreader)."""
+    import bipp_b200 as bipp
+
+    cfg, obs, s, xyz = _pipeline_case(n_ant=48, n_steps=4, image=40)
+    d_all = np.concatenate([bb.eigh_gram(cfg.wl, s[k], np.eye(cfg.n_antenna), xyz[k])[1] for k in range(2)])
+    intervals = bb.infer_intervals(n_levels, 1.0, "log", 0.0, np.inf, d_all)
+    ref_img, _ = _oracle_pipeline(cfg, obs, s, xyz, intervals)
+    n = cfg.image_size
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, _lattice(obs, n), obs.lmn[:, 2], obs.basis, tolerance=1e-6,
+                       chunk_steps=4)
+    pl.process(s, xyz, np.full(s.shape[0], cfg.wl))
+    img = pl.images()
+    pl.close()
+    assert img.shape[0] == n_levels
+    assert _rel_l2(img.T, ref_img) <= 1e-4
+
+
 def test_pipeline_plain_matches_batched(ctx):
     import bipp_b200 as bipp
 
