@@ -30,7 +30,20 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-steps/s at 512 antennas, 1024^2 px (4 levels, NUFFT eps 1e-5)"
+METRIC_C5 = "time-steps/s at 1024 antennas, 8 channels, 2048^2 px (8 levels, NUFFT eps 1e-5)"
 UNIT = "time-steps/s"
+
+
+def metric_of(args):
+    return METRIC_C5 if args.workload == "c5" else METRIC
+
+
+def workload_text(args):
+    if args.workload == "c5":
+        return (f"c5: {args.antennas} antennas log-radial 50 km, 25% flagged/step, 8 channels 1.5-3 m, 500 sources, "
+                f"8 levels, {args.image}^2 px over 16 deg, eps 1e-5; {args.time_steps} of 4096 time steps")
+    return (f"c2: {args.antennas} antennas log-radial 35 km, 380-512 kept/step, 200 sources, 4 levels, "
+            f"{args.image}^2 px over 16 deg, eps 1e-5")
 
 
 def parse():
@@ -39,18 +52,36 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--time-steps", type=int, default=2048)
-    ap.add_argument("--antennas", type=int, default=512)
-    ap.add_argument("--image", type=int, default=1024)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
+                    help="c2: 512 antennas, 2048 steps, 1024^2 px, 4 levels (the headline); c5: 1024 antennas, "
+                         "8 frequency channels, 2048^2 px, 8 levels (bounded to --time-steps time steps)")
+    ap.add_argument("--time-steps", type=int, default=None)
+    ap.add_argument("--antennas", type=int, default=None)
+    ap.add_argument("--image", type=int, default=None)
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
-    ap.add_argument("--chunk-steps", type=int, default=1024, help="time steps per eigensolver/VV chunk")
+    ap.add_argument("--chunk-steps", type=int, default=None, help="entries per eigensolver/VV chunk")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stages", action="store_true", help="report per-stage device times")
     ap.add_argument("--plain-steps", type=int, default=16,
                     help="time steps of the plain-GPU comparison (one NUFFT per step and level); 0 skips it")
-    return ap.parse_args()
+    a = ap.parse_args()
+    dflt = {"c2": dict(time_steps=2048, antennas=512, image=1024, chunk_steps=1024),
+            "c5": dict(time_steps=128, antennas=1024, image=2048, chunk_steps=128)}[a.workload]
+    for k, v in dflt.items():
+        if getattr(a, k) is None:
+            setattr(a, k, v)
+    return a
+
+
+def workload_config(args, seed_offset=0):
+    from bipp_b200 import simulate as sim
+
+    if args.workload == "c5":
+        return sim.config_c5(n_antenna=args.antennas, image_size=args.image, n_steps=args.time_steps,
+                             keep=(args.antennas * 3 // 4, args.antennas * 3 // 4), seed=5 + seed_offset)
+    return sim.config_c2(n_antenna=args.antennas, image_size=args.image, n_steps=args.time_steps, seed=2 + seed_offset)
 
 
 class ClockSampler:
@@ -107,23 +138,28 @@ class ClockSampler:
 
 
 def make_inputs(cfg, rank, device):
-    """Seeded C2-shaped inputs on the GPU: S^T per step (column-major S), xyz, wl."""
+    """Seeded inputs on the GPU, one entry per (time step, frequency channel), entry
+    t * n_channels + c: S^T (column-major S), xyz, wl."""
     import torch
 
     from bipp_b200 import simulate as sim
 
     obs = sim.observation(cfg)
     masks = sim.keep_masks(cfg)
-    T, N = cfg.n_steps, cfg.n_antenna
-    S = torch.empty((T, N, N), dtype=torch.complex64, device=device)
-    xyz = torch.empty((T, N, 3), dtype=torch.float64, device=device)
-    chunk = 64
+    T, N, C = cfg.n_steps, cfg.n_antenna, cfg.n_channels
+    wls = cfg.wavelengths()
+    S = torch.empty((T * C, N, N), dtype=torch.complex64, device=device)
+    xyz = torch.empty((T * C, N, 3), dtype=torch.float64, device=device)
+    wl = torch.empty((T * C,), dtype=torch.float64, device=device)
+    chunk = 64 if N <= 512 else 16
     for s0 in range(0, T, chunk):
         steps = list(range(s0, min(T, s0 + chunk)))
-        s, x = sim.visibilities(obs, steps, device=device, dtype=torch.complex64, masks=masks)
-        S[s0:s0 + len(steps)] = s.transpose(1, 2)
-        xyz[s0:s0 + len(steps)] = x
-    wl = torch.full((T,), cfg.wl, dtype=torch.float64, device=device)
+        for c in range(C):
+            s, x = sim.visibilities(obs, steps, device=device, dtype=torch.complex64, masks=masks, wl=float(wls[c]),
+                                    noise_key=c)
+            S[s0 * C + c:(s0 + len(steps)) * C:C] = s.transpose(1, 2)
+            xyz[s0 * C + c:(s0 + len(steps)) * C:C] = x
+            wl[s0 * C + c:(s0 + len(steps)) * C:C] = float(wls[c])
     torch.cuda.synchronize()
     return obs, S, xyz, wl
 
@@ -134,30 +170,33 @@ def lattice_of(obs, n):
     return (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
 
 
-def calibrate_levels(ctx, cfg, S, xyz, n_cal=64):
-    """Energy levels: k-means (log) over positive eigenvalues of the first n_cal steps
+def calibrate_levels(ctx, cfg, S, xyz, wl, n_cal=64):
+    """Energy levels: k-means (log) over positive eigenvalues of the first n_cal entries
     (python/bipp/parameter_estimator.py:55-105), then frozen."""
     import bipp_b200 as bipp
     from bipp_b200.parameter_estimator import infer_intervals
 
-    n_cal = min(n_cal, cfg.n_steps)
+    n_cal = min(n_cal, S.shape[0])
     s_host = S[:n_cal].transpose(1, 2).cpu().numpy()
     x_host = xyz[:n_cal].cpu().numpy()
-    _, d, nred, _ = bipp.eigh_gram_batched(np.full(n_cal, cfg.wl, np.float32), s_host, x_host, ctx=ctx)
+    w_host = wl[:n_cal].cpu().numpy().astype(np.float32)
+    _, d, nred, _ = bipp.eigh_gram_batched(w_host, s_host, x_host, ctx=ctx)
     return infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d)
 
 
-def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, threads=None):
+def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, threads=None, wl=None):
     """The reference's CPU path (compiled reference sources) on a bounded sample:
-    eigh_gram<float> + virtual_vis<float> per level on n_eig_steps steps, and the
-    reference direct sum nuft_sum<double> over all baselines of one step for n_pix
+    eigh_gram<float> + virtual_vis<float> per level on n_eig_steps entries, and the
+    reference direct sum nuft_sum<double> over all baselines of one entry for n_pix
     pixels, extrapolated to the full image and all levels (the reference's CPU NUFFT,
-    neonufft, is not available). Returns (steps/s, cores, sample description)."""
+    neonufft, is not available). A time step holds cfg.n_channels entries. Returns
+    (time-steps/s, cores, sample description)."""
     from oracle import ref
 
     from bipp_b200 import simulate as sim
 
     threads = threads or os.cpu_count() or 1
+    wl = float(cfg.wavelengths()[0]) if wl is None else wl
     ref.set_threads(threads)
     obs = sim.observation(cfg)
     N = cfg.n_antenna
@@ -168,7 +207,7 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
         s = S[k].transpose(0, 1).cpu().numpy().T  # logical S
         x = xyz[k].cpu().numpy().astype(np.float32)
         t0 = time.perf_counter()
-        v, d, nr, sc = ref.eigh_gram(cfg.wl, s, w, x, dtype=np.float32)
+        v, d, nr, sc = ref.eigh_gram(wl, s, w, x, dtype=np.float32)
         t1 = time.perf_counter()
         vvs = []
         for lo, hi in intervals:
@@ -180,7 +219,7 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
     t_eig /= n_eig_steps
     t_vv /= n_eig_steps
     vvs, x = last
-    uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / cfg.wl)
+    uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / wl)
     rng = np.random.default_rng(0)
     pix = rng.choice(obs.lmn.shape[0], n_pix, replace=False)
     lmn = obs.lmn[pix]
@@ -189,11 +228,11 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
     ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], lmn[:, 0], lmn[:, 1], lmn[:, 2], threads=threads)
     t_pix = time.perf_counter() - t0
     t_nuft = t_pix * (obs.lmn.shape[0] / n_pix) * len(intervals)
-    per_step = t_eig + t_vv + t_nuft
-    desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} on {n_eig_steps} steps "
-            f"({t_eig:.3f}+{t_vv:.3f} s/step); nuft_sum<double> all {N * N} baselines x {n_pix} px "
+    per_step = (t_eig + t_vv + t_nuft) * cfg.n_channels
+    desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} on {n_eig_steps} entries "
+            f"({t_eig:.3f}+{t_vv:.3f} s/entry); nuft_sum<double> all {N * N} baselines x {n_pix} px "
             f"({t_pix:.2f} s) extrapolated to {obs.lmn.shape[0]} px x {len(intervals)} levels "
-            f"({t_nuft:.1f} s/step); neonufft unavailable")
+            f"({t_nuft:.1f} s/entry); {cfg.n_channels} entries per time step; neonufft unavailable")
     return 1.0 / per_step, threads, desc
 
 
@@ -254,10 +293,12 @@ def run_reference(args):
 
     from bipp_b200 import simulate as sim
 
-    cfg = sim.config_c2(n_antenna=args.antennas, image_size=args.image, n_steps=max(8, args.steps + args.warmup))
+    args.time_steps = max(8, args.steps + args.warmup)
+    cfg = workload_config(args)
     obs = sim.observation(cfg)
     masks = sim.keep_masks(cfg)
-    s, x = sim.visibilities(obs, list(range(cfg.n_steps)), dtype=torch.complex64, masks=masks)
+    wl0 = float(cfg.wavelengths()[0])
+    s, x = sim.visibilities(obs, list(range(cfg.n_steps)), dtype=torch.complex64, masks=masks, wl=wl0)
     S = s.transpose(1, 2)
     from bipp_b200.parameter_estimator import infer_intervals
     from oracle import ref
@@ -265,22 +306,22 @@ def run_reference(args):
     ref.set_threads(os.cpu_count() or 1)
     d_all = []
     for k in range(2):
-        _, d, _, _ = ref.eigh_gram(cfg.wl, s[k].numpy(), np.eye(cfg.n_antenna), x[k].numpy().astype(np.float32),
+        _, d, _, _ = ref.eigh_gram(wl0, s[k].numpy(), np.eye(cfg.n_antenna), x[k].numpy().astype(np.float32),
                                    dtype=np.float32)
         d_all.append(d)
     intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, np.concatenate(d_all))
     vals = []
     for k in range(args.warmup + args.steps):
-        v, cores, desc = cpu_reference_sample(cfg, S[k:k + 1], x[k:k + 1], intervals, n_eig_steps=1, n_pix=1024)
+        v, cores, desc = cpu_reference_sample(cfg, S[k:k + 1], x[k:k + 1], intervals, n_eig_steps=1, n_pix=1024,
+                                              wl=wl0)
         if k >= args.warmup:
             vals.append(v)
     value = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": metric_of(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded C2-shaped observation)",
-            "config": {"workload": "c2: 512 antennas log-radial 35 km, 380-512 kept/step, 200 sources, 4 levels, "
-                                   "1024^2 px over 16 deg, eps 1e-5", "time_steps_per_batch": args.time_steps},
+            "data": "synthetic (seeded observation of the workload's shape)",
+            "config": {"workload": workload_text(args), "time_steps_per_batch": args.time_steps},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -307,14 +348,16 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     device = torch.device("cuda", local)
     ctx = bipp.Context("GPU", device=local)
-    cfg = sim.config_c2(n_antenna=args.antennas, image_size=args.image, n_steps=args.time_steps, seed=2 + rank)
+    cfg = workload_config(args, rank)
     obs, S, xyz, wl = make_inputs(cfg, rank, device)
-    intervals = calibrate_levels(ctx, cfg, S, xyz)
+    intervals = calibrate_levels(ctx, cfg, S, xyz, wl)
     n = cfg.image_size
     pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
-                       tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, cfg.n_steps), max_steps=cfg.n_steps,
+                       tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, S.shape[0]), max_steps=S.shape[0],
                        mode=args.mode)
-    T = cfg.n_steps
+    T = S.shape[0]  # entries: time steps x channels
+    S_bytes = S.numel() * 8
+    T_steps = cfg.n_steps
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
 
     def one_step():
@@ -342,7 +385,7 @@ def main():
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
-    value = args.steps * T * world / (ms_max / 1000.0)
+    value = args.steps * T_steps * world / (ms_max / 1000.0)
 
     # images: one reduction of the level images over ranks per run (SUM, to rank 0)
     img = torch.empty((cfg.n_levels, n * n), dtype=torch.float32, device=device)
@@ -368,7 +411,7 @@ def main():
     # time and one NUFFT per step and level (no batching across steps or levels)
     plain = None
     if rank == 0 and args.plain_steps > 0 and args.mode == "batched":
-        ns = min(args.plain_steps, T)
+        ns = min(args.plain_steps * cfg.n_channels, T)
         pp = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
                            tolerance=cfg.eps, chunk_steps=1, max_steps=ns, mode="plain")
         pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())  # warm-up
@@ -379,8 +422,8 @@ def main():
         pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())
         p1.record(stream)
         torch.cuda.synchronize()
-        pv = ns / (p0.elapsed_time(p1) / 1000.0)
-        plain = {"value": pv, "unit": UNIT, "sample": f"first {ns} time steps of the batch",
+        pv = ns / cfg.n_channels / (p0.elapsed_time(p1) / 1000.0)
+        plain = {"value": pv, "unit": UNIT, "sample": f"first {ns} entries (time step x channel) of the batch",
                  "chosen_over_plain": value / pv}
         pp.close()
 
@@ -409,7 +452,7 @@ def main():
         ems = torch.tensor([e0.elapsed_time(e1)], device=device, dtype=torch.float64)
         if world > 1:
             dist.all_reduce(ems, op=dist.ReduceOp.MAX)
-        e2e = {"value": args.e2e_steps * T * world / (float(ems.item()) / 1000.0), "unit": UNIT,
+        e2e = {"value": args.e2e_steps * T_steps * world / (float(ems.item()) / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": int(S_h.numel() * 8 + xyz_h.numel() * 8 + wl_h.numel() * 8),
                "d2h_bytes_per_step": int(img_h.numel() * 4)}
 
@@ -417,21 +460,21 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             Sc = S_h if not args.no_e2e else S  # noqa: F821
-            v, cores, desc = cpu_reference_sample(cfg, Sc, xyz, intervals)
+            v, cores, desc = cpu_reference_sample(cfg, Sc, xyz, intervals, wl=float(wl[0].item()))
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": metric_of(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded C2-shaped observation, generated on the GPU)",
-                "config": {"workload": "c2: 512 antennas log-radial 35 km, 380-512 kept/step, 200 sources, "
-                                       "4 levels, 1024^2 px over 16 deg, eps 1e-5",
-                           "time_steps_per_batch": T, "mode": args.mode, "parallelism": f"dp{world} (steps)",
-                           "l2": "inputs (4.3 GB/batch) larger than L2; no flush"},
+                "data": "synthetic (seeded observation of the workload's shape, generated on the GPU)",
+                "config": {"workload": workload_text(args),
+                           "time_steps_per_batch": T_steps, "entries_per_batch": T, "mode": args.mode,
+                           "parallelism": f"dp{world} (steps)",
+                           "l2": f"inputs ({S_bytes / 1e9:.1f} GB/batch) larger than L2; no flush"},
                 "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,
                 "cpu_baseline": cpu, "roofline": roof, "plain_gpu": plain}
         print(json.dumps(line))

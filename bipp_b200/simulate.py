@@ -53,6 +53,14 @@ class SimConfig:
     latitude_deg: float = -30.0
     seed: int = 0
     double: bool = False
+    n_channels: int = 1                      # frequency channels per time step
+    wl_range: Optional[Tuple[float, float]] = None   # channel wavelengths, linearly spaced
+
+    def wavelengths(self) -> np.ndarray:
+        """(n_channels,) wavelengths in metres."""
+        if self.n_channels == 1 or self.wl_range is None:
+            return np.full(self.n_channels, self.wl)
+        return np.linspace(self.wl_range[0], self.wl_range[1], self.n_channels)
 
 
 def config_c1(**kw) -> SimConfig:
@@ -71,6 +79,27 @@ def config_c2(**kw) -> SimConfig:
                   z_spread_m=10.0, wl=2.0, n_steps=2048, dt_s=8.0, n_src=200, flux=(0.01, 10.0),
                   src_radius_deg=8.0, noise_sigma=0.01, n_levels=4, image_size=1024,
                   fov_deg=16.0, eps=1e-5, keep=(380, 512), seed=2, double=False)
+    return dataclasses.replace(c, **kw)
+
+
+def config_c3(**kw) -> SimConfig:
+    """Precision study on one large step: 550 antennas log-radial to 65 km, wl 0.21 m,
+    1000 sources (0.001-1 Jy), 8 levels, 4096^2 px, NUFFT eps 1e-6."""
+    c = SimConfig(name="c3_n550_4096px", n_antenna=550, layout="logradial", extent_m=65000.0,
+                  z_spread_m=10.0, wl=0.21, n_steps=1, dt_s=8.0, n_src=1000, flux=(0.001, 1.0),
+                  src_radius_deg=2.0, noise_sigma=0.01, n_levels=8, image_size=4096,
+                  fov_deg=4.0, eps=1e-6, keep=None, seed=3, double=False)
+    return dataclasses.replace(c, **kw)
+
+
+def config_c5(**kw) -> SimConfig:
+    """Full pipeline: 1024 antennas log-radial to 50 km, 25% flagged per step, 4096 steps
+    x 8 channels (wl 1.5-3 m), 500 sources (0.001-10 Jy), 8 levels, 2048^2 px, eps 1e-5."""
+    c = SimConfig(name="c5_n1024_2048px", n_antenna=1024, layout="logradial", extent_m=50000.0,
+                  z_spread_m=10.0, wl=2.0, n_steps=4096, dt_s=8.0, n_src=500, flux=(0.001, 10.0),
+                  src_radius_deg=8.0, noise_sigma=0.01, n_levels=8, image_size=2048,
+                  fov_deg=16.0, eps=1e-5, keep=(768, 768), seed=5, double=False, n_channels=8,
+                  wl_range=(1.5, 3.0))
     return dataclasses.replace(c, **kw)
 
 
@@ -178,11 +207,14 @@ def keep_masks(cfg: SimConfig) -> np.ndarray:
 
 
 def visibilities(obs: Observation, steps: Sequence[int], device="cpu", dtype=None,
-                 masks: Optional[np.ndarray] = None) -> Tuple[torch.Tensor, torch.Tensor]:
-    """S (len(steps), N, N) and positions xyz (len(steps), N, 3) for the given steps.
-    Noise X ~ CN(0, sigma^2), E = (X + X^H)/2; diagonal zeroed; flagged antennas
-    become zero rows/columns."""
+                 masks: Optional[np.ndarray] = None, wl: Optional[float] = None,
+                 noise_key: int = 0) -> Tuple[torch.Tensor, torch.Tensor]:
+    """S (len(steps), N, N) and positions xyz (len(steps), N, 3) for the given steps at
+    wavelength wl (default cfg.wl). Noise X ~ CN(0, sigma^2), E = (X + X^H)/2; diagonal
+    zeroed; flagged antennas become zero rows/columns. noise_key separates the noise of
+    the frequency channels of one step."""
     cfg = obs.cfg
+    wl = cfg.wl if wl is None else wl
     if dtype is None:
         dtype = torch.complex128 if cfg.double else torch.complex64
     rdtype = torch.float64 if dtype == torch.complex128 else torch.float32
@@ -192,11 +224,11 @@ def visibilities(obs: Observation, steps: Sequence[int], device="cpu", dtype=Non
     dirs = torch.from_numpy(obs.src_dirs).to(device)
     flux = torch.from_numpy(obs.src_flux).to(device)
     # phase (B,Q,N) in float64, then complex
-    ph = (2 * math.pi / cfg.wl) * torch.einsum("qc,bnc->bqn", dirs, xyz_t)
+    ph = (2 * math.pi / wl) * torch.einsum("qc,bnc->bqn", dirs, xyz_t)
     a = torch.polar(torch.ones_like(ph), ph)                                 # exp(+i 2pi/wl r.p)
     s = torch.einsum("bqi,q,bqj->bij", a.conj(), flux.to(a.dtype), a)     # sum_q I_q e^{-i..(p_i-p_j)}
     g = torch.Generator(device=device)
-    g.manual_seed(cfg.seed * 1000003 + int(steps[0]))
+    g.manual_seed(cfg.seed * 1000003 + int(steps[0]) + 7919 * int(noise_key))
     sig = cfg.noise_sigma / math.sqrt(2.0)
     xr = torch.randn((len(steps), n, n), generator=g, device=device, dtype=torch.float64) * sig
     xi = torch.randn((len(steps), n, n), generator=g, device=device, dtype=torch.float64) * sig
