@@ -289,7 +289,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   }
   // 5. back-transform Y = Q Z -> T1
   mark(6);
-  if (Nmax <= kBtMaxRows) {
+  if (Nmax <= (sizeof(C) == 8 ? kBtMaxRows : kBtMaxRows / 2)) {
     // blocked: T of each 16-reflector block into G's storage (free between the triangular
     // inverse and the final GEMM), then one pass over Y per 16-column slice
     C* Tblk = reinterpret_cast<C*>(G);
@@ -299,17 +299,25 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     bt_larft_kernel<C, R><<<dim3(std::max(1, nblk), nb), 256, 0, st>>>(A, w.tau.template get<C>(), nred, Nmax, Tblk,
                                                                        tStride);
     B2_CHECK_LAUNCH();
-    const size_t smem = bt_apply_smem(Nmax, sizeof(C));
     const dim3 grid((Nmax + kBtCB - 1) / kBtCB, nb);
-#define B2_BT(KR)                                                                            \
+#define B2_BT(KR, NT)                                                                        \
   {                                                                                          \
-    auto k = bt_apply_kernel<C, R, KR>;                                                      \
+    auto k = bt_apply_kernel<C, R, KR, NT>;                                                  \
+    const size_t smem = bt_apply_smem(Nmax, sizeof(C), NT);                                  \
     smem_optin(k, smem);                                                                     \
     count_launch();                                                                          \
-    k<<<grid, kBtApplyThreads, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange);     \
+    k<<<grid, NT, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange);                  \
   }
-    const int kr = (Nmax + kBtRG - 1) / kBtRG;
-    if (kr <= 2) B2_BT(2) else if (kr <= 4) B2_BT(4) else if (kr <= 6) B2_BT(6) else B2_BT(8)
+    // 64 row groups of 256 threads up to 512 rows; 128 row groups of 512 threads above
+    if (Nmax <= 512) {
+      const int kr = (Nmax + 63) / 64;
+      if (kr <= 2) B2_BT(2, 256) else if (kr <= 4) B2_BT(4, 256) else if (kr <= 6) B2_BT(6, 256) else B2_BT(8, 256)
+    } else {
+      if constexpr (sizeof(C) == 8) {
+        const int kr = (Nmax + 127) / 128;
+        if (kr <= 6) B2_BT(6, 512) else B2_BT(8, 512)
+      }
+    }
 #undef B2_BT
     B2_CHECK_LAUNCH();
   } else {
@@ -318,13 +326,14 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       auto k = backtransform_kernel<C, R, 16>;
       smem_optin(k, smem16);
       count_launch();
-      k<<<dim3((Nmax + 15) / 16, nb), kBtThreads, smem16, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1);
+      k<<<dim3((Nmax + 15) / 16, nb), kBtThreads, smem16, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1,
+                                                                  krange);
     } else {
       const size_t smem4 = ((size_t)Nmax * 4 + Nmax + kBtThreads) * sizeof(C);
       auto k = backtransform_kernel<C, R, 4>;
       smem_optin(k, smem4);
       count_launch();
-      k<<<dim3((Nmax + 3) / 4, nb), kBtThreads, smem4, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1);
+      k<<<dim3((Nmax + 3) / 4, nb), kBtThreads, smem4, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1, krange);
     }
     B2_CHECK_LAUNCH();
   }

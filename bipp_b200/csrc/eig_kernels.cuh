@@ -1105,11 +1105,13 @@ constexpr int kBtThreads = 256;
 template <typename C, typename R, int kBtCols>
 __global__ void __launch_bounds__(kBtThreads)
 backtransform_kernel(const C* __restrict__ A, const C* __restrict__ taus, const R* __restrict__ Z,
-                     const int* __restrict__ nred, int Nmax, C* __restrict__ Y) {
+                     const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange) {
   const int b = blockIdx.y;
   const int n = nred[b];
   const int c0 = blockIdx.x * kBtCols;
   if (c0 >= n) return;
+  // only the eigenvector columns [krange[2b], krange[2b+1]) are needed
+  if (krange && (c0 + kBtCols <= krange[2 * b] || c0 >= krange[2 * b + 1])) return;
   const int nc = min(kBtCols, n - c0);
   extern __shared__ unsigned char smem_raw[];
   C* ys = reinterpret_cast<C*>(smem_raw);   // [Nmax][kBtCols]
@@ -1167,8 +1169,7 @@ backtransform_kernel(const C* __restrict__ A, const C* __restrict__ taus, const 
 // registers (thread: one column, every 16th row) for all blocks.
 constexpr int kBtNB = 16;             // reflectors per block
 constexpr int kBtCB = 16;             // columns of Y per CTA
-constexpr int kBtApplyThreads = 256;  // 16 row groups x 16 columns
-constexpr int kBtMaxRows = 512;       // Nmax limit of the register-resident kernel
+constexpr int kBtMaxRows = 1024;      // Nmax limit of the register-resident kernel
 
 // element r of reflector i (v(i+1) = 1, stored below the subdiagonal of column i)
 template <typename C, typename R>
@@ -1227,16 +1228,16 @@ bt_larft_kernel(const C* __restrict__ A, const C* __restrict__ taus, const int* 
   for (int e = tid; e < kBtNB * kBtNB; e += blockDim.x) To[e] = T[e / kBtNB][e % kBtNB];
 }
 
-// Thread (row group rg = tid / 4, column group cg = tid % 4) holds Y rows rg + 64 q and
-// columns 4 cg .. 4 cg + 3 of the CTA's 16-column slice: every V element loaded from
-// shared memory feeds 4 columns. V^H Y partial sums are reduced over the 8 row groups
-// of a warp with shuffles, then over the 8 warps in shared memory.
-constexpr int kBtRG = kBtApplyThreads / 4;   // 64 row groups
+// NT threads (256 up to 512 rows, 512 up to 1024 rows). Thread (row group rg = tid / 4,
+// column group cg = tid % 4) holds Y rows rg + NT/4 q and columns 4 cg .. 4 cg + 3 of the
+// CTA's 16-column slice: every V element loaded from shared memory feeds 4 columns. V^H Y
+// partial sums are reduced over the 8 row groups of a warp with shuffles, then over the
+// NT/32 warps in shared memory.
 constexpr int kBtVS = kBtNB + 2;             // padded row stride of the V block (16-byte aligned rows)
 constexpr int kBtJC = 2;                     // reflectors per register chunk
 
-template <typename C, typename R, int KR>
-__global__ void __launch_bounds__(kBtApplyThreads, sizeof(C) == 8 ? 2 : 1)
+template <typename C, typename R, int KR, int NT>
+__global__ void __launch_bounds__(NT, (sizeof(C) == 8 ? 512 : 256) / NT > 0 ? (sizeof(C) == 8 ? 512 : 256) / NT : 1)
 bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tStride, const R* __restrict__ Z,
                 const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange) {
   const int b = blockIdx.y;
@@ -1248,8 +1249,10 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
   if (c0 + kBtCB <= cLo || c0 >= cHi) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Vs = reinterpret_cast<C*>(smem_raw);              // [Nmax][kBtVS] block of reflectors (row-major)
-  C* red = Vs + (long long)Nmax * kBtVS;               // [8 warps][16 j][16 c]
-  C* Ts = red + 8 * kBtNB * kBtCB;                     // [16][16]
+  constexpr int RG = NT / 4, NW = NT / 32;
+  static_assert(NT >= kBtNB * kBtCB, "one thread per element of W");
+  C* red = Vs + (long long)Nmax * kBtVS;               // [NW warps][16 j][16 c]
+  C* Ts = red + NW * kBtNB * kBtCB;                    // [16][16]
   C* Wt = Ts + kBtNB * kBtNB;                          // [16 j][16 c]
   const C* Ab = A + (long long)b * Nmax * Nmax;
   const R* Zb = Z + (long long)b * Nmax * Nmax;
@@ -1258,7 +1261,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
   C y[KR][4];
 #pragma unroll
   for (int q = 0; q < KR; ++q) {
-    const int r = rg + kBtRG * q;
+    const int r = rg + RG * q;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int col = c0 + 4 * cg + u;
@@ -1291,7 +1294,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
         for (int u = 0; u < 4; ++u) w[a][u] = mk(R(0), R(0));
 #pragma unroll
       for (int q = 0; q < KR; ++q) {
-        const int r = rg + kBtRG * q;
+        const int r = rg + RG * q;
         if (r > i0 && r < n) {
           C v[kBtJC];
 #pragma unroll
@@ -1321,18 +1324,23 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
       }
     }
     __syncthreads();
-    // W[j][c] over the 8 warps, then Wt = T W (thread = (j, c))
+    // W[j][c] over the NW warps, then Wt = T W (thread = (j, c))
     {
-      const int j = tid / kBtCB, c = tid % kBtCB;
+      const bool act = tid < kBtNB * kBtCB;
+      const int j = (tid / kBtCB) % kBtNB, c = tid % kBtCB;
       C s0 = mk(R(0), R(0));
+      if (act) {
 #pragma unroll
-      for (int g = 0; g < 8; ++g) s0 = s0 + red[(g * kBtNB + j) * kBtCB + c];
+        for (int g = 0; g < NW; ++g) s0 = s0 + red[(g * kBtNB + j) * kBtCB + c];
+      }
       __syncthreads();
-      red[j * kBtCB + c] = s0;
+      if (act) red[j * kBtCB + c] = s0;
       __syncthreads();
-      C t = mk(R(0), R(0));
-      for (int l = j; l < kBtNB; ++l) cfma(t, Ts[j * kBtNB + l], red[l * kBtCB + c]);
-      Wt[j * kBtCB + c] = t;
+      if (act) {
+        C t = mk(R(0), R(0));
+        for (int l = j; l < kBtNB; ++l) cfma(t, Ts[j * kBtNB + l], red[l * kBtCB + c]);
+        Wt[j * kBtCB + c] = t;
+      }
     }
     __syncthreads();
     // Y -= V Wt, kBtJC reflectors at a time
@@ -1345,7 +1353,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
         for (int u = 0; u < 4; ++u) wt[a][u] = Wt[(kBtJC * jc + a) * kBtCB + 4 * cg + u];
 #pragma unroll
       for (int q = 0; q < KR; ++q) {
-        const int r = rg + kBtRG * q;
+        const int r = rg + RG * q;
         if (r > i0 && r < n) {
           C v[kBtJC];
 #pragma unroll
@@ -1368,7 +1376,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
   C* Yb = Y + (long long)b * Nmax * Nmax;
 #pragma unroll
   for (int q = 0; q < KR; ++q) {
-    const int r = rg + kBtRG * q;
+    const int r = rg + RG * q;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int col = c0 + 4 * cg + u;
@@ -1377,9 +1385,9 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
   }
 }
 
-// shared memory of bt_apply_kernel
-constexpr size_t bt_apply_smem(int Nmax, size_t complexBytes) {
-  return ((size_t)Nmax * kBtVS + 8 * kBtNB * kBtCB + kBtNB * kBtNB + kBtNB * kBtCB) * complexBytes;
+// shared memory of bt_apply_kernel with nt threads
+constexpr size_t bt_apply_smem(int Nmax, size_t complexBytes, int nt) {
+  return ((size_t)Nmax * kBtVS + (nt / 32) * kBtNB * kBtCB + kBtNB * kBtNB + kBtNB * kBtCB) * complexBytes;
 }
 
 }  // namespace bippb200

@@ -181,7 +181,7 @@ extern "C" BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl
       const size_t smem = ((size_t)N * 16 + N + kBtThreads) * sizeof(float2);
       smem_optin(backtransform_kernel<float2, float, 16>, smem);
       backtransform_kernel<float2, float, 16><<<dim3((N + 15) / 16, 1), kBtThreads, smem, st>>>(w.A, w.tau, w.Z, nred,
-                                                                                               N, w.T1);
+                                                                                               N, w.T1, nullptr);
     }
     GemmArgs<float2> g3{};
     g3.A = w.Linv; g3.strideA = n2; g3.lda = N; g3.opA = 1;
