@@ -4,7 +4,7 @@
   1024 x 1024 pixels over 16 degrees, NUFFT tolerance 1e-5; four time steps spread over
   the 4.5-hour observation (so that the w extent is the full one).
 - precision study: 550 antennas to 65 km, wavelength 0.21 m, 1000 sources, 8 levels,
-  4096 x 4096 pixels over 4 degrees, NUFFT tolerance 1e-6; one time step.
+  4096 x 4096 pixels over 4 degrees, NUFFT tolerance 1e-6; one time step, 16,384 pixels.
 - full pipeline: 1024 antennas to 50 km with 25% flagged, 8 frequency channels
   (1.5-3 m), 500 sources, 8 levels, 2048 x 2048 pixels over 16 degrees, tolerance 1e-5;
   two time steps x two channels (the extreme wavelengths) in one batch.
@@ -81,7 +81,7 @@ def test_pipeline_image_error_at_benchmark_shape(ctx):
 def test_pipeline_image_error_precision_study(ctx):
     from bipp_b200 import simulate as sim
 
-    err = _image_error(ctx, sim.config_c3(), [(0, 0)], 1024, 1)
+    err = _image_error(ctx, sim.config_c3(), [(0, 0)], 16384, 1)
     assert err <= 1e-4, err
 
 
