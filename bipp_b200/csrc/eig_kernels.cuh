@@ -668,11 +668,64 @@ __device__ __forceinline__ C warp_reduce_scatter(C (&v)[G], int lane) {
   return r;
 }
 
+// off-diagonal tile of 32 rows x 4*NG columns with all rows valid: fully unrolled, no
+// predicates. p: this lane's row at the tile's first column; vU, wU, x, y: based at the
+// tile's first column.
+template <bool UPD, int NG>
+__device__ __forceinline__ void trd_tile_full(float2* __restrict__ p, long long ld, const float2* __restrict__ vU,
+                                              const float2* __restrict__ wU, const float2* __restrict__ x,
+                                              float2 vr, float2 wr, float2 xr, float2& ry,
+                                              float2* __restrict__ y, int lane) {
+  float2 an[4];
+  float2* pn[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    pn[u] = p + u * ld;
+    an[u] = *pn[u];
+  }
+  const long long ld4 = 4 * ld;
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    float2 a[4];
+    float2* pa[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) { a[u] = an[u]; pa[u] = pn[u]; }
+    if (g < NG - 1) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { pn[u] = pa[u] + ld4; an[u] = *pn[u]; }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int c = 4 * g + u;
+      if (UPD) {
+        const float2 vc = vU[c], wc = wU[c];
+        float ax = a[u].x, ay = a[u].y;
+        ax = fmaf(-vr.x, wc.x, ax); ax = fmaf(-vr.y, wc.y, ax); ax = fmaf(-wr.x, vc.x, ax); ax = fmaf(-wr.y, vc.y, ax);
+        ay = fmaf(-vr.y, wc.x, ay); ay = fmaf(vr.x, wc.y, ay); ay = fmaf(-wr.y, vc.x, ay); ay = fmaf(wr.x, vc.y, ay);
+        a[u] = make_float2(ax, ay);
+        *pa[u] = a[u];
+      }
+      const float2 xc = x[c];
+      ry.x = fmaf(a[u].x, xc.x, fmaf(-a[u].y, xc.y, ry.x));
+      ry.y = fmaf(a[u].x, xc.y, fmaf(a[u].y, xc.x, ry.y));
+      a[u] = make_float2(fmaf(a[u].y, xr.y, a[u].x * xr.x), fmaf(-a[u].y, xr.x, a[u].x * xr.y));
+    }
+    const float2 s = warp_reduce_scatter<4>(a, lane);
+    if ((lane & 7) == 0) {
+      atomicAdd(&y[4 * g + (lane >> 3)].x, s.x);
+      atomicAdd(&y[4 * g + (lane >> 3)].y, s.y);
+    }
+  }
+}
+
 // One pass over the lower triangle of the mm x mm Hermitian block A0 (column-major, ld):
 // optionally the rank-2 update A -= vU wU^H + wU vU^H (UPD), and y += A x with the upper
-// triangle taken as the conjugate transpose of the lower one. Work unit: a 32 x 32 tile
-// per warp, lanes over rows; row sums stay in a register, column sums are reduced across
-// lanes G columns at a time; y (shared) is accumulated with shared-memory atomics.
+// triangle taken as the conjugate transpose of the lower one. Work unit: 32 rows x 16
+// columns per warp (units dealt round-robin), lanes over rows; row sums stay in a
+// register, column sums are reduced across lanes G columns at a time; y (shared) is
+// accumulated with shared-memory atomics. In single precision the units strictly below
+// the diagonal with all rows inside the block (most of them) take the unrolled,
+// predicate-free trd_tile_full; diagonal and edge units take the general loop.
 template <typename C, typename R, bool UPD>
 __device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int mm, const C* __restrict__ vU,
                                                const C* __restrict__ wU, const C* __restrict__ x,
@@ -681,15 +734,29 @@ __device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int m
   constexpr int LG = G == 8 ? 3 : G == 4 ? 2 : 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int nT = (mm + 31) >> 5;
-  const int nTiles = nT * (nT + 1) / 2;
+  constexpr int TC = 16, PR = 2;   // work unit: 32 rows x TC columns; row tile I holds PR (I + 1) units
+  const int nTiles = PR * nT * (nT + 1) / 2;
   const C zero = mk(R(0), R(0));
   for (int t = warp; t < nTiles; t += nwarp) {
-    int I = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
-    while ((I + 1) * (I + 2) / 2 <= t) ++I;
-    while (I * (I + 1) / 2 > t) --I;
-    const int J = t - I * (I + 1) / 2;
+    int I = (int)((sqrtf(8.0f * (float)(t / PR) + 1.0f) - 1.0f) * 0.5f);
+    while (PR * (I + 1) * (I + 2) / 2 <= t) ++I;
+    while (PR * I * (I + 1) / 2 > t) --I;
+    const int J = t - PR * I * (I + 1) / 2;
     const int r = I * 32 + lane;
     const bool rv = r < mm;
+    if constexpr (sizeof(C) == 8) {
+      if (J * TC + TC <= I * 32 && I * 32 + 32 <= mm) {
+        const C xr = x[r];
+        const C vr = UPD ? vU[r] : zero, wr = UPD ? wU[r] : zero;
+        C ry = zero;
+        trd_tile_full<UPD, TC / 4>(A0 + r + (long long)J * TC * ld, ld, UPD ? vU + J * TC : nullptr,
+                                   UPD ? wU + J * TC : nullptr, x + J * TC, vr, wr, xr, ry, y + J * TC, lane);
+        atomicAdd(&y[r].x, ry.x);
+        atomicAdd(&y[r].y, ry.y);
+
+        continue;
+      }
+    }
     C vr = zero, wr = zero, xr = zero;
     if (rv) {
       xr = x[r];
@@ -697,15 +764,15 @@ __device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int m
     }
     C ry = zero;
     C* rowp = A0 + (rv ? r : 0);
-    const int cEnd = min(mm, J * 32 + 32);
+    const int cEnd = min(mm, J * TC + TC);
     // loads of the next G columns are issued before the current ones are used
     C an[G];
 #pragma unroll
     for (int u = 0; u < G; ++u) {
-      const int c = J * 32 + u;
+      const int c = J * TC + u;
       an[u] = (rv && c < mm && c <= r) ? rowp[(long long)c * ld] : zero;
     }
-    for (int c0 = J * 32; c0 < cEnd; c0 += G) {
+    for (int c0 = J * TC; c0 < cEnd; c0 += G) {
       C a[G];
 #pragma unroll
       for (int u = 0; u < G; ++u) a[u] = an[u];
