@@ -271,7 +271,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     auto k = hetrd_kernel<C, R>;
     smem_optin(k, smem);
     count_launch();
-    k<<<nb, kTrdThreads, smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
+    k<<<nb, trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
                                      w.tau.template get<C>());
     B2_CHECK_LAUNCH();
   }

@@ -605,7 +605,10 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs<C> g) {
 // Follows the reflector conventions of LAPACK ?hetd2/?larfg: H_i = I - tau v v^H with
 // v(0) = 1, H_i^H (alpha; x) = (beta; 0), beta real; A = Q T Q^H, Q = H_0 H_1 ... .
 // v(1:) is stored below the subdiagonal of column i of A, tau in tauOut, T in (d, e).
-constexpr int kTrdThreads = 1024;
+constexpr int kTrdThreads = 1024;   // upper bound (launch bounds); see trd_threads()
+// threads per matrix: a matrix of at most 256 (512) rows leaves most of 1024 threads idle
+// at barriers, so several CTAs share an SM and hide each other's barrier waits
+inline int trd_threads(int Nmax) { return Nmax <= 256 ? 256 : Nmax <= 512 ? 512 : 1024; }
 
 template <typename C, typename R>
 __device__ __forceinline__ void householder(C* __restrict__ col, int m, C* __restrict__ v, R* red,
@@ -671,17 +674,21 @@ __device__ __forceinline__ C warp_reduce_scatter(C (&v)[G], int lane) {
 // off-diagonal tile of 32 rows x 4*NG columns with all rows valid: fully unrolled, no
 // predicates. p: this lane's row at the tile's first column; vU, wU, x, y: based at the
 // tile's first column.
-template <bool UPD, int NG>
+template <bool UPD, int NG, bool PART>
 __device__ __forceinline__ void trd_tile_full(float2* __restrict__ p, long long ld, const float2* __restrict__ vU,
                                               const float2* __restrict__ wU, const float2* __restrict__ x,
                                               float2 vr, float2 wr, float2 xr, float2& ry,
-                                              float2* __restrict__ y, int lane) {
+                                              float2* __restrict__ y, int lane, bool rv) {
+  // register slot u of a group holds column 4 g + (u ^ q), q = lane >> 3: the columns each
+  // lane keeps in the reduce-scatter below are then always slots 0 and 1 (no selects)
+  const int q = lane >> 3;
+  const float2 z2 = make_float2(0.f, 0.f);
   float2 an[4];
   float2* pn[4];
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
-    pn[u] = p + u * ld;
-    an[u] = *pn[u];
+    pn[u] = p + (u ^ q) * ld;
+    an[u] = (!PART || rv) ? *pn[u] : z2;
   }
   const long long ld4 = 4 * ld;
 #pragma unroll
@@ -692,25 +699,38 @@ __device__ __forceinline__ void trd_tile_full(float2* __restrict__ p, long long 
     for (int u = 0; u < 4; ++u) { a[u] = an[u]; pa[u] = pn[u]; }
     if (g < NG - 1) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) { pn[u] = pa[u] + ld4; an[u] = *pn[u]; }
+      for (int u = 0; u < 4; ++u) { pn[u] = pa[u] + ld4; an[u] = (!PART || rv) ? *pn[u] : z2; }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const int c = 4 * g + u;
+      const int c = 4 * g + (u ^ q);
       if (UPD) {
         const float2 vc = vU[c], wc = wU[c];
         float ax = a[u].x, ay = a[u].y;
         ax = fmaf(-vr.x, wc.x, ax); ax = fmaf(-vr.y, wc.y, ax); ax = fmaf(-wr.x, vc.x, ax); ax = fmaf(-wr.y, vc.y, ax);
         ay = fmaf(-vr.y, wc.x, ay); ay = fmaf(vr.x, wc.y, ay); ay = fmaf(-wr.y, vc.x, ay); ay = fmaf(wr.x, vc.y, ay);
         a[u] = make_float2(ax, ay);
-        *pa[u] = a[u];
+        if (!PART || rv) *pa[u] = a[u];
       }
       const float2 xc = x[c];
       ry.x = fmaf(a[u].x, xc.x, fmaf(-a[u].y, xc.y, ry.x));
       ry.y = fmaf(a[u].x, xc.y, fmaf(a[u].y, xc.x, ry.y));
       a[u] = make_float2(fmaf(a[u].y, xr.y, a[u].x * xr.x), fmaf(-a[u].y, xr.x, a[u].x * xr.y));
     }
-    const float2 s = warp_reduce_scatter<4>(a, lane);
+    // lanes with bit 4 clear keep columns 0,1 of the group, the others 2,3; then bit 3
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      a[u].x += __shfl_xor_sync(0xffffffffu, a[u + 2].x, 16);
+      a[u].y += __shfl_xor_sync(0xffffffffu, a[u + 2].y, 16);
+    }
+    a[0].x += __shfl_xor_sync(0xffffffffu, a[1].x, 8);
+    a[0].y += __shfl_xor_sync(0xffffffffu, a[1].y, 8);
+    float2 s = a[0];
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
     if ((lane & 7) == 0) {
       atomicAdd(&y[4 * g + (lane >> 3)].x, s.x);
       atomicAdd(&y[4 * g + (lane >> 3)].y, s.y);
@@ -745,14 +765,21 @@ __device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int m
     const int r = I * 32 + lane;
     const bool rv = r < mm;
     if constexpr (sizeof(C) == 8) {
-      if (J * TC + TC <= I * 32 && I * 32 + 32 <= mm) {
-        const C xr = x[r];
-        const C vr = UPD ? vU[r] : zero, wr = UPD ? wU[r] : zero;
+      if (J * TC + TC <= I * 32) {
+        const C xr = rv ? x[r] : zero;
+        const C vr = (UPD && rv) ? vU[r] : zero, wr = (UPD && rv) ? wU[r] : zero;
         C ry = zero;
-        trd_tile_full<UPD, TC / 4>(A0 + r + (long long)J * TC * ld, ld, UPD ? vU + J * TC : nullptr,
-                                   UPD ? wU + J * TC : nullptr, x + J * TC, vr, wr, xr, ry, y + J * TC, lane);
-        atomicAdd(&y[r].x, ry.x);
-        atomicAdd(&y[r].y, ry.y);
+        C* pr = A0 + (rv ? r : 0) + (long long)J * TC * ld;
+        if (I * 32 + 32 <= mm)
+          trd_tile_full<UPD, TC / 4, false>(pr, ld, UPD ? vU + J * TC : nullptr, UPD ? wU + J * TC : nullptr,
+                                            x + J * TC, vr, wr, xr, ry, y + J * TC, lane, true);
+        else
+          trd_tile_full<UPD, TC / 4, true>(pr, ld, UPD ? vU + J * TC : nullptr, UPD ? wU + J * TC : nullptr,
+                                           x + J * TC, vr, wr, xr, ry, y + J * TC, lane, rv);
+        if (rv) {
+          atomicAdd(&y[r].x, ry.x);
+          atomicAdd(&y[r].y, ry.y);
+        }
 
         continue;
       }

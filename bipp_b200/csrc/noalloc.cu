@@ -169,7 +169,7 @@ extern "C" BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl
     {
       const size_t smem = hetrd_smem_bytes(N, sizeof(float2));
       smem_optin(hetrd_kernel<float2, float>, smem);
-      hetrd_kernel<float2, float><<<1, kTrdThreads, smem, st>>>(w.A, nred, N, w.d, w.e, w.tau);
+      hetrd_kernel<float2, float><<<1, trd_threads(N), smem, st>>>(w.A, nred, N, w.d, w.e, w.tau);
     }
     {
       const size_t smem = 4 * (size_t)N * sizeof(double);
