@@ -140,8 +140,9 @@ prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long s
 // ------------------------------------------------------------------------------------
 constexpr int kCholNB = 32;
 constexpr int kCholThreads = 256;
+// shared memory: diagonal block D, its inverse Dinv, and two 64-row panel tiles
 template <typename E>
-constexpr size_t chol_smem() { return (size_t)(kCholNB + 128) * (kCholNB + 1) * sizeof(E); }
+constexpr size_t chol_smem() { return (size_t)(2 * kCholNB + 128) * (kCholNB + 1) * sizeof(E); }
 constexpr size_t kCholSmem = chol_smem<double2>();
 
 // FP64 element helpers: E = double2 (complex Hermitian G) or double (real symmetric G,
@@ -185,8 +186,11 @@ __device__ __forceinline__ double2 e_div(double2 a, double2 d) {
 }
 __device__ __forceinline__ double e_div(double a, double d) { return a / d; }
 
+// Panel rows below the diagonal block are X = A L_kk^-H with L_kk^-1 formed in shared
+// memory (as the triangular inverse does per block), a register-tiled product that keeps
+// the kernel at three CTAs per SM in the real case.
 template <typename E>
-__global__ void __launch_bounds__(kCholThreads)
+__global__ void __launch_bounds__(kCholThreads, sizeof(E) == 8 ? 3 : 1)
 cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status) {
   const int b = blockIdx.x;
   const int n = nred[b];
@@ -194,8 +198,9 @@ cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* 
   extern __shared__ __align__(16) unsigned char chol_raw[];
   E* chol_smem = reinterpret_cast<E*>(chol_raw);
   E (*D)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem);
-  E (*Pi)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + kCholNB * (kCholNB + 1));
-  E (*Pj)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + (kCholNB + 64) * (kCholNB + 1));
+  E (*Dinv)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + kCholNB * (kCholNB + 1));
+  E (*Pi)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + 2 * kCholNB * (kCholNB + 1));
+  E (*Pj)[kCholNB + 1] = reinterpret_cast<E (*)[kCholNB + 1]>(chol_smem + (2 * kCholNB + 64) * (kCholNB + 1));
   __shared__ int s_bad;
   if (threadIdx.x == 0) s_bad = 0;
   const int tid = threadIdx.x;
@@ -239,22 +244,50 @@ cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* 
       const int r = e % kb, c = e / kb;
       if (r >= c) Gb[(k0 + r) + (long long)(k0 + c) * Nmax] = D[r][c];
     }
-    // 4. panel: rows i >= k0+kb: x L_kk^H = a  (row-wise forward substitution)
-    for (int i = k0 + kb + tid; i < n; i += blockDim.x) {
-      E x[kCholNB];
-#pragma unroll
-      for (int c = 0; c < kCholNB; ++c) x[c] = (c < kb) ? Gb[i + (long long)(k0 + c) * Nmax] : zero;
-#pragma unroll
-      for (int c = 0; c < kCholNB; ++c) {
-        if (c < kb) {
-          E acc = x[c];
-          for (int m = 0; m < c; ++m) e_sub_mulc(acc, x[m], D[c][m]);
-          x[c] = e_scale(acc, 1.0 / e_re(D[c][c]));
+    // 4. Dinv = L_kk^-1 (lower; zero above the diagonal and outside kb): thread c forms
+    // column c by forward substitution
+    if (tid < kCholNB) {
+      const int c = tid;
+      for (int r = 0; r < kCholNB; ++r) {
+        E acc = e_real(zero, r == c ? 1.0 : 0.0);
+        if (r < kb && c < kb && r >= c) {
+          for (int m = c; m < r; ++m) e_sub_mul(acc, D[r][m], Dinv[m][c]);
+          Dinv[r][c] = e_div(acc, D[r][r]);
+        } else {
+          Dinv[r][c] = zero;
         }
       }
+    }
+    // 5. panel rows i >= k0+kb, 64 at a time: X = A L_kk^-H, X[i][c] = sum_m A[i][m] conj(Dinv[c][m])
+    for (int p0 = k0 + kb; p0 < n; p0 += 64) {
+      __syncthreads();
+      for (int e = tid; e < 64 * kCholNB; e += blockDim.x) {
+        const int r = e % 64, c = e / 64;
+        Pi[r][c] = (p0 + r < n && c < kb) ? Gb[(p0 + r) + (long long)(k0 + c) * Nmax] : zero;
+      }
+      __syncthreads();
+      const int tr = tid % 16, tc = tid / 16;  // rows tr + 16 a, columns tc + 16 c
+      E acc[4][2];
 #pragma unroll
-      for (int c = 0; c < kCholNB; ++c)
-        if (c < kb) Gb[i + (long long)(k0 + c) * Nmax] = x[c];
+      for (int a = 0; a < 4; ++a) acc[a][0] = acc[a][1] = zero;
+      for (int m = 0; m < kb; ++m) {
+        E pa[4], pb[2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) pa[a] = Pi[tr + 16 * a][m];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) pb[c] = Dinv[tc + 16 * c][m];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) e_add_mulc(acc[a][c], pa[a], pb[c]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int i = p0 + tr + 16 * a, col = tc + 16 * c;
+          if (i < n && col < kb) Gb[i + (long long)(k0 + col) * Nmax] = acc[a][c];
+        }
     }
     __syncthreads();
     // 5. trailing update A[i,j] -= sum_m P[i,m] conj(P[j,m]) for j <= i, tiles 64x64
