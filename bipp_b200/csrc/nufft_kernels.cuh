@@ -166,9 +166,14 @@ static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long
     const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
     const double* U = P.antUVW + (long long)st * P.nAnt * 3;
     const double sc = P.uvwScale[st];
-    const double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
-    const double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
-    const double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
+    double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
+    double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    // only the real part of the image is kept, and a point and its mirror (-u, -v, -w,
+    // conjugate value) have the same real part: every point is taken with w >= 0, so the
+    // w-grid spans [0, max w] instead of [-max w, max w]
+    const bool flip = w < 0.0;
+    if (flip) { u = -u; v = -v; w = -w; }
     const PtCoord c = point_coord(g, u, v, w);
     atomicAdd(counts + tile_key(g, c), 1);
   }
@@ -193,9 +198,14 @@ static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, lo
     const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
     const double* U = P.antUVW + (long long)st * P.nAnt * 3;
     const double sc = P.uvwScale[st];
-    const double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
-    const double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
-    const double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
+    double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
+    double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    // only the real part of the image is kept, and a point and its mirror (-u, -v, -w,
+    // conjugate value) have the same real part: every point is taken with w >= 0, so the
+    // w-grid spans [0, max w] instead of [-max w, max w]
+    const bool flip = w < 0.0;
+    if (flip) { u = -u; v = -v; w = -w; }
     const PtCoord c = point_coord(g, u, v, w);
     const int key = tile_key(g, c);
     const int pos = atomicAdd(cursor + key, 1);
@@ -212,7 +222,8 @@ static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, lo
     const float wgt = (r == s) ? 1.0f : 2.0f;   // lower triangle stands for (r,s) and (s,r)
     const float2* vvb = P.vv + (long long)st * P.vvStepStride + r + (long long)s * P.Nmax;
     for (int l = 0; l < P.levels; ++l) {
-      const float2 a = vvb[(long long)l * P.vvLevelStride];
+      float2 a = vvb[(long long)l * P.vvLevelStride];
+      if (flip) a.y = -a.y;
       vals[(long long)pos * nchAll + l] = make_float2(wgt * (a.x * cs - a.y * sn), wgt * (a.x * sn + a.y * cs));
     }
   }

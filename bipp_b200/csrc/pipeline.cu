@@ -352,7 +352,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
 
   if (p->mode == 0) {
     // batched: one NUFFT over all steps of the call, all levels as channels
-    p->core.begin(-Xw, Xw);
+    p->core.begin(0.0, Xw);  // points are folded to w >= 0 (real image)
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
     p->core.end_count(pairOff[T]);
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_chunk(p, s0, std::min(chunk, T - s0), pairOff, L, 0, false, ms);
@@ -366,7 +366,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     // plain: one step at a time, one NUFFT per step and level
     for (int b = 0; b < T; ++b) {
       for (int l = 0; l < L; ++l) {
-        p->core.begin(-wr[b], wr[b]);
+        p->core.begin(0.0, wr[b]);
         pipeline_count(p, b, 1, pairOff);
         p->core.end_count(pairOff[b + 1] - pairOff[b]);
         pipeline_chunk(p, b, 1, pairOff, 1, l, l > 0, ms);
