@@ -571,7 +571,7 @@ static void nufft_transform_lattice(bipp_nufft_s* p, long long n, long long ld) 
   host_minmax(ctx, p->uvw.get<float>(), n, p->mm, umin, umax);
   host_minmax(ctx, p->uvw.get<float>() + ld, n, p->mm, vmin, vmax);
   host_minmax(ctx, p->uvw.get<float>() + 2 * ld, n, p->mm, wmin, wmax);
-  p->core.begin(wmin, wmax);
+  p->core.begin(0.0, std::max(-wmin, wmax));  // points are folded to w >= 0
   const double su = std::max(std::fabs(umin), std::fabs(umax)), sv = std::max(std::fabs(vmin), std::fabs(vmax));
   // first-order correction for the FP32 rounding of the pixel coordinates when the
   // residual phase could exceed a tenth of the tolerance

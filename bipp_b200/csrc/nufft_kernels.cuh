@@ -248,10 +248,11 @@ static __global__ void vv_trace_kernel(int nSteps, int levels, const int* __rest
 // lattice-residual channels (values * u/su, values * v/sv)
 static __global__ void baseline_count_kernel(NufftGeom g, BaselinePoints P, int* __restrict__ counts) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
-    const double u = (double)P.uvw[t] * P.uvwScale;
-    const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
-    const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    double u = (double)P.uvw[t] * P.uvwScale;
+    double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
+    double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
     if (u == 0.0 && v == 0.0 && w == 0.0) continue;  // zero baseline: added analytically
+    if (w < 0.0) { u = -u; v = -v; w = -w; }         // folded to w >= 0 (real image)
     atomicAdd(counts + tile_key(g, point_coord(g, u, v, w)), 1);
   }
 }
@@ -261,14 +262,19 @@ static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, in
                                         int sincos64, int corrTerms, double su, double sv,
                                         double* __restrict__ zeroAcc, int nchAll) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < P.n; t += (long long)gridDim.x * blockDim.x) {
-    const double u = (double)P.uvw[t] * P.uvwScale;
-    const double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
-    const double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
+    double u = (double)P.uvw[t] * P.uvwScale;
+    double v = (double)P.uvw[t + P.lduvw] * P.uvwScale;
+    double w = (double)P.uvw[t + 2 * P.lduvw] * P.uvwScale;
     if (u == 0.0 && v == 0.0 && w == 0.0) {
       // exp(i 0) = 1 at every pixel: Re(value) adds to the whole image
       for (int l = 0; l < P.levels; ++l) atomicAdd(zeroAcc + l, (double)P.values[(long long)l * P.ldv + t].x);
       continue;
     }
+    // the image is the real part: the mirror (-u, -v, -w, conjugate value) contributes the
+    // same, so every point is taken with w >= 0 (the first-order channels follow, since
+    // Re(i d u q) is unchanged under u -> -u, q -> conj q)
+    const bool flip = w < 0.0;
+    if (flip) { u = -u; v = -v; w = -w; }
     const PtCoord c = point_coord(g, u, v, w);
     const int pos = atomicAdd(cursor + tile_key(g, c), 1);
     if (pos < 0 || pos >= valStride) continue;  // keys of both passes agree; never taken
@@ -282,7 +288,8 @@ static __global__ void baseline_scatter_kernel(NufftGeom g, BaselinePoints P, in
     if (sincos64) { double s64, c64; sincos(ph, &s64, &c64); sn = (float)s64; cs = (float)c64; }
     else sincosf((float)ph, &sn, &cs);
     for (int l = 0; l < P.levels; ++l) {
-      const float2 a = P.values[(long long)l * P.ldv + t];
+      float2 a = P.values[(long long)l * P.ldv + t];
+      if (flip) a.y = -a.y;
       const float2 q = make_float2(a.x * cs - a.y * sn, a.x * sn + a.y * cs);
       vals[(long long)pos * nchAll + l] = q;
       if (corrTerms) {
