@@ -244,15 +244,15 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-def profiled_traffic_per_grid_byte():
-    """DRAM bytes per grid byte of one spreading launch, from the committed ncu summary
-    (dram__bytes_read.sum + dram__bytes_write.sum of one launch / that launch's slab
-    bytes): the slab is written once and the reads follow the slab's points."""
+def profiled_traffic_ratio():
+    """DRAM bytes per algorithmic byte of a full-size spreading launch, from the committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of two launches of the
+    2048-step batch / their algorithmic bytes)."""
     path = os.path.join(ROOT, "profiles", "spread_tc_kernel_c2.md")
     try:
         with open(path) as f:
             for ln in f:
-                if ln.startswith("traffic_bytes_per_grid_byte:"):
+                if ln.startswith("traffic_per_algorithmic_byte:"):
                     return float(ln.split(":", 1)[1].split()[0])
     except OSError:
         pass
@@ -273,8 +273,8 @@ def spread_roofline(stats, spread_ms, n_levels):
     peaks, label = measured_peaks()
     achieved = per_launch / dur_s / 1e9
     flops = stats["points"] * n_levels * 4 * stats["W"] ** 3 / slabs  # real weight x complex value: 4 flops
-    tpg = profiled_traffic_per_grid_byte()
-    traffic = int(tpg * stats["grid_bytes"] / slabs) if tpg else None
+    ratio = profiled_traffic_ratio()
+    traffic = int(ratio * per_launch) if ratio else None
     return {"kernel": "spread_tc_kernel", "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 5),
             "peak_source": label, "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch),
