@@ -27,9 +27,14 @@ constexpr int kTcMaxChan = 8;                 // channels handled by the tensor-
 // shared-memory layout (bytes); one K-step of A is 128 rows x 8 tf32
 constexpr int kTcAStep = kTcM * 8 * 4;
 // per-visit kernel values at every tile position (zero outside the support) and the
-// channel values, stored position-major with a padded visit stride (conflict-free both
-// when a thread per visit writes them and when a thread per cell reads them)
-constexpr int kTcVS = kTcVisits + 1;
+// channel values, stored position-major, 16 visits per row, so that the operand builders
+// read 4 visits with one 16-byte load. Rows read by 8 different threads of a quarter warp
+// (x positions, channel values) have their 16-byte chunks permuted by the row (tab_sw):
+// conflict-free for those loads and for the writes of a thread per visit.
+constexpr int kTcVS = kTcVisits;
+__device__ __forceinline__ int tab_sw(int row, int v) {
+  return row * kTcVS + ((((v >> 2) ^ (row >> 1)) & 3) << 2) + (v & 3);
+}
 static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mapping assumes 16 x 8 x 8 tiles, 16 visits");
 
 // Shape of the kernel for CH channels (4 or 8): accumulator 128 x N, N = 8 planes x CH
@@ -273,43 +278,43 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       }
       // per-visit tables from the prefetched point data
       {
-        float* tab = (pa < 4) ? ex + (4 * pa) * kTcVS : (pa < 6) ? ey + (4 * (pa - 4)) * kTcVS : ew + (4 * (pa - 6)) * kTcVS;
+        float* tab = (pa < 4) ? ex : (pa < 6) ? ey : ew;
+        const bool swz = pa < 4;
+        const int first = 4 * ((pa < 4) ? pa : (pa < 6) ? pa - 4 : pa - 6);   // first table row of this role
         if (pv < nk) {
-          int l = pfL, first;
+          int l = pfL;
           if (pa < 4) {
             l -= x0;
             l = ((l % g.nx) + g.nx) % g.nx;
             if (l > g.nx / 2) l -= g.nx;
-            first = 4 * pa;
           } else if (pa < 6) {
             l -= y0;
             l = ((l % g.ny) + g.ny) % g.ny;
             if (l > g.ny / 2) l -= g.ny;
-            first = 4 * (pa - 4);
           } else {
             l -= w0;
-            first = 4 * (pa - 6);
           }
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int j = first + i - l;   // support index of tile position first + i
-            tab[i * kTcVS + pv] = ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - pfD) * invHalf, g.beta) : 0.f;
+            tab[swz ? tab_sw(first + i, pv) : (first + i) * kTcVS + pv] =
+                ((unsigned)j < (unsigned)W) ? es_kernel(((float)j - pfD) * invHalf, g.beta) : 0.f;
           }
           if (pa >= 6) {
 #pragma unroll
             for (int cc = 0; cc < CPR; ++cc) {
               const int c = CPR * (pa - 6) + cc;
-              val[(2 * c) * kTcVS + pv] = pfX[cc].x;
-              val[(2 * c + 1) * kTcVS + pv] = pfX[cc].y;
+              val[tab_sw(2 * c, pv)] = pfX[cc].x;
+              val[tab_sw(2 * c + 1, pv)] = pfX[cc].y;
             }
           }
         } else if (pv < steps * 8) {
           // padding visits of the last K-step contribute nothing (values too: 0 x stale
           // shared memory could be 0 x NaN)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) tab[i * kTcVS + pv] = 0.f;
+          for (int i = 0; i < 4; ++i) tab[swz ? tab_sw(first + i, pv) : (first + i) * kTcVS + pv] = 0.f;
           if (pa >= 6)
-            for (int c = 2 * CPR * (pa - 6); c < 2 * CPR * (pa - 5); ++c) val[c * kTcVS + pv] = 0.f;
+            for (int c = 2 * CPR * (pa - 6); c < 2 * CPR * (pa - 5); ++c) val[tab_sw(c, pv)] = 0.f;
         }
       }
       __syncthreads();
@@ -318,10 +323,19 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       // A: row tid (cell xm, ym), 8 visits per K-step
       for (int s = 0; s < steps; ++s) {
         float h[8], l[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int v = s * 8 + k;
-          split_tf32(ex[xm * kTcVS + v] * ey[ym * kTcVS + v], h[k], l[k]);
+        {
+          const float4 x0 = *reinterpret_cast<const float4*>(ex + tab_sw(xm, 8 * s));
+          const float4 x1 = *reinterpret_cast<const float4*>(ex + tab_sw(xm, 8 * s + 4));
+          const float4 y0 = *reinterpret_cast<const float4*>(ey + ym * kTcVS + 8 * s);
+          const float4 y1 = *reinterpret_cast<const float4*>(ey + ym * kTcVS + 8 * s + 4);
+          split_tf32(x0.x * y0.x, h[0], l[0]);
+          split_tf32(x0.y * y0.y, h[1], l[1]);
+          split_tf32(x0.z * y0.z, h[2], l[2]);
+          split_tf32(x0.w * y0.w, h[3], l[3]);
+          split_tf32(x1.x * y1.x, h[4], l[4]);
+          split_tf32(x1.y * y1.y, h[5], l[5]);
+          split_tf32(x1.z * y1.z, h[6], l[6]);
+          split_tf32(x1.w * y1.w, h[7], l[7]);
         }
         const uint32_t ah = sbase + S::OffAhi + s * kTcAStep + tid * 16;
         const uint32_t al = sbase + S::OffAlo + s * kTcAStep + tid * 16;
@@ -341,10 +355,14 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           for (int q = 0; q < VPT / 4; ++q) {
             const int k0 = kh * VPT + 4 * q;   // first visit of this 16-byte group
             float h[4], l[4];
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-              const int v = s * 8 + k0 + kk;
-              split_tf32(ew[plane * kTcVS + v] * val[cc * kTcVS + v], h[kk], l[kk]);
+            {
+              const int v = s * 8 + k0;
+              const float4 e4 = *reinterpret_cast<const float4*>(ew + plane * kTcVS + v);
+              const float4 c4 = *reinterpret_cast<const float4*>(val + tab_sw(cc, v));
+              split_tf32(e4.x * c4.x, h[0], l[0]);
+              split_tf32(e4.y * c4.y, h[1], l[1]);
+              split_tf32(e4.z * c4.z, h[2], l[2]);
+              split_tf32(e4.w * c4.w, h[3], l[3]);
             }
             const uint32_t bh = sbase + S::OffBhi + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
             const uint32_t bl = sbase + S::OffBlo + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
