@@ -267,8 +267,14 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   // 3. tridiagonalisation
   mark(4);
   {
-    const size_t smem = hetrd_smem_bytes(Nmax, sizeof(C));
+    // single precision: blocked panels while the V/W panel fits in shared memory
+    bool blocked = false;
+    if constexpr (sizeof(C) == 8) blocked = hetrd_blk_smem_bytes(Nmax) <= ctx->maxSmemOptin;
+    const size_t smem = blocked ? hetrd_blk_smem_bytes(Nmax) : hetrd_smem_bytes(Nmax, sizeof(C));
     auto k = hetrd_kernel<C, R>;
+    if constexpr (sizeof(C) == 8) {
+      if (blocked) k = hetrd_blk_kernel<C, R>;
+    }
     smem_optin(k, smem);
     count_launch();
     k<<<nb, trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),

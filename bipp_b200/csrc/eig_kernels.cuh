@@ -875,18 +875,13 @@ __device__ __forceinline__ void trd_lower_pass(C* __restrict__ A0, int ld, int m
 // shared memory of hetrd_kernel: v, w, p, vn, y
 constexpr size_t hetrd_smem_bytes(int Nmax, size_t complexBytes) { return 5 * (size_t)Nmax * complexBytes; }
 
-// Only the lower triangle of A is read or written (the upper one is never touched).
+// Unblocked tridiagonalisation of columns i0 .. n-2 of one matrix (A[i0:, i0:] already
+// holds every earlier update). Only the lower triangle of A is read or written (the upper
+// one is never touched). smem_raw: 5 Nmax elements.
 template <typename C, typename R>
-__global__ void __launch_bounds__(kTrdThreads)
-hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
-             double* __restrict__ eOut, C* __restrict__ tauOut) {
-  const int b = blockIdx.x;
-  const int n = nred[b];
-  C* Ab = A + (long long)b * Nmax * Nmax;
-  double* d = dOut + (long long)b * Nmax;
-  double* e = eOut + (long long)b * Nmax;
-  C* taus = tauOut + (long long)b * Nmax;
-  extern __shared__ unsigned char smem_raw[];
+__device__ __forceinline__ void hetd2_tail(C* __restrict__ Ab, int n, int Nmax, int i0, double* __restrict__ d,
+                                           double* __restrict__ e, C* __restrict__ taus,
+                                           unsigned char* __restrict__ smem_raw) {
   C* v = reinterpret_cast<C*>(smem_raw);        // [Nmax] current reflector (relative to row i+1)
   C* w = v + Nmax;                              // [Nmax] w vector
   C* p = w + Nmax;                              // [Nmax] tau*A*v for the next step
@@ -896,26 +891,26 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
   __shared__ C s_tau, s_taun;
   __shared__ R s_beta;
   const int tid = threadIdx.x;
-  if (n <= 0) return;
-  if (n == 1) {
-    if (tid == 0) { d[0] = (double)Ab[0].x; }
+  if (n - i0 <= 0) return;
+  if (n - i0 == 1) {
+    if (tid == 0) { d[i0] = (double)Ab[i0 + (long long)i0 * Nmax].x; }
     return;
   }
 
-  // ---- step 0 set-up: reflector of column 0, p = tau A22 v ----
+  // ---- set-up: reflector of column i0, p = tau A22 v ----
   {
     C t; R be;
     for (int r = tid; r < n; r += blockDim.x) y[r] = mk(R(0), R(0));
-    householder<C, R>(Ab + 1, n - 1, v, red, t, be);
+    householder<C, R>(Ab + (i0 + 1) + (long long)i0 * Nmax, n - i0 - 1, v, red, t, be);
     if (tid == 0) { s_tau = t; s_beta = be; }
     __syncthreads();
-    trd_lower_pass<C, R, false>(Ab + 1 + Nmax, Nmax, n - 1, nullptr, nullptr, v, y);
+    trd_lower_pass<C, R, false>(Ab + (i0 + 1) + (long long)(i0 + 1) * Nmax, Nmax, n - i0 - 1, nullptr, nullptr, v, y);
     __syncthreads();
-    for (int r = tid; r < n - 1; r += blockDim.x) p[r] = cmul(s_tau, y[r]);
+    for (int r = tid; r < n - i0 - 1; r += blockDim.x) p[r] = cmul(s_tau, y[r]);
     __syncthreads();
   }
 
-  for (int i = 0; i < n - 1; ++i) {
+  for (int i = i0; i < n - 1; ++i) {
     const int m = n - i - 1;            // size of A22 = A[i+1:, i+1:]
     const C tau = s_tau;
     const R beta = s_beta;
@@ -982,6 +977,184 @@ hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* 
     if (tid == 0) s_tau = taun;
     __syncthreads();
   }
+}
+
+
+// Householder tridiagonalisation of every matrix of the batch, unblocked (LAPACK ?hetd2).
+template <typename C, typename R>
+__global__ void __launch_bounds__(kTrdThreads)
+hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
+             double* __restrict__ eOut, C* __restrict__ tauOut) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int b = blockIdx.x;
+  hetd2_tail<C, R>(A + (long long)b * Nmax * Nmax, nred[b], Nmax, 0, dOut + (long long)b * Nmax,
+                   eOut + (long long)b * Nmax, tauOut + (long long)b * Nmax, smem_raw);
+}
+
+// Blocked tridiagonalisation (LAPACK ?hetrd with ?latrd panels, lower), single precision.
+// Panels of kTrdNB columns: for panel column c the column is brought up to date with the
+// panel's earlier reflectors, its reflector v is formed, y = A22 v is a read-only pass over
+// the trailing block (stale for this panel), corrected by y -= V (W^H v) + W (V^H v), and
+// w = tau y - 1/2 tau (tau y)^H v ... v joins W. After the panel the trailing lower triangle
+// takes A -= V W^H + W V^H in one pass (warp per 32 x 32 tile, the row's V and W in
+// registers). The last kTrdNX columns use the unblocked hetd2_tail. V and W live in
+// shared memory interleaved per reflector, row r: (V[r][q], W[r][q]) for q < kTrdNB.
+constexpr int kTrdNB = 8;
+constexpr int kTrdNX = 64;
+constexpr int kTrdVWS = 2 * kTrdNB + 2;   // float2 row stride of the V/W panel (144 B: 16-byte rows, no bank conflicts)
+// shared memory of hetrd_blk_kernel: 5 vectors, the V/W panel, 2 kTrdNB dot products
+constexpr size_t hetrd_blk_smem_bytes(int Nmax) {
+  return ((5 * (size_t)Nmax * 8 + 15) & ~(size_t)15) + (size_t)Nmax * kTrdVWS * 8 + 2 * kTrdNB * 8;
+}
+
+// rank-2 kTrdNB update of the trailing lower triangle rows/cols s0 .. n-1
+__device__ __forceinline__ void trd_her2k(float2* __restrict__ Ab, int Nmax, int n, int s0,
+                                          const float2* __restrict__ VW) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int mt = n - s0;
+  const int nT = (mt + 31) >> 5;
+  const int nTiles = nT * (nT + 1) / 2;
+  for (int t = warp; t < nTiles; t += nwarp) {
+    int I = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    const int J = t - I * (I + 1) / 2;
+    const int r = s0 + I * 32 + lane;
+    const bool rv = r < n;
+    // this row's (V, W) pairs
+    float4 rw[kTrdNB];
+    const float4* rp = reinterpret_cast<const float4*>(VW + (long long)(rv ? r : s0) * kTrdVWS);
+#pragma unroll
+    for (int q = 0; q < kTrdNB; ++q) rw[q] = rp[q];
+    const int c0 = s0 + J * 32;
+    const int cEnd = min(n, c0 + 32);
+    float2* colp = Ab + (rv ? r : s0) + (long long)c0 * Nmax;
+#pragma unroll 2
+    for (int c = c0; c < cEnd; ++c, colp += Nmax) {
+      const float4* cp = reinterpret_cast<const float4*>(VW + (long long)c * kTrdVWS);
+      float ax = 0.f, ay = 0.f;
+#pragma unroll
+      for (int q = 0; q < kTrdNB; ++q) {
+        const float4 cq = cp[q];   // (V[c].x, V[c].y, W[c].x, W[c].y)
+        // V[r] conj(W[c]) + W[r] conj(V[c])
+        ax = fmaf(rw[q].x, cq.z, ax); ax = fmaf(rw[q].y, cq.w, ax);
+        ay = fmaf(rw[q].y, cq.z, ay); ay = fmaf(-rw[q].x, cq.w, ay);
+        ax = fmaf(rw[q].z, cq.x, ax); ax = fmaf(rw[q].w, cq.y, ax);
+        ay = fmaf(rw[q].w, cq.x, ay); ay = fmaf(-rw[q].z, cq.y, ay);
+      }
+      if (rv && c <= r) {
+        float2 a = *colp;
+        a.x -= ax;
+        a.y -= ay;
+        *colp = a;
+      }
+    }
+  }
+}
+
+template <typename C, typename R>
+__global__ void __launch_bounds__(kTrdThreads)
+hetrd_blk_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
+                 double* __restrict__ eOut, C* __restrict__ tauOut) {
+  static_assert(sizeof(C) == 8, "single precision");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int b = blockIdx.x;
+  const int n = nred[b];
+  C* Ab = A + (long long)b * Nmax * Nmax;
+  double* d = dOut + (long long)b * Nmax;
+  double* e = eOut + (long long)b * Nmax;
+  C* taus = tauOut + (long long)b * Nmax;
+  C* v = reinterpret_cast<C*>(smem_raw);   // [Nmax] reflector of the current column
+  C* y = v + Nmax;                          // [Nmax] mat-vec, then w
+  C* VW = reinterpret_cast<C*>(smem_raw + ((5 * (size_t)Nmax * 8 + 15) & ~(size_t)15));  // [Nmax][kTrdVWS]
+  C* tq = VW + (long long)Nmax * kTrdVWS;   // [2 kTrdNB] W^H v, then V^H v
+  __shared__ R red[32];
+  __shared__ C s_tau;
+  __shared__ R s_beta;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const int T = blockDim.x;
+  const C zero = mk(R(0), R(0));
+  int k0 = 0;
+  for (; n - k0 > kTrdNX; k0 += kTrdNB) {
+    for (int j = 0; j < kTrdNB; ++j) {
+      const int c = k0 + j, m = n - c - 1;
+      // column c (rows c..n-1) with the panel's earlier reflectors: A -= V W^H + W V^H
+      if (j > 0) {
+        const C* cw = VW + (long long)c * kTrdVWS;
+        for (int r = c + tid; r < n; r += T) {
+          const C* rw = VW + (long long)r * kTrdVWS;
+          C a = Ab[r + (long long)c * Nmax];
+          for (int q = 0; q < j; ++q) a = a - cmulc(rw[2 * q], cw[2 * q + 1]) - cmulc(rw[2 * q + 1], cw[2 * q]);
+          if (r == c) a.y = R(0);
+          Ab[r + (long long)c * Nmax] = a;
+        }
+        __syncthreads();
+      }
+      // reflector from rows c+1..n-1 of column c
+      {
+        C t; R be;
+        householder<C, R>(Ab + (c + 1) + (long long)c * Nmax, m, v, red, t, be);
+        if (tid == 0) { s_tau = t; s_beta = be; }
+      }
+      __syncthreads();
+      const C tau = s_tau;
+      for (int r = tid; r < m; r += T) {
+        const C vr = v[r];
+        if (r > 0) Ab[(c + 1 + r) + (long long)c * Nmax] = vr;
+        VW[(long long)(c + 1 + r) * kTrdVWS + 2 * j] = vr;
+        y[r] = zero;
+      }
+      if (tid == 0) {
+        e[c] = (double)s_beta;
+        taus[c] = tau;
+        d[c] = (double)Ab[c + (long long)c * Nmax].x;
+        Ab[(c + 1) + (long long)c * Nmax] = mk(s_beta, R(0));
+      }
+      __syncthreads();
+      // y = A22 v over the trailing block as stored (read-only pass)
+      trd_lower_pass<C, R, false>(Ab + (c + 1) + (long long)(c + 1) * Nmax, Nmax, m, nullptr, nullptr, v, y);
+      __syncthreads();
+      if (j > 0) {
+        // tq[q] = W_q^H v, tq[kTrdNB + q] = V_q^H v (q < j), one warp per dot product
+        for (int wq = warp; wq < 2 * j; wq += nwarp) {
+          const int q = wq < j ? wq : wq - j;
+          const int sel = wq < j ? 1 : 0;   // 1: W column, 0: V column
+          C acc = zero;
+          for (int r = lane; r < m; r += 32) cfma_cj(acc, VW[(long long)(c + 1 + r) * kTrdVWS + 2 * q + sel], v[r]);
+          acc.x = warp_sum(acc.x);
+          acc.y = warp_sum(acc.y);
+          if (lane == 0) tq[(wq < j ? 0 : kTrdNB) + q] = acc;
+        }
+        __syncthreads();
+        // y -= V (W^H v) + W (V^H v)
+        for (int r = tid; r < m; r += T) {
+          const C* rw = VW + (long long)(c + 1 + r) * kTrdVWS;
+          C s = y[r];
+          for (int q = 0; q < j; ++q) s = s - cmul(rw[2 * q], tq[q]) - cmul(rw[2 * q + 1], tq[kTrdNB + q]);
+          y[r] = s;
+        }
+        __syncthreads();
+      }
+      // w = tau y - 1/2 tau ((tau y)^H v) v  -> W column j
+      R pr = 0, pi = 0;
+      for (int r = tid; r < m; r += T) {
+        const C wv = cmul(tau, y[r]);
+        y[r] = wv;
+        const C pv = cconjmul(wv, v[r]);
+        pr += pv.x;
+        pi += pv.y;
+      }
+      pr = block_sum(pr, red);
+      pi = block_sum(pi, red);
+      const C alph = cscale(cmul(tau, mk(pr, pi)), R(-0.5));
+      for (int r = tid; r < m; r += T) VW[(long long)(c + 1 + r) * kTrdVWS + 2 * j + 1] = y[r] + cmul(alph, v[r]);
+      __syncthreads();
+    }
+    // trailing block rows/cols k0 + kTrdNB .. n-1
+    trd_her2k(Ab, Nmax, n, k0 + kTrdNB, VW);
+    __syncthreads();
+  }
+  hetd2_tail<C, R>(Ab, n, Nmax, k0, d, e, taus, smem_raw);
 }
 
 // ------------------------------------------------------------------------------------
