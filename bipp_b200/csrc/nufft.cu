@@ -175,6 +175,9 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   g_.nc = 0.5 * (nmin + nmax);
   Sn_ = std::max(0.5 * (nmax - nmin), 1e-12);
   g_.hw = M_PI / (sigma * Sn_);
+  g_.ihx = 1.0 / g_.hx;
+  g_.ihy = 1.0 / g_.hy;
+  g_.ihw = 1.0 / g_.hw;
   std::vector<double> nt(P);
   for (long long p = 0; p < P; ++p) nt[p] = n[p] - g_.nc;
   nTilde_.alloc(ctx, P * sizeof(double));

@@ -30,6 +30,7 @@ struct NufftGeom {
   int nx, ny, nw;                   // grid sizes (nx, ny periodic; nw linear)
   int jc;                           // w-grid index of t = 0
   double hx, hy, hw;                // grid spacings (x,y in radians per cell; w in w-units)
+  double ihx, ihy, ihw;             // their reciprocals (per-point coordinates multiply)
   int W;                            // kernel width (cells)
   float beta;                       // ES kernel shape
   int ntx, nty, ntw;                // tile counts
@@ -44,7 +45,8 @@ __device__ __forceinline__ float es_kernel(float z, float beta) {
 __device__ __forceinline__ double wrap_pi(double x) {
   // to [-pi, pi)
   const double twopi = 6.283185307179586476925286766559;
-  return x - twopi * floor(x / twopi + 0.5);
+  const double inv_twopi = 0.15915494309189533576888376337251;
+  return x - twopi * floor(x * inv_twopi + 0.5);
 }
 
 // grid coordinates of one point: first support cell and offset (gx - ix0) in FP32
@@ -57,9 +59,9 @@ struct PtCoord {
 static __device__ __noinline__ PtCoord point_coord(const NufftGeom& g, double u, double v, double w) {
   const double x = u * g.Bl + v * g.Bm;
   const double y = u * g.Al + v * g.Am;
-  const double gx = wrap_pi(x) / g.hx;
-  const double gy = wrap_pi(y) / g.hy;
-  const double gw = (w - g.wc) / g.hw + g.jc;
+  const double gx = wrap_pi(x) * g.ihx;
+  const double gy = wrap_pi(y) * g.ihy;
+  const double gw = (w - g.wc) * g.ihw + g.jc;
   const double half = 0.5 * g.W;
   PtCoord c;
   c.ix0 = (int)ceil(gx - half);

@@ -89,10 +89,11 @@ def test_eigenvector_g_orthonormality(ctx):
     assert np.abs(s @ x - G @ x * d[:nr]).max() < 1e-9 * np.abs(s).max()
 
 
-@pytest.mark.parametrize("n", [64, 200, 512])
+@pytest.mark.parametrize("n", [64, 200, 300, 512, 768])
 def test_larger_sizes_against_fp64_oracle(ctx, n):
-    """FP32 GPU eigensolve at N up to 512 (the 512-antenna workload size) against scipy
-    FP64, with random flagging."""
+    """FP32 GPU eigensolve at N up to 768 against scipy FP64, with random flagging: the
+    unblocked tridiagonalisation (N = 64), and the blocked one with 256 (N = 200), 512
+    (N = 300, 512) and 1024 (N = 768) threads per matrix."""
     import bipp_b200 as bipp
     from bipp_b200 import simulate as sim
 
