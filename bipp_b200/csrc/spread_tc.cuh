@@ -283,14 +283,15 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
         const int first = 4 * ((pa < 4) ? pa : (pa < 6) ? pa - 4 : pa - 6);   // first table row of this role
         if (pv < nk) {
           int l = pfL;
-          if (pa < 4) {
-            l -= x0;
-            l = ((l % g.nx) + g.nx) % g.nx;
-            if (l > g.nx / 2) l -= g.nx;
-          } else if (pa < 6) {
-            l -= y0;
-            l = ((l % g.ny) + g.ny) % g.ny;
-            if (l > g.ny / 2) l -= g.ny;
+          // periodic offset of the support start from the tile, in (-n/2, n/2]: the start
+          // lies in [-n/2 - W/2, n/2) and the tile origin in [0, n), so the difference
+          // lies in (-3n/2 - W/2, n/2) and two conditional additions wrap it
+          if (pa < 6) {
+            const int np = (pa < 4) ? g.nx : g.ny;
+            l -= (pa < 4) ? x0 : y0;
+            if (l <= -(np >> 1)) l += np;
+            if (l <= -(np >> 1)) l += np;
+            if (l > (np >> 1)) l -= np;
           } else {
             l -= w0;
           }
