@@ -42,6 +42,7 @@ enum StatusBits : int {
   kStatusCholeskyNotPD = 1,   // non-positive pivot in the FP64 Cholesky of G
   kStatusNonFinite = 2,       // NaN/Inf met in the inputs or the reduction
   kStatusClusterFix = 4,      // eigenvector cluster re-orthogonalised (informational)
+  kStatusTensorTimeout = 8,   // a tensor-core MMA completion wait ran out (GPU error)
 };
 
 // ---- complex helpers --------------------------------------------------------------

@@ -9,6 +9,7 @@
 #include "context.hpp"
 #include "eig.hpp"
 #include "eig_kernels.cuh"
+#include "gemm_tc.cuh"
 
 namespace bippb200 {
 
@@ -245,11 +246,26 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g1.B = A; g1.strideB = n2; g1.ldb = Nmax; g1.opB = 0;
     g1.Cm = T1; g1.strideC = n2; g1.ldc = Nmax;
     g1.n = nred; g1.triA = 1; g1.triB = 0; g1.outMode = 0; g1.levels = 1;
+    // single precision with a real Gram matrix: both products on the tensor cores
+    // (C = L^-1 (L^-1 S)^H, Hermitian); otherwise the FP32/FP64 SIMT GEMM
+    const bool tcReduce = realG && sizeof(C) == 8;
     count_launch();
-    if (realG)
+    if (tcReduce) {
+      if constexpr (sizeof(C) == 8) {
+        TgArgs t{};
+        t.L = reinterpret_cast<const float*>(Linv); t.strideL = n2; t.ldl = Nmax;
+        t.B = A; t.strideB = n2; t.ldb = Nmax; t.opB = 0;
+        t.C = T1; t.strideC = n2; t.ldc = Nmax;
+        t.n = nred; t.lowerOnly = 0; t.status = L.status + L.batchOffset;
+        const dim3 tg((Nmax + kTgM - 1) / kTgM, (Nmax + kTgNC - 1) / kTgNC, nb);
+        smem_optin(gemm_tc_kernel, kTgSmem);
+        gemm_tc_kernel<<<tg, kTgThreads, kTgSmem, st>>>(t);
+      }
+    } else if (realG) {
       gemm_kernel<C, R, R, C><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
-    else
+    } else {
       gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g1);
+    }
     B2_CHECK_LAUNCH();
     // A = T1 * Linv^H (Hermitian: lower tiles + mirror)
     GemmArgs<C> g2{};
@@ -258,10 +274,22 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     g2.Cm = A; g2.strideC = n2; g2.ldc = Nmax;
     g2.n = nred; g2.triA = 0; g2.triB = 1; g2.outMode = 1; g2.levels = 1;
     count_launch();
-    if (realG)
+    if (tcReduce) {
+      if constexpr (sizeof(C) == 8) {
+        // only the lower triangle of the reduced matrix is read afterwards
+        TgArgs t{};
+        t.L = reinterpret_cast<const float*>(Linv); t.strideL = n2; t.ldl = Nmax;
+        t.B = T1; t.strideB = n2; t.ldb = Nmax; t.opB = 1;
+        t.C = A; t.strideC = n2; t.ldc = Nmax;
+        t.n = nred; t.lowerOnly = 1; t.status = L.status + L.batchOffset;
+        const dim3 tg((Nmax + kTgM - 1) / kTgM, (Nmax + kTgNC - 1) / kTgNC, nb);
+        gemm_tc_kernel<<<tg, kTgThreads, kTgSmem, st>>>(t);
+      }
+    } else if (realG) {
       gemm_kernel<C, R, C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
-    else
+    } else {
       gemm_kernel<C, R><<<dim3(tiles, tiles, nb), kGemmThreads, 0, st>>>(g2);
+    }
     B2_CHECK_LAUNCH();
   }
   // 3. tridiagonalisation
@@ -470,6 +498,7 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   }
   sync(ctx);
   // nred from the flag pass is authoritative even when nred was 0 (kernels skipped)
+  if (status & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
   if (status & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
   for (size_t c = 0; c < nBeam; ++c) d[c] = (c < (size_t)nred) ? (T)lam[c] : T(0);
   if (v) {
@@ -546,6 +575,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
   d2h(ctx, stat.data(), dStatus.get(), nBatch * sizeof(int));
   sync(ctx);
   for (size_t b = 0; b < nBatch; ++b) {
+    if (stat[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
     if (stat[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
     nBeamReduced[b] = (size_t)nredh[b];
     scale[b] = nvish[b] ? 1.0f / (float)nvish[b] : 0.0f;

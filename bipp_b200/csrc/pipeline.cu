@@ -386,8 +386,10 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   d2h(ctx, st.data(), p->status.get(), T * sizeof(int));
   sync(ctx);
   if (p->timing) { cudaEventDestroy(ev0); cudaEventDestroy(ev1); }
-  for (int b = 0; b < T; ++b)
+  for (int b = 0; b < T; ++b) {
+    if (st[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
     if (st[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
+  }
 }
 
 extern "C" {
