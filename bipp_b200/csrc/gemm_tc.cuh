@@ -83,6 +83,37 @@ __global__ void __launch_bounds__(kTgThreads, 3) gemm_tc_kernel(TgArgs a) {
   uint32_t parity = 0;
   bool pending = false;
   const int row = i0 + tid;   // row of A staged by this thread
+  // raw operands of one phase, loaded into registers one phase ahead: A row `row`, 32 k;
+  // B units (complex column j, k quad) u = tid + 128 m
+  float ra[kTgKP];
+  float2 rb[4][4];
+  auto load_phase = [&](int k0) {
+#pragma unroll
+    for (int kk = 0; kk < kTgKP; ++kk) {
+      const int k = k0 + kk;
+      ra[kk] = (row < n && k < n) ? Lb[row + (long long)k * a.ldl] : 0.f;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int u = tid + kTgThreads * m;
+      const int col = j0 + u % kTgNC, q = u / kTgNC;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = k0 + 4 * q + e;
+        float2 v = make_float2(0.f, 0.f);
+        if (col < n && k < n) {
+          if (a.opB == 0) {
+            v = Bb[k + (long long)col * a.ldb];
+          } else {
+            v = Bb[col + (long long)k * a.ldb];
+            v.y = -v.y;
+          }
+        }
+        rb[m][e] = v;
+      }
+    }
+  };
+  load_phase(0);
   for (int k0 = 0; k0 < kmax; k0 += kTgKP) {
     // the operands of the previous phase must have been consumed
     if (tid == 0 && pending) {
@@ -98,46 +129,23 @@ __global__ void __launch_bounds__(kTgThreads, 3) gemm_tc_kernel(TgArgs a) {
     // A: thread = row; 8 quads of k, each one 16-byte row chunk of a K-half
 #pragma unroll
     for (int q = 0; q < kTgKP / 4; ++q) {
-      float v[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int k = k0 + 4 * q + e;
-        v[e] = (row < n && k < n) ? Lb[row + (long long)k * a.ldl] : 0.f;
-      }
       float h[4], l[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) split_tf32(v[e], h[e], l[e]);
+      for (int e = 0; e < 4; ++e) split_tf32(ra[4 * q + e], h[e], l[e]);
       const uint32_t off = (q >> 1) * kTgAStep + (q & 1) * (kTgAStep / 2) + tid * 16;
       st_shared_v4(sbase + kTgOffAhi + off, h[0], h[1], h[2], h[3]);
       st_shared_v4(sbase + kTgOffAlo + off, l[0], l[1], l[2], l[3]);
     }
-    // B: units (complex column j, k quad), 512 per phase, 4 per thread; real rows 2j (re), 2j+1 (im)
+    // B: real rows 2j (re), 2j+1 (im)
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int u = tid + kTgThreads * m;
       const int j = u % kTgNC, q = u / kTgNC;
-      const int col = j0 + j;
-      float re[4], im[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int k = k0 + 4 * q + e;
-        float2 v = make_float2(0.f, 0.f);
-        if (col < n && k < n) {
-          if (a.opB == 0) {
-            v = Bb[k + (long long)col * a.ldb];
-          } else {
-            v = Bb[col + (long long)k * a.ldb];
-            v.y = -v.y;
-          }
-        }
-        re[e] = v.x;
-        im[e] = v.y;
-      }
       float rh[4], rl[4], ih[4], il[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        split_tf32(re[e], rh[e], rl[e]);
-        split_tf32(im[e], ih[e], il[e]);
+        split_tf32(rb[m][e].x, rh[e], rl[e]);
+        split_tf32(rb[m][e].y, ih[e], il[e]);
       }
       const uint32_t off = (q >> 1) * kTgBStep + (q & 1) * (kTgBStep / 2) + (2 * j) * 16;
       st_shared_v4(sbase + kTgOffBhi + off, rh[0], rh[1], rh[2], rh[3]);
@@ -145,6 +153,8 @@ __global__ void __launch_bounds__(kTgThreads, 3) gemm_tc_kernel(TgArgs a) {
       st_shared_v4(sbase + kTgOffBhi + off + 16, ih[0], ih[1], ih[2], ih[3]);
       st_shared_v4(sbase + kTgOffBlo + off + 16, il[0], il[1], il[2], il[3]);
     }
+    // the next phase's operands are read from memory while this phase's MMAs run
+    if (k0 + kTgKP < kmax) load_phase(k0 + kTgKP);
     // make the operand writes visible to the tensor core, then one thread issues
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
