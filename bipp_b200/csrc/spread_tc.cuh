@@ -193,16 +193,8 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     for (int v0 = 0; v0 < nvis; v0 += kTcVisits) {
       const int nk = min(kTcVisits, nvis - v0);
       const int steps = (nk + 7) >> 3;
-      // the operands of the previous phase must have been consumed
-      if (tid == 0 && pending) {
-        if (mbar_wait(bar, parity)) {
-          parity ^= 1u;
-          pending = false;
-        } else {
-          sOk = 0;
-        }
-      }
-      // per-visit tables from the prefetched point data
+      // per-visit tables from the prefetched point data (the tensor cores read only the
+      // operand blocks, so the tables are rebuilt while the previous phase's MMAs run)
       {
         float* tab = (pa < 4) ? ex : (pa < 6) ? ey : ew;
         const bool swz = pa < 4;
@@ -242,6 +234,15 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           for (int i = 0; i < 4; ++i) tab[swz ? tab_sw(first + i, pv) : (first + i) * kTcVS + pv] = 0.f;
           if (pa >= 6)
             for (int c = 2 * CPR * (pa - 6); c < 2 * CPR * (pa - 5); ++c) val[tab_sw(c, pv)] = 0.f;
+        }
+      }
+      // the operands of the previous phase must have been consumed before they are rewritten
+      if (tid == 0 && pending) {
+        if (mbar_wait(bar, parity)) {
+          parity ^= 1u;
+          pending = false;
+        } else {
+          sOk = 0;
         }
       }
       __syncthreads();
