@@ -68,7 +68,7 @@ def parse():
                     help="time steps of the plain-GPU comparison (one NUFFT per step and level); 0 skips it")
     a = ap.parse_args()
     dflt = {"c2": dict(time_steps=2048, antennas=512, image=1024, chunk_steps=2048),
-            "c5": dict(time_steps=128, antennas=1024, image=2048, chunk_steps=512)}[a.workload]
+            "c5": dict(time_steps=128, antennas=1024, image=2048, chunk_steps=592)}[a.workload]
     for k, v in dflt.items():
         if getattr(a, k) is None:
             setattr(a, k, v)
