@@ -6,7 +6,7 @@
 // i.e. the product of A (128 cells x K visits) and B (K visits x 16 CH columns: 8 planes x
 // CH = 4 or 8 channels x re/im). Threads write A and B for 16 visits at a time into shared memory
 // (canonical K-major, no swizzle), one thread issues tcgen05.mma (kind::tf32) into a
-// 128 x 64 FP32 accumulator in tensor memory, and the epilogue reads it back with
+// 128 x 16 CH FP32 accumulator in tensor memory, and the epilogue reads it back with
 // tcgen05.ld and writes the tile once. FP32 accuracy comes from the 3xTF32 split
 // a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi (a_hi = tf32(a), a_lo = tf32(a - a_hi)).
 // Every wait on the MMA completion barrier is bounded; a timeout sets an error flag
