@@ -164,6 +164,12 @@ def make_inputs(cfg, rank, device):
     return obs, S, xyz, wl
 
 
+def lower_block_bytes(n, t, cols=64):
+    """Bytes of visibilities a host-input pipeline call copies: the lower triangle of each
+    n x n complex64 matrix in blocks of `cols` columns, from each block's diagonal down."""
+    return t * 8 * sum((n - c0) * min(cols, n - c0) for c0 in range(0, n, cols))
+
+
 def lattice_of(obs, n):
     l = obs.lmn[:, 0].reshape(n, n)
     m = obs.lmn[:, 1].reshape(n, n)
@@ -453,7 +459,7 @@ def main():
         if world > 1:
             dist.all_reduce(ems, op=dist.ReduceOp.MAX)
         e2e = {"value": args.e2e_steps * T_steps * world / (float(ems.item()) / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": int(S_h.numel() * 8 + xyz_h.numel() * 8 + wl_h.numel() * 8),
+               "h2d_bytes_per_step": int(lower_block_bytes(cfg.n_antenna, T) + xyz_h.numel() * 8 + wl_h.numel() * 8),
                "d2h_bytes_per_step": int(img_h.numel() * 4)}
 
     cpu = None

@@ -243,7 +243,8 @@ BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipel
 /* Process nSteps time steps: s [nSteps][nAntenna x nAntenna] complex float (lower triangle
  * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. onDevice != 0: the
  * three pointers are device pointers (s is read in place, not modified), else host
- * pointers (copied in by the call). The steps' contributions are accumulated into the
+ * pointers (copied in by the call; of s only the lower triangle is copied, in blocks of 64
+ * columns from each block's diagonal row down). The steps' contributions are accumulated into the
  * images. Fails with BIPP_EIGENSOLVER_ERROR when a Gram matrix is not positive definite
  * and with BIPP_GPU_ERROR when a tensor-core completion wait runs out (a GPU fault). */
 BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s,
