@@ -256,14 +256,18 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           const float4 x1 = *reinterpret_cast<const float4*>(ex + tab_sw(xm, 8 * s + 4));
           const float4 y0 = *reinterpret_cast<const float4*>(ey + ym * kTcVS + 8 * s);
           const float4 y1 = *reinterpret_cast<const float4*>(ey + ym * kTcVS + 8 * s + 4);
-          split_tf32(x0.x * y0.x, h[0], l[0]);
-          split_tf32(x0.y * y0.y, h[1], l[1]);
-          split_tf32(x0.z * y0.z, h[2], l[2]);
-          split_tf32(x0.w * y0.w, h[3], l[3]);
-          split_tf32(x1.x * y1.x, h[4], l[4]);
-          split_tf32(x1.y * y1.y, h[5], l[5]);
-          split_tf32(x1.z * y1.z, h[6], l[6]);
-          split_tf32(x1.w * y1.w, h[7], l[7]);
+          // products and splits two at a time (packed FP32x2)
+          const float2 pr[4] = {__fmul2_rn(make_float2(x0.x, x0.y), make_float2(y0.x, y0.y)),
+                                __fmul2_rn(make_float2(x0.z, x0.w), make_float2(y0.z, y0.w)),
+                                __fmul2_rn(make_float2(x1.x, x1.y), make_float2(y1.x, y1.y)),
+                                __fmul2_rn(make_float2(x1.z, x1.w), make_float2(y1.z, y1.w))};
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            float2 hi2, lo2;
+            split_tf32x2(pr[t], hi2, lo2);
+            h[2 * t] = hi2.x; h[2 * t + 1] = hi2.y;
+            l[2 * t] = lo2.x; l[2 * t + 1] = lo2.y;
+          }
         }
         const uint32_t ah = sbase + S::OffAhi + s * kTcAStep + tid * 16;
         const uint32_t al = sbase + S::OffAlo + s * kTcAStep + tid * 16;
@@ -287,10 +291,13 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
               const int v = s * 8 + k0;
               const float4 e4 = *reinterpret_cast<const float4*>(ew + plane * kTcVS + v);
               const float4 c4 = *reinterpret_cast<const float4*>(val + tab_sw(cc, v));
-              split_tf32(e4.x * c4.x, h[0], l[0]);
-              split_tf32(e4.y * c4.y, h[1], l[1]);
-              split_tf32(e4.z * c4.z, h[2], l[2]);
-              split_tf32(e4.w * c4.w, h[3], l[3]);
+              const float2 p0 = __fmul2_rn(make_float2(e4.x, e4.y), make_float2(c4.x, c4.y));
+              const float2 p1 = __fmul2_rn(make_float2(e4.z, e4.w), make_float2(c4.z, c4.w));
+              float2 h0, l0, h1, l1;
+              split_tf32x2(p0, h0, l0);
+              split_tf32x2(p1, h1, l1);
+              h[0] = h0.x; h[1] = h0.y; h[2] = h1.x; h[3] = h1.y;
+              l[0] = l0.x; l[1] = l0.y; l[2] = l1.x; l[3] = l1.y;
             }
             const uint32_t bh = sbase + S::OffBhi + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
             const uint32_t bl = sbase + S::OffBlo + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;

@@ -65,6 +65,13 @@ __device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
   lo = x - hi;
 }
 
+// split_tf32 of two values; lo = hi * (-1) + x exactly, one packed FMA for both
+__device__ __forceinline__ void split_tf32x2(float2 x, float2& hi, float2& lo) {
+  hi.x = __uint_as_float((__float_as_uint(x.x) + 0x1000u) & 0xFFFFE000u);
+  hi.y = __uint_as_float((__float_as_uint(x.y) + 0x1000u) & 0xFFFFE000u);
+  lo = __ffma2_rn(hi, make_float2(-1.f, -1.f), x);
+}
+
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, float a, float b, float c, float d) {
   asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
 }
