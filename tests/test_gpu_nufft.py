@@ -288,3 +288,27 @@ def test_pipeline_accumulates_over_calls(ctx):
     b = pl.images()
     pl.close()
     assert _rel_l2(b, a.astype(np.float64)) <= 1e-5
+
+
+def test_pipeline_reads_only_lower_triangle(ctx):
+    """The pipeline reads (and, for host inputs, copies) only the lower triangle of each
+    S: NaN above the diagonal gives the same images."""
+    import bipp_b200 as bipp
+
+    cfg, obs, s, xyz = _pipeline_case(n_ant=48, n_steps=3, image=32, keep=(30, 48))
+    intervals = np.array([[0.0, 1.0], [1.0, np.inf]])
+    n = cfg.image_size
+    wl = np.full(s.shape[0], cfg.wl)
+    s_upper_nan = s.copy()
+    iu = np.triu_indices(cfg.n_antenna, 1)
+    for k in range(s.shape[0]):
+        s_upper_nan[k][iu] = np.nan
+    imgs = []
+    for sk in (s, s_upper_nan):
+        pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, _lattice(obs, n), obs.lmn[:, 2], obs.basis,
+                           tolerance=1e-6)
+        pl.process(sk, xyz, wl)
+        imgs.append(pl.images())
+        pl.close()
+    assert np.all(np.isfinite(imgs[1]))
+    assert _rel_l2(imgs[1], imgs[0].astype(np.float64)) <= 1e-6
