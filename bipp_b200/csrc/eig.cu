@@ -159,6 +159,7 @@ void EigWork<T>::reserve(bipp_ctx_s* ctx, int nBatch, int nmax) {
   e.alloc(ctx, (size_t)nmax * sizeof(double) * nBatch);
   tau.alloc(ctx, (size_t)nmax * sizeof(C) * nBatch);
   krange.alloc(ctx, (size_t)2 * sizeof(int) * nBatch);
+  order.alloc(ctx, (size_t)sizeof(int) * nBatch);
 }
 
 template <typename T>
@@ -304,9 +305,14 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       if (blocked) k = hetrd_blk_kernel<C, R>;
     }
     smem_optin(k, smem);
+    // largest matrices first, so that the last wave holds the small ones
+    int* order = w.order.template get<int>();
+    count_launch();
+    order_by_size_kernel<<<1, 1024, 0, st>>>(nred, nb, order);
+    B2_CHECK_LAUNCH();
     count_launch();
     k<<<nb, trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
-                                     w.tau.template get<C>());
+                                     w.tau.template get<C>(), order);
     B2_CHECK_LAUNCH();
   }
   // 4. tridiagonal eigenpairs (FP64); workspace aliases W64 (free after trinv)

@@ -10,7 +10,7 @@ namespace bippb200 {
 template <typename T>
 struct EigWork {
   int capBatch = 0, Nmax = 0;
-  DevBuf A, G, W64, Linv, T1, Z, d, e, tau, krange;
+  DevBuf A, G, W64, Linv, T1, Z, d, e, tau, krange, order;
   void reserve(bipp_ctx_s* ctx, int nBatch, int Nmax);
   // compacted eigenvectors (column c = eigenvector of eigenvalue c), ld Nmax
   typename Cplx<T>::type* X(bool gram);

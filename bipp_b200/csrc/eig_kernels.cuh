@@ -299,9 +299,10 @@ cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* 
       for (int tj = 0; tj <= ti; ++tj) {
         const int i0 = t0 + ti * 64, j0 = t0 + tj * 64;
         __syncthreads();
+        // the row panel of tile row ti is loaded once, the column panel per tile
         for (int e = tid; e < 64 * kCholNB; e += blockDim.x) {
           const int r = e % 64, c = e / 64;
-          Pi[r][c] = (i0 + r < n && c < kb) ? Gb[(i0 + r) + (long long)(k0 + c) * Nmax] : zero;
+          if (tj == 0) Pi[r][c] = (i0 + r < n && c < kb) ? Gb[(i0 + r) + (long long)(k0 + c) * Nmax] : zero;
           Pj[r][c] = (j0 + r < n && c < kb) ? Gb[(j0 + r) + (long long)(k0 + c) * Nmax] : zero;
         }
         __syncthreads();
@@ -980,15 +981,42 @@ __device__ __forceinline__ void hetd2_tail(C* __restrict__ Ab, int n, int Nmax, 
 }
 
 
+// order[r] = the matrix of rank r when sorted by size, largest first (ties by index):
+// one CTA, rank of each matrix by counting (nb is at most a few thousand)
+static __global__ void order_by_size_kernel(const int* __restrict__ nred, int nb, int* __restrict__ order) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int nbv = nred[b];
+    int rank = 0;
+    for (int c = 0; c < nb; ++c) {
+      const int nc = nred[c];
+      rank += (nc > nbv) || (nc == nbv && c < b);
+    }
+    order[rank] = b;
+  }
+}
+
 // Householder tridiagonalisation of every matrix of the batch, unblocked (LAPACK ?hetd2).
 template <typename C, typename R>
 __global__ void __launch_bounds__(kTrdThreads)
 hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
-             double* __restrict__ eOut, C* __restrict__ tauOut) {
+             double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int b = blockIdx.x;
+  const int b = order ? order[blockIdx.x] : blockIdx.x;
   hetd2_tail<C, R>(A + (long long)b * Nmax * Nmax, nred[b], Nmax, 0, dOut + (long long)b * Nmax,
                    eOut + (long long)b * Nmax, tauOut + (long long)b * Nmax, smem_raw);
+}
+
+// sums of two values over the block with one pair of barriers; scratch holds 64 values
+template <typename R>
+__device__ __forceinline__ void block_sum2(R& a, R& b, R* scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (lane == 0) { scratch[wid] = a; scratch[32 + wid] = b; }
+  __syncthreads();
+  a = warp_sum((lane < nw) ? scratch[lane] : R(0));
+  b = warp_sum((lane < nw) ? scratch[32 + lane] : R(0));
 }
 
 // Blocked tridiagonalisation (LAPACK ?hetrd with ?latrd panels, lower), single precision.
@@ -1055,10 +1083,10 @@ __device__ __forceinline__ void trd_her2k(float2* __restrict__ Ab, int Nmax, int
 template <typename C, typename R>
 __global__ void __launch_bounds__(kTrdThreads)
 hetrd_blk_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
-                 double* __restrict__ eOut, C* __restrict__ tauOut) {
+                 double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr) {
   static_assert(sizeof(C) == 8, "single precision");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int b = blockIdx.x;
+  const int b = order ? order[blockIdx.x] : blockIdx.x;
   const int n = nred[b];
   C* Ab = A + (long long)b * Nmax * Nmax;
   double* d = dOut + (long long)b * Nmax;
@@ -1068,7 +1096,7 @@ hetrd_blk_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, doub
   C* y = v + Nmax;                          // [Nmax] mat-vec, then w
   C* VW = reinterpret_cast<C*>(smem_raw + ((5 * (size_t)Nmax * 8 + 15) & ~(size_t)15));  // [Nmax][kTrdVWS]
   C* tq = VW + (long long)Nmax * kTrdVWS;   // [2 kTrdNB] W^H v, then V^H v
-  __shared__ R red[32];
+  __shared__ R red[64];
   __shared__ C s_tau;
   __shared__ R s_beta;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
@@ -1144,8 +1172,7 @@ hetrd_blk_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, doub
         pr += pv.x;
         pi += pv.y;
       }
-      pr = block_sum(pr, red);
-      pi = block_sum(pi, red);
+      block_sum2(pr, pi, red);
       const C alph = cscale(cmul(tau, mk(pr, pi)), R(-0.5));
       for (int r = tid; r < m; r += T) VW[(long long)(c + 1 + r) * kTrdVWS + 2 * j + 1] = y[r] + cmul(alph, v[r]);
       __syncthreads();
