@@ -209,6 +209,12 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     gram_whgw_kernel<C><<<256, 256, 0, st>>>(L.nAnt, nred0, L.W, L.ldw, L.idx, tmp.get<double2>(), G, Nmax);
     B2_CHECK_LAUNCH();
   }
+  // per-matrix kernels take the matrices largest first, so that their last wave holds
+  // the smallest ones
+  int* sizeOrder = w.order.template get<int>();
+  count_launch();
+  order_by_size_kernel<<<1, 1024, 0, st>>>(nred, nb, sizeOrder);
+  B2_CHECK_LAUNCH();
   const int tiles = (Nmax + kGemmBM - 1) / kGemmBM;
   const bool realG = L.gram && L.identityW;
   if (L.gram) {
@@ -218,12 +224,12 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       smem_optin(k, chol_smem<double>());
       count_launch();
       k<<<nb, kCholThreads, chol_smem<double>(), st>>>(reinterpret_cast<double*>(G), nred, Nmax,
-                                                        L.status + L.batchOffset);
+                                                        L.status + L.batchOffset, sizeOrder);
     } else {
       auto k = cholesky_kernel<double2>;
       smem_optin(k, kCholSmem);
       count_launch();
-      k<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset);
+      k<<<nb, kCholThreads, kCholSmem, st>>>(G, nred, Nmax, L.status + L.batchOffset, sizeOrder);
     }
     B2_CHECK_LAUNCH();
     mark(2);
@@ -232,12 +238,12 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       smem_optin(k, trinv_smem<double>());
       count_launch();
       k<<<nb, 256, trinv_smem<double>(), st>>>(reinterpret_cast<const double*>(G), reinterpret_cast<double*>(W64),
-                                               reinterpret_cast<R*>(Linv), nred, Nmax);
+                                               reinterpret_cast<R*>(Linv), nred, Nmax, sizeOrder);
     } else {
       auto k = trinv_kernel<double2, C>;
       smem_optin(k, kTrinvSmem);
       count_launch();
-      k<<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax);
+      k<<<nb, 256, kTrinvSmem, st>>>(G, W64, Linv, nred, Nmax, sizeOrder);
     }
     B2_CHECK_LAUNCH();
     // T1 = Linv * A (Linv real for W = I)
@@ -305,14 +311,9 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       if (blocked) k = hetrd_blk_kernel<C, R>;
     }
     smem_optin(k, smem);
-    // largest matrices first, so that the last wave holds the small ones
-    int* order = w.order.template get<int>();
-    count_launch();
-    order_by_size_kernel<<<1, 1024, 0, st>>>(nred, nb, order);
-    B2_CHECK_LAUNCH();
     count_launch();
     k<<<nb, trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
-                                     w.tau.template get<C>(), order);
+                                     w.tau.template get<C>(), sizeOrder);
     B2_CHECK_LAUNCH();
   }
   // 4. tridiagonal eigenpairs (FP64); workspace aliases W64 (free after trinv)
@@ -324,7 +325,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     count_launch();
     k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
-                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues);
+                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues, sizeOrder);
     B2_CHECK_LAUNCH();
   }
   // 5. back-transform Y = Q Z -> T1
@@ -346,7 +347,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     const size_t smem = bt_apply_smem(Nmax, sizeof(C), NT);                                  \
     smem_optin(k, smem);                                                                     \
     count_launch();                                                                          \
-    k<<<grid, NT, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange);                  \
+    k<<<grid, NT, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange, sizeOrder);       \
   }
     // 64 row groups of 256 threads up to 512 rows; 128 row groups of 512 threads above
     if (Nmax <= 512) {
@@ -367,13 +368,14 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
       smem_optin(k, smem16);
       count_launch();
       k<<<dim3((Nmax + 15) / 16, nb), kBtThreads, smem16, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1,
-                                                                  krange);
+                                                                  krange, sizeOrder);
     } else {
       const size_t smem4 = ((size_t)Nmax * 4 + Nmax + kBtThreads) * sizeof(C);
       auto k = backtransform_kernel<C, R, 4>;
       smem_optin(k, smem4);
       count_launch();
-      k<<<dim3((Nmax + 3) / 4, nb), kBtThreads, smem4, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1, krange);
+      k<<<dim3((Nmax + 3) / 4, nb), kBtThreads, smem4, st>>>(A, w.tau.template get<C>(), Z, nred, Nmax, T1, krange,
+                                                              sizeOrder);
     }
     B2_CHECK_LAUNCH();
   }

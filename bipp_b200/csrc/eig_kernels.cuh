@@ -191,8 +191,9 @@ __device__ __forceinline__ double e_div(double a, double d) { return a / d; }
 // the kernel at three CTAs per SM in the real case.
 template <typename E>
 __global__ void __launch_bounds__(kCholThreads, sizeof(E) == 8 ? 3 : 1)
-cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status) {
-  const int b = blockIdx.x;
+cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status,
+                const int* __restrict__ order = nullptr) {
+  const int b = order ? order[blockIdx.x] : blockIdx.x;
   const int n = nred[b];
   E* Gb = G + (long long)b * Nmax * Nmax;
   extern __shared__ __align__(16) unsigned char chol_raw[];
@@ -363,9 +364,9 @@ constexpr size_t kTrinvSmem = trinv_smem<double2>();
 template <typename E, typename O>
 __global__ void __launch_bounds__(256)
 trinv_kernel(const E* __restrict__ L, E* __restrict__ W64, O* __restrict__ LinvOut, const int* __restrict__ nred,
-             int Nmax) {
+             int Nmax, const int* __restrict__ order = nullptr) {
   constexpr int NB = 32;
-  const int b = blockIdx.x;
+  const int b = order ? order[blockIdx.x] : blockIdx.x;
   const int n = nred[b];
   const E* Lb = L + (long long)b * Nmax * Nmax;
   E* Wb = W64 + (long long)b * Nmax * Nmax;
@@ -1216,8 +1217,8 @@ __global__ void __launch_bounds__(kTriThreads)
 tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, const int* __restrict__ nred,
                int Nmax, double* __restrict__ lamOut, R* __restrict__ Z, double* __restrict__ work,
                int* __restrict__ status, double vecLo = -INFINITY, double vecHi = INFINITY,
-               int* __restrict__ krange = nullptr, int allValues = 1) {
-  const int b = blockIdx.x;
+               int* __restrict__ krange = nullptr, int allValues = 1, const int* __restrict__ order = nullptr) {
+  const int b = order ? order[blockIdx.x] : blockIdx.x;
   const int n = nred[b];
   if (n <= 0) return;
   extern __shared__ double smem_d[];
@@ -1432,8 +1433,9 @@ constexpr int kBtThreads = 256;
 template <typename C, typename R, int kBtCols>
 __global__ void __launch_bounds__(kBtThreads)
 backtransform_kernel(const C* __restrict__ A, const C* __restrict__ taus, const R* __restrict__ Z,
-                     const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange) {
-  const int b = blockIdx.y;
+                     const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange,
+                const int* __restrict__ order = nullptr) {
+  const int b = order ? order[blockIdx.y] : blockIdx.y;
   const int n = nred[b];
   const int c0 = blockIdx.x * kBtCols;
   if (c0 >= n) return;
@@ -1566,8 +1568,9 @@ constexpr int kBtJC = 2;                     // reflectors per register chunk
 template <typename C, typename R, int KR, int NT>
 __global__ void __launch_bounds__(NT, (sizeof(C) == 8 ? 512 : 256) / NT > 0 ? (sizeof(C) == 8 ? 512 : 256) / NT : 1)
 bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tStride, const R* __restrict__ Z,
-                const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange) {
-  const int b = blockIdx.y;
+                const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange,
+                const int* __restrict__ order = nullptr) {
+  const int b = order ? order[blockIdx.y] : blockIdx.y;
   const int n = nred[b];
   const int c0 = blockIdx.x * kBtCB;
   if (c0 >= n) return;
