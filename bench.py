@@ -139,7 +139,7 @@ class ClockSampler:
 
 def make_inputs(cfg, rank, device):
     """Seeded inputs on the GPU, one entry per (time step, frequency channel), entry
-    t * n_channels + c: S^T (column-major S), xyz, wl."""
+    t * n_channels + c: S^T (column-major S), xyz, wl. Ranks differ only in the noise."""
     import torch
 
     from bipp_b200 import simulate as sim
@@ -156,7 +156,7 @@ def make_inputs(cfg, rank, device):
         steps = list(range(s0, min(T, s0 + chunk)))
         for c in range(C):
             s, x = sim.visibilities(obs, steps, device=device, dtype=torch.complex64, masks=masks, wl=float(wls[c]),
-                                    noise_key=c)
+                                    noise_key=c + 64 * rank)
             S[s0 * C + c:(s0 + len(steps)) * C:C] = s.transpose(1, 2)
             xyz[s0 * C + c:(s0 + len(steps)) * C:C] = x
             wl[s0 * C + c:(s0 + len(steps)) * C:C] = float(wls[c])
@@ -354,9 +354,16 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     device = torch.device("cuda", local)
     ctx = bipp.Context("GPU", device=local)
-    cfg = workload_config(args, rank)
+    # every rank images its own batch of the same observation (array, sky, flags), with
+    # its own noise draw
+    cfg = workload_config(args)
     obs, S, xyz, wl = make_inputs(cfg, rank, device)
     intervals = calibrate_levels(ctx, cfg, S, xyz, wl)
+    if world > 1:
+        # every rank images with rank 0's energy levels, so that the level images add up
+        iv = torch.from_numpy(np.ascontiguousarray(intervals, dtype=np.float64)).to(device)
+        dist.broadcast(iv, src=0)
+        intervals = iv.cpu().numpy()
     n = cfg.image_size
     pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
                        tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, S.shape[0]), max_steps=S.shape[0],
