@@ -190,6 +190,17 @@ def calibrate_levels(ctx, cfg, S, xyz, wl, n_cal=64):
     return infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d)
 
 
+def share_levels(intervals, device):
+    """Rank 0's energy-level intervals on every rank (a broadcast in the default process
+    group), so that the level images of all ranks add up."""
+    import torch
+    import torch.distributed as dist
+
+    iv = torch.from_numpy(np.ascontiguousarray(intervals, dtype=np.float64)).to(device)
+    dist.broadcast(iv, src=0)
+    return iv.cpu().numpy()
+
+
 def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, threads=None, wl=None):
     """The reference's CPU path (compiled reference sources) on a bounded sample:
     eigh_gram<float> + virtual_vis<float> per level on n_eig_steps entries, and the
@@ -360,10 +371,7 @@ def main():
     obs, S, xyz, wl = make_inputs(cfg, rank, device)
     intervals = calibrate_levels(ctx, cfg, S, xyz, wl)
     if world > 1:
-        # every rank images with rank 0's energy levels, so that the level images add up
-        iv = torch.from_numpy(np.ascontiguousarray(intervals, dtype=np.float64)).to(device)
-        dist.broadcast(iv, src=0)
-        intervals = iv.cpu().numpy()
+        intervals = share_levels(intervals, device)
     n = cfg.image_size
     pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
                        tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, S.shape[0]), max_steps=S.shape[0],

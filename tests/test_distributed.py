@@ -76,3 +76,34 @@ def test_gloo_sharded_synthesis_equals_single_process(size):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert np.abs(got - full).max() <= 1e-5 * np.abs(full).max()
+
+
+def _levels_worker(rank, size, port, out_q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size)
+    import bench
+
+    # each rank calibrated its own levels; all must use rank 0's
+    mine = np.array([[0.0, 1.0 + rank], [1.0 + rank, np.inf]])
+    shared = bench.share_levels(mine, torch.device("cpu"))
+    out_q.put((rank, shared))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gloo_bench_levels_are_rank0s():
+    """bench.py on N GPUs: every rank images with rank 0's energy levels (inf included)."""
+    size = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_levels_worker, args=(r, size, port, q)) for r in range(size)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(size)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for _, lv in got:
+        assert np.array_equal(lv, np.array([[0.0, 1.0], [1.0, np.inf]]))
