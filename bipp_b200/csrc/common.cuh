@@ -40,7 +40,7 @@ inline void require(bool ok, const char* msg, BippError code = BIPP_INVALID_PARA
 // Per-matrix status bits written by kernels and read back by the host.
 enum StatusBits : int {
   kStatusCholeskyNotPD = 1,   // non-positive pivot in the FP64 Cholesky of G
-  kStatusNonFinite = 2,       // NaN/Inf met in the inputs or the reduction
+  kStatusNonFinite = 2,       // NaN/Inf in an entry of S that enters the reduced matrix
   kStatusClusterFix = 4,      // eigenvector cluster re-orthogonalised (informational)
   kStatusTensorTimeout = 8,   // a tensor-core MMA completion wait ran out (GPU error)
 };

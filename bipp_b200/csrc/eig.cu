@@ -508,6 +508,7 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   // nred from the flag pass is authoritative even when nred was 0 (kernels skipped)
   if (status & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
   if (status & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
+  if (status & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
   for (size_t c = 0; c < nBeam; ++c) d[c] = (c < (size_t)nred) ? (T)lam[c] : T(0);
   if (v) {
     B2_CUDA(cudaMemcpy2DAsync(v, ldv * sizeof(C), dOut.get(), nAntenna * sizeof(C), nAntenna * sizeof(C), nBeam,
@@ -585,6 +586,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
   for (size_t b = 0; b < nBatch; ++b) {
     if (stat[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
     if (stat[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
+    if (stat[b] & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
     nBeamReduced[b] = (size_t)nredh[b];
     scale[b] = nvish[b] ? 1.0f / (float)nvish[b] : 0.0f;
   }

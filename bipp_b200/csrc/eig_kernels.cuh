@@ -63,7 +63,20 @@ prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long s
       }
     }
     long long nvis = block_sum(cnt, red_ll);
-    if (bad) atomicOr(status + bg, (int)kStatusNonFinite);
+    // a non-finite entry fails the flag test; it is an error only where its row and
+    // column are both kept, i.e. where it enters the reduced matrix (the reference's
+    // LAPACK call then returns info != 0)
+    if (__syncthreads_or(bad)) {
+      int kept = 0;
+      for (int col = warp; col < nBeam; col += nwarp) {
+        if (!flags[col]) continue;
+        for (int row = col + lane; row < nBeam; row += 32) {
+          const C v = Sb[row + (long long)col * lds];
+          if ((!isfinite(v.x) || !isfinite(v.y)) && flags[row]) kept = 1;
+        }
+      }
+      if (kept) atomicOr(status + bg, (int)kStatusNonFinite);
+    }
     __syncthreads();
     // compaction scan (warp 0)
     if (warp == 0) {

@@ -306,6 +306,20 @@ static void copy_lower_blocks(bipp_ctx_s* ctx, float2* dst, const float2* src, i
   }
 }
 
+// Status words of steps [s0, s0 + nb) after their eigensolve: a failed step ends the call
+// before anything is added to the images (the reference throws at the failing step,
+// src/host/lapack_api.hpp:133, before its NUFFT update).
+static void check_steps(bipp_pipeline_s* p, int s0, int nb) {
+  std::vector<int> st(nb);
+  d2h(p->ctx, st.data(), p->status.get<int>() + s0, nb * sizeof(int));
+  sync(p->ctx);
+  for (int b = 0; b < nb; ++b) {
+    if (st[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
+    if (st[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
+    if (st[b] & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
+  }
+}
+
 static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, const double* xyz, const double* wl,
                              int onDevice) {
   bipp_ctx_s* ctx = p->ctx;
@@ -358,6 +372,8 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     float a;
     cudaEventElapsedTime(&a, ev0, ev1);
     p->stageMs[2] += a;
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
   }
   std::vector<long long> pairOff(T + 1, 0);
   for (int b = 0; b < T; ++b) pairOff[b + 1] = pairOff[b] + (long long)nredH[b] * (nredH[b] + 1) / 2;
@@ -374,6 +390,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
     p->core.end_count(pairOff[T]);
     for (int s0 = 0; s0 < T; s0 += chunk) pipeline_chunk(p, s0, std::min(chunk, T - s0), pairOff, L, 0, false, ms);
+    check_steps(p, 0, T);
     double nm[4] = {0, 0, 0, 0};
     p->core.execute(p->images.get<float>(), p->P, p->timing ? nm : nullptr);
     p->stageMs[3] += nm[0];
@@ -388,6 +405,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
         pipeline_count(p, b, 1, pairOff);
         p->core.end_count(pairOff[b + 1] - pairOff[b]);
         pipeline_chunk(p, b, 1, pairOff, 1, l, l > 0, ms);
+        if (l == 0) check_steps(p, b, 1);
         double nm[4] = {0, 0, 0, 0};
         p->core.execute(p->images.get<float>() + (long long)l * p->P, p->P, p->timing ? nm : nullptr);
         p->stageMs[3] += nm[0];
@@ -400,14 +418,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   // keep eigenvalues of this call for calibration (host copy on demand)
   p->lastNred = nredH;
   p->stepsDone += T;
-  std::vector<int> st(T);
-  d2h(ctx, st.data(), p->status.get(), T * sizeof(int));
   sync(ctx);
-  if (p->timing) { cudaEventDestroy(ev0); cudaEventDestroy(ev1); }
-  for (int b = 0; b < T; ++b) {
-    if (st[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
-    if (st[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
-  }
 }
 
 extern "C" {

@@ -66,7 +66,12 @@ BIPP_B200_EXPORT BippError bipp_ctx_stream(bipp_ctx_t ctx, void** stream);
  * antenna positions; replaces bipp::eigh_gram<float/double> (include/bipp/bipp.hpp:70-75,
  * src/eigensolver.cpp:129-225). s: nBeam x nBeam (lower triangle used), w: nAntenna x
  * nBeam, xyz: nAntenna x 3. Outputs d[nBeam] ascending, zero padded; v nAntenna x nBeam
- * zero padded; *nBeamReduced and *scale = 1/nVis as the reference's returned pair. */
+ * zero padded; *nBeamReduced and *scale = 1/nVis as the reference's returned pair.
+ * Errors as the reference's LAPACK ?hegv (src/host/lapack_api.hpp:112-158, info != 0 ->
+ * EigensolverError): BIPP_EIGENSOLVER_ERROR when G is not positive definite or when a
+ * NaN/Inf entry of S's lower triangle lies in a kept row and column. A NaN/Inf entry fails
+ * the flag test like a zero, so an antenna whose entries are all NaN is dropped, and
+ * entries above the diagonal are never read. */
 BIPP_B200_EXPORT BippError bipp_eigh_gram_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam,
                                             const void* s, size_t lds, const void* w, size_t ldw,
                                             const float* xyz, size_t ldxyz, float* d, void* v, size_t ldv,
@@ -77,7 +82,8 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_d(bipp_ctx_t ctx, double wl, size_t nA
                                             size_t* nBeamReduced, double* scale);
 
 /* Standard Hermitian eigenproblem of S; replaces bipp::eigh<float/double>
- * (include/bipp/bipp.hpp:47-51, src/eigensolver.cpp:40-127). */
+ * (include/bipp/bipp.hpp:47-51, src/eigensolver.cpp:40-127). Non-finite entries as for
+ * bipp_eigh_gram_s (the reference's ?heev, src/host/lapack_api.hpp:70-110). */
 BIPP_B200_EXPORT BippError bipp_eigh_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam, const void* s,
                                        size_t lds, const void* w, size_t ldw, float* d, void* v, size_t ldv,
                                        size_t* nBeamReduced, float* scale);
@@ -90,7 +96,8 @@ BIPP_B200_EXPORT BippError bipp_eigh_d(bipp_ctx_t ctx, double wl, size_t nAntenn
  * dataset creation (python/bipp/apps/create_dataset.py:78-103) calls eigh_gram once per
  * step; this is its batched form. s: [nBatch][nAntenna x nAntenna] (lds = nAntenna),
  * xyz: [nBatch][nAntenna x 3], wl: [nBatch]; d: [nBatch][nAntenna], v: [nBatch][nAntenna x
- * nAntenna]; nBeamReduced, scale: [nBatch]. */
+ * nAntenna]; nBeamReduced, scale: [nBatch]. Fails as bipp_eigh_gram_s when any step
+ * fails. */
 BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna,
                                                     const float* wl, const void* s, const float* xyz, float* d,
                                                     void* v, size_t* nBeamReduced, float* scale);
@@ -109,7 +116,7 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatc
  * s (nAntenna x nAntenna complex float, lower triangle used, lds), xyz (nAntenna x 3
  * double, ldxyz); outputs d[nAntenna] (ascending, zero padded), v (nAntenna x nAntenna,
  * ldv, zero padded), *nBeamReduced, *scale (= 1/nVis) and *info (1 if the Cholesky
- * factorisation of G failed, else 0). The call is asynchronous on `stream` (a
+ * factorisation of G failed or a kept entry of S is not finite, else 0). The call is asynchronous on `stream` (a
  * cudaStream_t). Every call on a device shares the array, so calls that overlap on the
  * GPU race; serialise them (one stream, or events). The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress) and should come before any stream
@@ -243,10 +250,13 @@ BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipel
 /* Process nSteps time steps: s [nSteps][nAntenna x nAntenna] complex float (lower triangle
  * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. onDevice != 0: the
  * three pointers are device pointers (s is read in place, not modified), else host
- * pointers (copied in by the call; of s only the lower triangle is copied, in blocks of 64
- * columns from each block's diagonal row down). The steps' contributions are accumulated into the
- * images. Fails with BIPP_EIGENSOLVER_ERROR when a Gram matrix is not positive definite
- * and with BIPP_GPU_ERROR when a tensor-core completion wait runs out (a GPU fault). */
+ * pointers (copied in by the call; of s only the lower triangle is copied, in blocks of
+ * 64 columns from each block's diagonal row down). The steps' contributions are
+ * accumulated into the images. Fails with BIPP_EIGENSOLVER_ERROR when a Gram matrix is
+ * not positive definite or a kept entry of some S is not finite (as bipp_eigh_gram_s;
+ * checked after the eigensolve, so a failing call adds nothing to the images in batched
+ * mode, while plain mode keeps the steps before the failing one), and with
+ * BIPP_GPU_ERROR when a tensor-core completion wait runs out (a GPU fault). */
 BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s,
                                                  const double* xyz, const double* wl, int onDevice);
 /* Images [nLevels][nPixel] (normalised by the number of processed steps if normalize),

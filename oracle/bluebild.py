@@ -16,6 +16,19 @@ import scipy.linalg as sla
 TWO_PI = 2.0 * 3.14159265358979323846
 
 
+class EigensolverError(RuntimeError):
+    """The reference's EigensolverError (include/bipp/exceptions.hpp), raised when its LAPACK
+    call returns info != 0 (src/host/lapack_api.hpp:88, 109, 133, 157)."""
+
+
+def _check_reduced(s_red, g=None):
+    """The reduced lower triangle of S (and G) must be finite: the reference hands it to
+    LAPACK ?heev/?hegv, which reports a NaN/Inf entry as info != 0 (observed with the
+    compiled reference sources), raised as EigensolverError."""
+    if not np.isfinite(np.tril(s_red)).all() or (g is not None and not np.isfinite(g).all()):
+        raise EigensolverError("non-finite entry in the reduced matrix")
+
+
 # --- flagging + compaction -------------------------------------------------------
 
 def flag_nonzero_gram(s, eps):
@@ -76,7 +89,11 @@ def eigh_gram(wl, s, w, xyz, dtype=np.float64):
         s_red = np.tril(s_red) + np.tril(s_red, -1).conj().T  # lower half is used
         w_red = w[:, idx]
         g = gram_matrix(w_red, xyz, wl)
-        dd, x = sla.eigh(s_red, g)
+        _check_reduced(s_red, g)
+        try:
+            dd, x = sla.eigh(s_red, g)
+        except np.linalg.LinAlgError as e:  # G not positive definite: ?hegv info > n
+            raise EigensolverError(str(e)) from e
         d[:nred] = dd
         v[:, :nred] = w_red @ x
     scale = 1.0 / nvis if nvis else 0.0
@@ -97,6 +114,7 @@ def eigh(wl, s, w, dtype=np.float64):
     v = np.zeros((n_ant, n_beam), dtype=ct)
     if nred:
         s_red = s[np.ix_(idx, idx)]
+        _check_reduced(s_red)
         s_red = np.tril(s_red) + np.tril(s_red, -1).conj().T
         dd, x = np.linalg.eigh(s_red)
         d[:nred] = dd

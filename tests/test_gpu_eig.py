@@ -7,7 +7,7 @@ FP32 entry points agree with the FP64 reference to 1e-5 relative on eigenvalues
 import numpy as np
 import pytest
 
-from conftest import golden
+from conftest import golden, nonfinite_cases
 from oracle import bluebild as bb
 
 pytestmark = pytest.mark.gpu
@@ -156,6 +156,57 @@ def test_invalid_gram_raises_eigensolver_error(ctx):
     xyz[3, 0] = np.nan
     with pytest.raises(bipp.EigensolverError):
         bipp.eigh_gram(2.0, s, np.eye(n), xyz, ctx=ctx)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("fn", ["eigh_gram", "eigh"])
+def test_nonfinite_entries_as_reference(ctx, prec, fn):
+    """Non-finite visibilities behave as in the reference (the oracle is pinned to the
+    compiled reference on these cases): a NaN antenna is dropped like a zero antenna, a
+    NaN above the diagonal is never read, a NaN/Inf in a kept entry of the lower triangle
+    raises EigensolverError, and the context stays usable after the error."""
+    import bipp_b200 as bipp
+
+    xyz, zero_ant, nan_ant, upper, bad = nonfinite_cases()
+    n = zero_ant.shape[0]
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    eye = np.eye(n, dtype=ct)
+    xyz_t = xyz.astype(dt)
+    if fn == "eigh_gram":
+        call = lambda s: bipp.eigh_gram_full(dt(2.0), s.astype(ct), eye, xyz_t, ctx=ctx)  # noqa: E731
+        orc = lambda s: bb.eigh_gram(2.0, s.astype(ct), np.eye(n), xyz_t.astype(np.float64))  # noqa: E731
+    else:
+        call = lambda s: bipp.eigh(dt(2.0), s.astype(ct), eye, ctx=ctx, full=True)  # noqa: E731
+        orc = lambda s: bb.eigh(2.0, s.astype(ct), np.eye(n))  # noqa: E731
+    tol_d, tol_p = (1e-10, 1e-9) if prec == "f64" else (1e-5, 1e-4)
+    for s in (zero_ant, nan_ant, upper):
+        v, d, nr, sc = call(s)
+        vr, dr, nrr, scr = orc(s)
+        assert nr == nrr and abs(sc - scr) <= 1e-6 * scr
+        assert _rel(d, dr) <= tol_d
+        assert _rel(_prod(v, d), _prod(vr, dr)) <= tol_p
+    for name, s in bad.items():
+        with pytest.raises(bipp.EigensolverError):
+            call(s)
+    assert call(zero_ant)[2] == n - 1
+
+
+def test_nonfinite_entries_batched(ctx):
+    """The batched eigh_gram: a NaN antenna step equals its zero-antenna twin, and one step
+    with a NaN in a kept entry fails the call with EigensolverError."""
+    import bipp_b200 as bipp
+
+    xyz, zero_ant, nan_ant, upper, bad = nonfinite_cases()
+    xyz3 = np.stack([xyz] * 3).astype(np.float32)
+    wl = np.full(3, 2.0, dtype=np.float32)
+    s = np.stack([zero_ant, nan_ant, upper]).astype(np.complex64)
+    v, d, nred, scale = bipp.eigh_gram_batched(wl, s, xyz3, ctx=ctx)
+    assert nred[0] == nred[1] == 23 and nred[2] == 24 and scale[0] == scale[1]
+    assert _rel(d[1], d[0]) <= 1e-6
+    assert _rel(_prod(v[1], d[1]), _prod(v[0], d[0])) <= 1e-5
+    s[1] = bad["lower"].astype(np.complex64)
+    with pytest.raises(bipp.EigensolverError):
+        bipp.eigh_gram_batched(wl, s, xyz3, ctx=ctx)
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])

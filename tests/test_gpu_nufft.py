@@ -312,3 +312,36 @@ def test_pipeline_reads_only_lower_triangle(ctx):
         pl.close()
     assert np.all(np.isfinite(imgs[1]))
     assert _rel_l2(imgs[1], imgs[0].astype(np.float64)) <= 1e-6
+
+
+def test_pipeline_nonfinite_visibilities(ctx):
+    """Flagged antennas given as NaN rows and columns image like zero ones; a NaN in a kept
+    entry of the lower triangle of one step raises EigensolverError and adds nothing to
+    the images (the reference throws at that step, before its NUFFT update)."""
+    import bipp_b200 as bipp
+
+    cfg, obs, s, xyz = _pipeline_case(n_ant=48, n_steps=3, image=32, keep=(30, 48))
+    intervals = np.array([[0.0, 1.0], [1.0, np.inf]])
+    n = cfg.image_size
+    wl = np.full(s.shape[0], cfg.wl)
+    s_nan = s.copy()
+    for k in range(s.shape[0]):
+        flagged = np.abs(s[k]).sum(0) == 0
+        assert flagged.any()
+        s_nan[k][:, flagged] = np.nan
+        s_nan[k][flagged, :] = np.nan
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, _lattice(obs, n), obs.lmn[:, 2], obs.basis, tolerance=1e-6)
+    pl.process(s, xyz, wl)
+    a = pl.images()
+    pl.reset()
+    pl.process(s_nan, xyz, wl)
+    b = pl.images()
+    assert np.all(np.isfinite(b))
+    assert _rel_l2(b, a.astype(np.float64)) <= 1e-6
+    bad = s.copy()
+    kept = np.nonzero(np.abs(s[1]).sum(0) > 0)[0]
+    bad[1][kept[-1], kept[0]] = bad[1][kept[0], kept[-1]] = np.nan
+    with pytest.raises(bipp.EigensolverError):
+        pl.process(bad, xyz, wl)
+    assert np.array_equal(pl.images(), b)
+    pl.close()

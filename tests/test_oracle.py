@@ -4,7 +4,7 @@ the compiled reference directly when it is available in this container."""
 import numpy as np
 import pytest
 
-from conftest import golden
+from conftest import golden, nonfinite_cases
 from oracle import bluebild as bb
 from oracle import ref
 
@@ -127,3 +127,46 @@ def test_restatement_vs_compiled_reference_random():
     assert np.abs(d_r - d_o).max() <= 1e-12 * np.abs(d_r).max()
     g_r = ref.gram_matrix(w, xyz, 2.0)
     assert np.abs(g_r - bb.gram_matrix(w, xyz, 2.0)).max() <= 1e-14
+
+
+@pytest.mark.parametrize("fn", ["eigh_gram", "eigh"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_nonfinite_entries(fn, dtype):
+    """A NaN antenna is dropped like a zero antenna; a NaN/Inf in a kept entry of the lower
+    triangle raises EigensolverError; one above the diagonal is never read."""
+    xyz, zero_ant, nan_ant, upper, bad = nonfinite_cases()
+    n = zero_ant.shape[0]
+    call = (lambda s: bb.eigh_gram(2.0, s, np.eye(n), xyz, dtype=dtype)) if fn == "eigh_gram" else \
+        (lambda s: bb.eigh(2.0, s, np.eye(n), dtype=dtype))
+    vz, dz, nz, sz = call(zero_ant)
+    vn, dn, nn, sn = call(nan_ant)
+    assert nz == nn == n - 1 and sz == sn
+    assert np.array_equal(dz, dn) and np.array_equal(vz, vn)
+    assert call(upper)[2] == n
+    for s in bad.values():
+        with pytest.raises(bb.EigensolverError):
+            call(s)
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+@pytest.mark.parametrize("fn", ["eigh_gram", "eigh"])
+def test_nonfinite_entries_match_compiled_reference(fn):
+    xyz, zero_ant, nan_ant, upper, bad = nonfinite_cases()
+    n = zero_ant.shape[0]
+    for dt in (np.float64, np.float32):
+        if fn == "eigh_gram":
+            r = lambda s: ref.eigh_gram(2.0, s, np.eye(n), xyz, dtype=dt)  # noqa: E731
+            o = lambda s: bb.eigh_gram(2.0, s, np.eye(n), xyz, dtype=dt)  # noqa: E731
+        else:
+            r = lambda s: ref.eigh(2.0, s, np.eye(n), dtype=dt)  # noqa: E731
+            o = lambda s: bb.eigh(2.0, s, np.eye(n), dtype=dt)  # noqa: E731
+        for s in (nan_ant, upper):
+            vr, dr, nr, sr = r(s)
+            vo, do, no, so = o(s)
+            assert nr == no and abs(sr - so) <= 1e-6 * sr
+            assert np.abs(dr - do).max() <= (1e-12 if dt == np.float64 else 2e-5) * np.abs(dr).max()
+        for s in bad.values():
+            with pytest.raises(RuntimeError, match="BippError 6"):
+                r(s)
+            with pytest.raises(bb.EigensolverError):
+                o(s)
