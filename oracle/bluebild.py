@@ -157,6 +157,8 @@ def infer_intervals(n_level, sigma, cluster_func, d_min, d_max, d_all):
     """k-means level intervals, seed 42. python/bipp/parameter_estimator.py:55-105."""
     import sklearn.cluster as skcl
 
+    if cluster_func == "log" and d_min < 0:
+        raise ValueError(f'Cluster function "log" requires non-negative minimum eigenvalue restriction. Got {d_min}')
     d_all = np.array(d_all).flatten()
     d_all = d_all[d_all != 0.0]
     d_all = d_all[d_all >= d_min]

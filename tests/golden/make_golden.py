@@ -16,6 +16,9 @@ Outputs (compressed .npz, a few hundred KB in total):
                  seeded small problem.
   partition.npz  reference DomainPartition::grid (src/host/domain_partition.hpp:35-101) on the
                  seeded distributions of tests/test_domain_partition.cpp:102-131 (numpy RNG).
+  levels.npz     the reference's own Python energy-level estimator and eigenvalue filters
+                 (python/bipp/parameter_estimator.py:18-105, python/bipp/filter.py:7-51)
+                 on seeded eigenvalue spectra, loaded from the reference's source files.
 """
 from __future__ import annotations
 
@@ -135,12 +138,85 @@ def partition():
     np.savez_compressed(os.path.join(HERE, "partition.npz"), **out)
 
 
+def _load_reference_levels(refdir: str):
+    """The reference's parameter_estimator.py and filter.py, executed from its source tree.
+    Their package imports (bipp.pybipp, bipp.statistics, bipp.gram, bipp.imot_tools) are
+    stubbed with empty modules: the functions used here need only numpy and scikit-learn."""
+    import importlib.util
+    import types
+
+    names = ["bipp", "bipp.imot_tools", "bipp.imot_tools.math", "bipp.imot_tools.math.linalg",
+             "bipp.imot_tools.util", "bipp.imot_tools.util.argcheck", "bipp.statistics", "bipp.gram", "bipp.pybipp",
+             "bipp.filter"]
+    saved = {k: sys.modules.get(k) for k in names}
+    stubs = {k: types.ModuleType(k) for k in names}
+    for k, m in stubs.items():
+        if "." in k:
+            parent, child = k.rsplit(".", 1)
+            setattr(stubs[parent], child, m)
+    sys.modules.update(stubs)
+
+    def load(modname, rel):
+        spec = importlib.util.spec_from_file_location(modname, os.path.join(refdir, rel))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        return m
+
+    try:
+        filt = load("bipp.filter", os.path.join("python", "bipp", "filter.py"))
+        sys.modules["bipp.filter"] = filt
+        stubs["bipp"].filter = filt
+        pe = load("bipp_reference_parameter_estimator", os.path.join("python", "bipp", "parameter_estimator.py"))
+    finally:
+        for k, m in saved.items():
+            if m is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = m
+    return pe, filt
+
+
+# (n_level, sigma, cluster_func, d_min, d_max) cases of infer_intervals
+LEVEL_CASES = [(4, 1.0, "log", 0.0, np.inf), (8, 0.95, "log", 0.0, 1e6), (3, 0.9, "log", 1e-3, np.inf),
+               (1, 1.0, "log", 0.0, np.inf), (4, 1.0, "none", -50.0, 1e4), (2, 0.99, "none", 0.0, np.inf)]
+FILTERS = ["lsq", "std", "sqrt", "inv", "inv_sqrt"]
+
+
+def levels(refdir: str):
+    pe, filt = _load_reference_levels(refdir)
+    rng = np.random.default_rng(7)
+    # a spectrum like a time step's: a few strong source eigenvalues, a lognormal bulk,
+    # zeros (padding of flagged antennas) and small negative noise eigenvalues
+    d_all = np.concatenate([rng.lognormal(3.0, 1.5, 40), rng.lognormal(-1.0, 1.0, 1500), np.zeros(60),
+                            -rng.lognormal(-3.0, 0.5, 200)])
+    rng.shuffle(d_all)
+    out = {"d_all": d_all, "case_n": np.array([c[0] for c in LEVEL_CASES]),
+           "case_sigma": np.array([c[1] for c in LEVEL_CASES]), "case_func": np.array([c[2] for c in LEVEL_CASES]),
+           "case_lo": np.array([c[3] for c in LEVEL_CASES]), "case_hi": np.array([c[4] for c in LEVEL_CASES]),
+           "filters": np.array(FILTERS)}
+    for k, (n, sigma, f, lo, hi) in enumerate(LEVEL_CASES):
+        out[f"intervals_{k}"] = pe.infer_intervals(n, sigma, f, lo, hi, d_all)
+    # centroids in arbitrary order (the interval rule indexes the sorted centroids with
+    # the original positions)
+    for k, c in enumerate([np.array([10.0, 1.0, 0.1]), np.array([3.0, 10.0, 1.0, 0.1]), np.array([0.5, 7.0]),
+                           np.array([2.0])]):
+        out[f"centroid_{k}"] = c
+        out[f"centroid_intervals_{k}"] = pe.centroid_to_intervals(c, 0.0, 100.0)
+    d = np.array([-4.0, -0.25, 0.0, 0.25, 1.0, 9.0])
+    out["filter_d"] = d
+    for name in FILTERS:
+        out[f"filter_{name}"] = filt.apply_filter(name, d.copy())
+        out[f"filter_{name}_bounded"] = filt.Filter(name, -0.5, 2.0)(d.copy())
+    np.savez_compressed(os.path.join(HERE, "levels.npz"), **out)
+
+
 if __name__ == "__main__":
     refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     lofar(refdir)
     synth_eig()
     nuft()
     partition()
+    levels(refdir)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -195,7 +195,7 @@ def _lattice(obs, n):
     return (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
 
 
-def _oracle_pipeline(cfg, obs, s, xyz, intervals):
+def _oracle_pipeline(cfg, obs, s, xyz, intervals, filt="lsq"):
     steps = []
     for k in range(s.shape[0]):
         v, d, nr, sc = bb.eigh_gram(cfg.wl, s[k].astype(np.complex128), np.eye(cfg.n_antenna), xyz[k])
@@ -207,7 +207,7 @@ def _oracle_pipeline(cfg, obs, s, xyz, intervals):
     for st in steps:
         uvw = st["uvw"] * (bb.TWO_PI / st["wl"])
         for lv in range(intervals.shape[0]):
-            dl = bb.level_eigenvalues(st["d"], intervals[lv, 0], intervals[lv, 1])
+            dl = bb.level_eigenvalues(st["d"], intervals[lv, 0], intervals[lv, 1], filt)
             vv = bb.virtual_vis(st["scale"], dl, st["v"]).reshape(-1, order="F")
             out[:, lv] += bb.nuft_sum(1.0, vv, uvw[:, 0], uvw[:, 1], uvw[:, 2], obs.lmn[:, 0], obs.lmn[:, 1],
                                       obs.lmn[:, 2])
@@ -345,3 +345,28 @@ def test_pipeline_nonfinite_visibilities(ctx):
         pl.process(bad, xyz, wl)
     assert np.array_equal(pl.images(), b)
     pl.close()
+
+
+@pytest.mark.parametrize("filt", ["std", "sqrt", "inv", "inv_sqrt"])
+def test_pipeline_filters_vs_fp64_oracle(ctx, filt):
+    """The reference's eigenvalue filters (python/bipp/filter.py:7-51: level mask, then the
+    filter) through the batched pipeline, on two positive levels and one negative level
+    whose bounds sit in wide gaps of the spectra; a wrong filter is off by O(1)."""
+    import bipp_b200 as bipp
+
+    cfg, obs, s, xyz = _pipeline_case(n_ant=32, n_steps=3, image=24)
+    dmax = bb.eigh_gram(cfg.wl, s[0], np.eye(cfg.n_antenna), xyz[0])[1].max()
+    intervals = np.array([[0.2, np.inf], [0.02, 0.2], [-0.11, -0.02]]) * dmax
+    intervals[0, 1] = np.inf
+    ref_img, steps = _oracle_pipeline(cfg, obs, s, xyz, intervals, filt)
+    for st in steps:
+        for lo, hi in intervals:
+            assert ((st["d"] >= lo) & (st["d"] <= hi)).sum() >= 2
+    n = cfg.image_size
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, _lattice(obs, n), obs.lmn[:, 2], obs.basis, tolerance=1e-6,
+                       filter=filt)
+    pl.process(s, xyz, np.full(s.shape[0], cfg.wl))
+    img = pl.images()
+    pl.close()
+    for lv in range(intervals.shape[0]):
+        assert _rel_l2(img[lv], ref_img[:, lv]) <= 1e-3, (lv, _rel_l2(img[lv], ref_img[:, lv]))

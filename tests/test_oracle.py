@@ -170,3 +170,34 @@ def test_nonfinite_entries_match_compiled_reference(fn):
                 r(s)
             with pytest.raises(bb.EigensolverError):
                 o(s)
+
+
+def test_levels_and_filters_match_reference_python():
+    """Energy-level intervals (k-means, seed 42), the centroid-to-interval rule (also for
+    centroids in arbitrary order) and the five eigenvalue filters, unbounded and through
+    the level bounds, against the reference's own Python run on the same inputs
+    (tests/golden/levels.npz); the oracle and the host-side estimator of the package both."""
+    from bipp_b200 import parameter_estimator as pe
+
+    g = golden("levels.npz")
+    for k in range(len(g["case_n"])):
+        args = (int(g["case_n"][k]), float(g["case_sigma"][k]), str(g["case_func"][k]), float(g["case_lo"][k]),
+                float(g["case_hi"][k]), g["d_all"])
+        want = g[f"intervals_{k}"]
+        for got in (bb.infer_intervals(*args), pe.infer_intervals(*args)):
+            assert got.shape == want.shape
+            assert np.allclose(got, want, rtol=1e-12, atol=0)
+    k = 0
+    while f"centroid_{k}" in g.files:
+        for fn in (bb.centroid_to_intervals, pe.centroid_to_intervals):
+            assert np.array_equal(fn(g[f"centroid_{k}"], 0.0, 100.0), g[f"centroid_intervals_{k}"])
+        k += 1
+    d = g["filter_d"]
+    for name in g["filters"]:
+        name = str(name)
+        assert np.array_equal(bb.apply_filter(name, d), g[f"filter_{name}"])
+        assert np.array_equal(bb.level_eigenvalues(d, -0.5, 2.0, name), g[f"filter_{name}_bounded"])
+    with pytest.raises(ValueError):
+        bb.infer_intervals(2, 1.0, "log", -1.0, np.inf, g["d_all"])
+    with pytest.raises(ValueError):
+        pe.infer_intervals(2, 1.0, "log", -1.0, np.inf, g["d_all"])
