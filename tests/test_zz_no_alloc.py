@@ -83,3 +83,22 @@ def test_noalloc_rejects_sizes_above_the_maximum():
     rc = lib.bipp_eigh_gram_noalloc_s(0, None, np.float32(2.0), n, buf, n, buf, n, buf, buf, n, buf, buf, buf)
     assert rc == 3
     assert b"BIPP_NOALLOC_MAX_ANTENNA" in lib.bipp_last_error()
+
+
+def test_noalloc_nonfinite_entries():
+    """Non-finite visibilities as in the reference: a NaN antenna is dropped like a zero
+    antenna (info 0), a NaN in a kept entry of the lower triangle gives info 1 (the
+    reference's EigensolverError), and the next call is unaffected."""
+    from bipp_b200 import _lib
+    from conftest import nonfinite_cases
+
+    lib = _lib.load()
+    xyz, zero_ant, nan_ant, upper, bad = nonfinite_cases()
+    xyz = xyz.astype(np.float32).astype(np.float64)
+    vz, dz, nz, sz, iz = _noalloc(lib, 2.0, zero_ant.astype(np.complex64), xyz)
+    vn, dn, nn, sn, inn = _noalloc(lib, 2.0, nan_ant.astype(np.complex64), xyz)
+    assert iz == inn == 0 and nz == nn == zero_ant.shape[0] - 1 and sz == sn
+    assert np.abs(dn - dz).max() <= 1e-6 * np.abs(dz).max()
+    assert np.abs(_prod(vn, dn) - _prod(vz, dz)).max() <= 1e-5 * np.abs(_prod(vz, dz)).max()
+    assert _noalloc(lib, 2.0, bad["lower"].astype(np.complex64), xyz)[4] == 1
+    assert _noalloc(lib, 2.0, zero_ant.astype(np.complex64), xyz)[4] == 0
