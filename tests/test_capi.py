@@ -63,3 +63,29 @@ def test_error_message_plumbing():
     rc = lib.bipp_ctx_create(1, C.byref(h))  # CPU rejected
     assert rc == 3
     assert b"CPU" in lib.bipp_last_error()
+
+
+def test_null_handles_are_rejected_without_a_gpu():
+    """Every entry point checks its handle and pointers before any device work: null
+    handles give BIPP_INVALID_POINTER_ERROR (4) or BIPP_INVALID_HANDLE_ERROR (5) with a
+    message, and destroying a null handle succeeds (as deleting a null object)."""
+    from bipp_b200 import _lib
+
+    lib = _lib.load()
+    for name, argtypes in _lib.SIGNATURES.items():
+        if name in ("bipp_last_error", "bipp_kernel_launch_count"):
+            continue
+        args = []
+        for t in argtypes:
+            if t in (C.c_float, C.c_double):
+                args.append(t(2.0))
+            elif t in (C.c_int, C.c_size_t):
+                args.append(t(4))
+            else:
+                args.append(None)
+        rc = getattr(lib, name)(*args)
+        if name.endswith("_destroy"):
+            assert rc == 0, name
+        else:
+            assert rc in (4, 5), (name, rc)
+            assert b"null" in lib.bipp_last_error(), name
