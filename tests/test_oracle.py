@@ -201,3 +201,43 @@ def test_levels_and_filters_match_reference_python():
         bb.infer_intervals(2, 1.0, "log", -1.0, np.inf, g["d_all"])
     with pytest.raises(ValueError):
         pe.infer_intervals(2, 1.0, "log", -1.0, np.inf, g["d_all"])
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_restatement_vs_compiled_reference_beamformed(seed):
+    """Random beamformed problems (complex W, nBeam < nAntenna, flagged beams): eigh_gram,
+    eigh, the Gram matrix, virtual visibilities and the direct sum of the restatement
+    against the compiled reference, in FP64 (FP32 for the direct sum as well)."""
+    rng = np.random.default_rng(100 + seed)
+    n_ant, n_beam = 30, 18
+    w = (rng.standard_normal((n_ant, n_beam)) + 1j * rng.standard_normal((n_ant, n_beam))) / np.sqrt(n_ant)
+    xyz = rng.uniform(-40, 40, (n_ant, 3))
+    a = rng.standard_normal((n_beam, n_beam)) + 1j * rng.standard_normal((n_beam, n_beam))
+    s = a @ a.conj().T / n_beam
+    s[:, 2 + seed] = s[2 + seed, :] = 0
+    wl = 1.5 + 0.5 * seed
+    g_r, g_o = ref.gram_matrix(w, xyz, wl), bb.gram_matrix(w, xyz, wl)
+    assert np.abs(g_r - g_o).max() <= 1e-12 * np.abs(g_r).max()
+    v_r, d_r, nr_r, sc_r = ref.eigh_gram(wl, s, w, xyz)
+    v_o, d_o, nr_o, sc_o = bb.eigh_gram(wl, s, w, xyz)
+    assert nr_r == nr_o == n_beam - 1 and sc_r == sc_o
+    assert np.abs(d_r - d_o).max() <= 1e-10 * np.abs(d_r).max()
+    p_r, p_o = _pair_product(v_r, d_r), _pair_product(v_o, d_o)
+    assert np.abs(p_r - p_o).max() <= 1e-9 * np.abs(p_r).max()
+    v2_r, d2_r, nr2_r, _ = ref.eigh(wl, s, w)
+    v2_o, d2_o, nr2_o, _ = bb.eigh(wl, s, w)
+    assert nr2_r == nr2_o and np.abs(d2_r - d2_o).max() <= 1e-12 * np.abs(d2_r).max()
+    # one level: the upper half of the spectrum, as the reference's level mask
+    dl = d_r * (d_r >= np.median(d_r[:nr_r]))
+    vv_r, vv_o = ref.virtual_vis(sc_r, dl, v_r), bb.virtual_vis(sc_r, dl, v_r)
+    assert np.abs(vv_r - vv_o).max() <= 1e-12 * np.abs(vv_r).max()
+    # direct sum of those virtual visibilities onto random pixels
+    au = xyz @ rng.standard_normal((3, 3))
+    uvw = (au[:, None, :] - au[None, :, :]).transpose(1, 0, 2).reshape(-1, 3) * (2 * np.pi / wl)
+    pix = rng.uniform(-0.1, 0.1, (64, 3))
+    vals = vv_r.reshape(-1, order="F")
+    for dt, tol in ((np.float64, 1e-10), (np.float32, 1e-5)):
+        out_r = ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], pix[:, 0], pix[:, 1], pix[:, 2], dtype=dt)
+        out_o = bb.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], pix[:, 0], pix[:, 1], pix[:, 2])
+        assert np.abs(out_r - out_o).max() <= tol * np.abs(out_o).max()
