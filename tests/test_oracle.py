@@ -241,3 +241,35 @@ def test_restatement_vs_compiled_reference_beamformed(seed):
         out_r = ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], pix[:, 0], pix[:, 1], pix[:, 2], dtype=dt)
         out_o = bb.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], pix[:, 0], pix[:, 1], pix[:, 2])
         assert np.abs(out_r - out_o).max() <= tol * np.abs(out_o).max()
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+def test_lofar_image_oracle_vs_compiled_reference():
+    """The FP64 image oracle (bb.image_synthesis, the checker of the GPU image tests)
+    against the compiled reference's own pieces on the reference's LOFAR test input, in
+    the flow of tests/test_nufft_synthesis_lofar.cpp:86-233: eigh_gram<float> per sample,
+    the level mask with its index cut at n_eig_int (:112-124), virtual_vis<double>, the
+    exact sum nuft_sum<double> that the NUFFT approximates, 1/nSamples. The pixel grid of
+    the missing output file is replaced by a 24 x 24 grid of direction cosines."""
+    g = golden("lofar.npz")
+    wl, n_eig, intervals = float(g["wl"]), int(g["n_eig"]), g["intervals"]
+    l, m = np.meshgrid(np.linspace(-0.05, 0.05, 24), np.linspace(-0.04, 0.06, 24))
+    l, m = l.ravel(), m.ravel()
+    lmn = np.stack([l, m, np.sqrt(1 - l ** 2 - m ** 2)], 1)
+    steps, want = [], np.zeros((lmn.shape[0], len(intervals)))
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = ref.eigh_gram(wl, g["s"][k], g["w"][k], g["xyz"][k], dtype=np.float32)
+        assert nr == n_eig
+        steps.append(dict(uvw=g["uvw"][k], v=v, d=d, scale=sc, wl=wl))
+        uvw = g["uvw"][k].astype(np.float64) * (2 * np.pi / wl)
+        for lv, (lo, hi) in enumerate(intervals):
+            dl = d.astype(np.float64)
+            dl[:n_eig] *= (dl[:n_eig] >= lo) & (dl[:n_eig] <= hi)
+            dl[n_eig:] = 0
+            vv = ref.virtual_vis(sc, dl, v.astype(np.complex128)).reshape(-1, order="F")
+            want[:, lv] += ref.nuft_sum(1.0, vv, uvw[:, 0], uvw[:, 1], uvw[:, 2], lmn[:, 0], lmn[:, 1], lmn[:, 2])
+    want /= len(steps)
+    got = bb.image_synthesis(steps, intervals, lmn)
+    for lv in range(len(intervals)):
+        assert np.abs(want[:, lv]).max() > 0
+        assert np.abs(got[:, lv] - want[:, lv]).max() <= 1e-9 * np.abs(want[:, lv]).max()
