@@ -12,6 +12,8 @@ from .api import (  # noqa: F401
     NufftSynthesisOptions,
     Partition,
     Pipeline,
+    communicator,
+    config,
     default_context,
     domain_partition_grid,
     eigh,
@@ -22,6 +24,7 @@ from .api import (  # noqa: F401
     image_synthesis,
     kernel_launch_count,
     nuft_sum,
+    split_selection,
     virtual_vis,
 )
 

@@ -11,6 +11,7 @@ libbipp_b200.so; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from typing import Dict, Mapping, Optional, Sequence
 
@@ -26,21 +27,72 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
-class Context:
-    """Context(pu) with pu in {"AUTO", "GPU"} (include/bipp/context.hpp:25). "CPU" raises
-    InvalidParameterError: this library has no CPU processing unit."""
+class _CompileConfig:
+    """pybipp's ``config`` (python/pybipp.cpp:295-302): what the library was built with.
+    CUDA only; multi-rank runs use torch.distributed, not MPI."""
 
-    def __init__(self, pu: str = "AUTO", device: Optional[int] = None):
+    cuda, rocm, umpire, omp, mpi = True, False, False, False, False
+
+
+config = _CompileConfig()
+
+
+class communicator:
+    """pybipp's ``communicator`` (python/pybipp.cpp:304-308, include/bipp/communicator.hpp:22-89):
+    ``communicator.world()`` is the job of one process per GPU, read from the RANK and
+    WORLD_SIZE variables that torch.distributed launchers set (the reference reads
+    MPI_COMM_WORLD); ``communicator.local()`` is this process alone. The transport of
+    the image reduction is torch.distributed (NCCL on GPUs), which must be initialised
+    when size > 1."""
+
+    def __init__(self, rank: int = 0, size: int = 1):
+        if size < 1 or not 0 <= rank < size:
+            raise InvalidParameterError(3, f"invalid communicator rank {rank} of {size}")
+        self._rank, self._size = int(rank), int(size)
+
+    @staticmethod
+    def world() -> "communicator":
+        return communicator(int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
+
+    @staticmethod
+    def local() -> "communicator":
+        return communicator(0, 1)
+
+    @property
+    def rank(self) -> int:
+        return self._rank
+
+    @property
+    def size(self) -> int:
+        return self._size
+
+
+class Context:
+    """Context(pu) or Context(pu, comm) with pu in {"AUTO", "GPU"} (include/bipp/context.hpp:25-66,
+    python/pybipp.cpp:310-315). "CPU" raises InvalidParameterError: this library has no
+    CPU processing unit. With a communicator, the GPU is rank % device count as in the
+    reference (src/context_internal.cpp:59-66) unless `device` is given, and
+    image_synthesis splits the samples over the ranks."""
+
+    def __init__(self, pu: str = "AUTO", comm: Optional[communicator] = None, device: Optional[int] = None):
         self._lib = _lib.load()
+        self.communicator = comm if comm is not None else communicator.local()
         h = C.c_void_p()
         code = _PU[pu.upper()] if isinstance(pu, str) else int(pu)
+        if device is None and comm is not None and self.communicator.size > 1:
+            import torch
+
+            n = torch.cuda.device_count()
+            device = self.communicator.rank % n if n else None
         if device is None:
             check(self._lib.bipp_ctx_create(code, C.byref(h)))
         else:
             check(self._lib.bipp_ctx_create_on_device(code, int(device), C.byref(h)))
         self.handle = h
 
+    @property
     def processing_unit(self) -> str:
+        """"AUTO", "CPU" or "GPU" (a read-only property, as pybipp's)."""
         pu = C.c_int()
         check(self._lib.bipp_ctx_processing_unit(self.handle, C.byref(pu)))
         return {0: "AUTO", 1: "CPU", 2: "GPU"}[pu.value]
@@ -408,7 +460,36 @@ def image_synthesis(ctx: Context, opt: NufftSynthesisOptions, dataset, selection
     selection: {tag: {sample_id: scaled eigenvalues [nBeam]}}; image_prop: an object
     with pixel_lmn() -> [nPixel, 3] or the lmn array itself. Returns {tag: image}; if
     image_file_name is given the images are also saved there with numpy.savez (the
-    reference's HDF5 image file format is not implemented)."""
+    reference's HDF5 image file format is not implemented).
+
+    With a context of several ranks (Context(pu, communicator.world())) every rank
+    images its contiguous block of the sorted sample ids, the images are summed into
+    rank 0 over torch.distributed and normalised there by the total sample count
+    (src/image_synthesis.cpp:71-80, 140-163); rank 0 returns the images, the other
+    ranks an empty dict."""
+    tags = _check_tags(selection)
+    lmn = image_prop.pixel_lmn() if hasattr(image_prop, "pixel_lmn") else image_prop
+    comm = getattr(ctx, "communicator", None) or communicator.local()
+    if comm.size == 1:
+        images = _synthesize(ctx, opt, dataset, selection, tags, lmn, opt.normalize_image)
+    else:
+        local, n_total = split_selection(selection, dataset.num_samples(), comm.rank, comm.size)
+        if len(local[tags[0]]):
+            images = _synthesize(ctx, opt, dataset, local, tags, lmn, False)
+        else:
+            images = np.zeros((len(tags), np.asarray(lmn).shape[0]), dtype=np.float32)
+        images = _reduce_images_to_root(images)
+        if comm.rank != 0:
+            return {}
+        if opt.normalize_image:
+            images *= np.float32(1.0) / np.float32(n_total)
+    out = {tag: images[i] for i, tag in enumerate(tags)}
+    if image_file_name:
+        np.savez(image_file_name, **out)
+    return out
+
+
+def _check_tags(selection) -> list:
     for tag in selection:
         if "/" in tag:
             raise InvalidParameterError(3, "Selection name must not contain '/'")
@@ -419,6 +500,58 @@ def image_synthesis(ctx: Context, opt: NufftSynthesisOptions, dataset, selection
     tags = list(selection.keys())
     if not tags:
         raise InvalidParameterError(3, "Empty selection")
+    return tags
+
+
+def split_selection(selection, n_dataset: int, rank: int, size: int):
+    """The block of `rank` among `size` ranks: per tag, the samples at positions
+    [rank * ceil(n / size), ...) of the id-sorted selection, after the reference's checks
+    over the whole selection (src/image_synthesis.cpp:44-105: no duplicate ids, ids below
+    the dataset's sample count, the same ids for every image). Returns ({tag: {id: ev}},
+    total sample count)."""
+    from .distributed import sample_split
+
+    tags = list(selection.keys())
+    if not tags:
+        raise InvalidParameterError(3, "Empty selection")
+    order = {}
+    for tag in tags:
+        ids = sorted(int(i) for i in selection[tag].keys())
+        if not ids:
+            raise InvalidParameterError(3, "Empty selection")
+        if len(set(ids)) != len(ids):
+            raise InvalidParameterError(3, "Selection sample id duplicate")
+        if ids[-1] >= n_dataset:
+            raise InvalidParameterError(3, "Selection sample id exceeds number of dataset samples")
+        order[tag] = ids
+    n_total = len(order[tags[0]])
+    for tag in tags:
+        if order[tag] != order[tags[0]]:
+            raise InvalidParameterError(3, "Selection must contain the same sample ids for all images.")
+    begin, count = sample_split(n_total, rank, size)
+    keys = {tag: {int(k): k for k in selection[tag].keys()} for tag in tags}
+    local = {tag: {i: selection[tag][keys[tag][i]] for i in order[tag][begin:begin + count]} for tag in tags}
+    return local, n_total
+
+
+def _reduce_images_to_root(images: np.ndarray) -> np.ndarray:
+    """Sum the [nImages, nPixel] float images of all ranks into rank 0 (NCCL on GPUs)."""
+    import torch
+    import torch.distributed as dist
+
+    from .distributed import reduce_images
+
+    if not dist.is_initialized():
+        raise InvalidParameterError(3, "a communicator of size > 1 needs an initialised torch.distributed group")
+    t = torch.from_numpy(np.ascontiguousarray(images, dtype=np.float32))
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    reduce_images(t, dst=0)
+    return t.cpu().numpy()
+
+
+def _synthesize(ctx: Context, opt: NufftSynthesisOptions, dataset, selection, tags, lmn, normalize: bool) -> np.ndarray:
+    """One bipp_image_synthesis call over the given selection: images [nImages, nPixel]."""
     n_beam = dataset.num_beam()
     n_samples = len(selection[tags[0]])
     ids = np.zeros((len(tags), max(n_samples, 1)), dtype=np.uint64)
@@ -437,7 +570,6 @@ def image_synthesis(ctx: Context, opt: NufftSynthesisOptions, dataset, selection
             keep.append(ev)
             ids[ti, k] = int(sid)
             ptrs[ti * n_samples + k] = ev.ctypes.data
-    lmn = image_prop.pixel_lmn() if hasattr(image_prop, "pixel_lmn") else image_prop
     lmn = np.asfortranarray(lmn, dtype=np.float32)
     n_pixel = lmn.shape[0]
     images = np.zeros((len(tags), n_pixel), dtype=np.float32)
@@ -477,12 +609,10 @@ def image_synthesis(ctx: Context, opt: NufftSynthesisOptions, dataset, selection
                                 _lib.NUM_SAMPLES_FN(f_nb), _lib.EIG_VEC_FN(f_vec), _lib.EIG_VAL_FN(f_val),
                                 _lib.UVW_FN(f_uvw), _lib.SCALAR_FN(f_wl), _lib.SCALAR_FN(f_sc))
     o = opt._c()
+    o.normalizeImage = 1 if normalize else 0
     check(ctx._lib.bipp_image_synthesis(ctx.handle, C.byref(o), C.byref(cbs), len(tags), n_samples, _ptr(ids),
                                         C.cast(ptrs, C.c_void_p), n_pixel, _ptr(lmn), n_pixel, _ptr(images)))
-    out = {tag: images[i] for i, tag in enumerate(tags)}
-    if image_file_name:
-        np.savez(image_file_name, **out)
-    return out
+    return images
 
 
 # --- batched pipeline ---------------------------------------------------------------------

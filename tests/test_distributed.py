@@ -107,3 +107,124 @@ def test_gloo_bench_levels_are_rank0s():
         assert p.exitcode == 0
     for _, lv in got:
         assert np.array_equal(lv, np.array([[0.0, 1.0], [1.0, np.inf]]))
+
+
+def test_split_selection_rules():
+    """Checks over the whole selection before the split, then contiguous blocks of the
+    id-sorted samples (src/image_synthesis.cpp:44-105)."""
+    import bipp_b200 as bipp
+
+    ev = np.ones(3, np.float32)
+    sel = {"a": {7: ev, 2: 2 * ev, 5: 3 * ev, 0: 4 * ev, 9: 5 * ev}, "b": {0: ev, 2: ev, 5: ev, 7: ev, 9: ev}}
+    blocks = [bipp.split_selection(sel, 10, r, 2) for r in range(2)]
+    assert [sorted(b[0]["a"]) for b in blocks] == [[0, 2, 5], [7, 9]]
+    assert all(b[1] == 5 for b in blocks)
+    assert np.array_equal(blocks[1][0]["a"][7], ev) and np.array_equal(blocks[0][0]["a"][0], 4 * ev)
+    assert [sorted(b[0]["b"]) for b in blocks] == [[0, 2, 5], [7, 9]]
+    assert sorted(bipp.split_selection(sel, 10, 2, 3)[0]["a"]) == [9]
+    assert sorted(bipp.split_selection(sel, 10, 3, 4)[0]["a"]) == []
+    for bad, msg in (({"a": {0: ev, 12: ev}}, "exceeds"), ({"a": {0: ev, 1: ev}, "b": {0: ev, 2: ev}}, "same sample"),
+                     ({"a": {}}, "Empty")):
+        with pytest.raises(bipp.InvalidParameterError, match=msg):
+            bipp.split_selection(bad, 10, 0, 2)
+
+
+def test_communicator():
+    import bipp_b200 as bipp
+
+    assert (bipp.communicator.local().rank, bipp.communicator.local().size) == (0, 1)
+    os.environ["RANK"], os.environ["WORLD_SIZE"] = "1", "3"
+    try:
+        w = bipp.communicator.world()
+        assert (w.rank, w.size) == (1, 3)
+    finally:
+        del os.environ["RANK"], os.environ["WORLD_SIZE"]
+    with pytest.raises(bipp.InvalidParameterError):
+        bipp.communicator(2, 2)
+    assert bipp.config.cuda and not bipp.config.mpi
+
+
+def _oracle_synthesize(ctx, opt, dataset, selection, tags, lmn, normalize):
+    """The per-rank GPU synthesis call stood in by the FP64 oracle: VV = V diag(scale ev)
+    V^H per image and sample, exact sum over the baselines, 1/nSamples if normalize."""
+    from oracle import bluebild as bb
+
+    lmn = np.asarray(lmn, np.float64)
+    out = np.zeros((len(tags), lmn.shape[0]))
+    for ti, tag in enumerate(tags):
+        for sid, ev in selection[tag].items():
+            uvw = dataset.uvw(sid).astype(np.float64) * (2 * np.pi / dataset.wl(sid))
+            vv = bb.virtual_vis(dataset.scale(sid), np.asarray(ev, np.float64), dataset.eig_vec(sid))
+            out[ti] += bb.nuft_sum(1.0, vv.reshape(-1, order="F"), uvw[:, 0], uvw[:, 1], uvw[:, 2],
+                                   lmn[:, 0], lmn[:, 1], lmn[:, 2])
+        if normalize:
+            out[ti] /= len(selection[tag])
+    return out.astype(np.float32)
+
+
+def _dataset_case():
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+    from oracle import bluebild as bb
+
+    cfg = sim.config_c1(n_antenna=10, n_steps=5, image_size=6)
+    obs = sim.observation(cfg)
+    s, xyz = sim.visibilities(obs, list(range(5)))
+    ds = bipp.InMemoryDataset(10, 10)
+    sel = {"lvl0": {}, "lvl1": {}}
+    for k in range(5):
+        v, d, nr, sc = bb.eigh_gram(cfg.wl, s[k].numpy(), np.eye(10), xyz[k].numpy())
+        ds.write(k, cfg.wl, sc, v, d, sim.baseline_uvw(obs, xyz[k].numpy()))
+        sel["lvl0"][k] = (d * (d > 0)).astype(np.float32)
+        sel["lvl1"][k] = (d * (d <= 0)).astype(np.float32)
+    return ds, sel, obs.lmn
+
+
+def _synthesis_worker(rank, size, port, out_q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size)
+    import types
+
+    import bipp_b200 as bipp
+    from bipp_b200 import api
+
+    api._synthesize = _oracle_synthesize
+    ds, sel, lmn = _dataset_case()
+    ctx = types.SimpleNamespace(communicator=bipp.communicator(rank, size))
+    out = bipp.image_synthesis(ctx, bipp.NufftSynthesisOptions(), ds, sel, lmn)
+    out_q.put((rank, out))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gloo_image_synthesis_over_two_ranks():
+    """image_synthesis with a context of two ranks: sample blocks per rank, one SUM
+    reduction into rank 0, normalisation by the total there; equal to one process over
+    all samples (the per-rank synthesis is the oracle, so this tests the host logic)."""
+    import types
+
+    import bipp_b200 as bipp
+    from bipp_b200 import api
+
+    ds, sel, lmn = _dataset_case()
+    saved = api._synthesize
+    api._synthesize = _oracle_synthesize
+    try:
+        full = bipp.image_synthesis(types.SimpleNamespace(communicator=bipp.communicator.local()),
+                                    bipp.NufftSynthesisOptions(), ds, sel, lmn)
+    finally:
+        api._synthesize = saved
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_synthesis_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert got[1] == {}
+    for tag in ("lvl0", "lvl1"):
+        assert np.abs(got[0][tag] - full[tag]).max() <= 1e-5 * np.abs(full[tag]).max()
