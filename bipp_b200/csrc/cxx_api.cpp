@@ -51,6 +51,9 @@ auto Communicator::local() -> Communicator { return Communicator(); }
 class ContextInternal {
 public:
   ContextInternal(BippProcessingUnit pu, std::size_t rank) {
+    // the processing unit is checked before the devices, as by the C ABI
+    if (pu == BIPP_PU_CPU)
+      throw InvalidParameterError("this library has no CPU processing unit; use BIPP_PU_GPU or BIPP_PU_AUTO");
     // device = rank % device count (src/context_internal.cpp:59-66)
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {

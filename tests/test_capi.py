@@ -89,3 +89,22 @@ def test_null_handles_are_rejected_without_a_gpu():
         else:
             assert rc in (4, 5), (name, rc)
             assert b"null" in lib.bipp_last_error(), name
+
+
+def test_cxx_shell_host_checks(tmp_path):
+    """The bipp C++ API shell (include/bipp/*.hpp) compiles and links against the
+    library with g++, and its host-side behaviour holds without a GPU: exception types
+    and codes, the CPU processing unit rejected, GPUSupportError for a GPU context
+    without a device, Communicator::world() (tests/cxx/shell_cpu_check.cpp)."""
+    import subprocess
+
+    import torch
+
+    exe = tmp_path / "shell_cpu_check"
+    libdir = os.path.join(ROOT, "bipp_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", os.path.join(ROOT, "tests", "cxx", "shell_cpu_check.cpp"),
+                    "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include", "-L" + libdir,
+                    "-lbipp_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    args = [str(exe)] + ([] if torch.cuda.is_available() else ["no-gpu"])
+    r = subprocess.run(args, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
