@@ -34,10 +34,10 @@ def _check_reduced(s_red, g=None):
 def flag_nonzero_gram(s, eps):
     """Rows/cols kept by eigh_gram: |s_ij|^2 > eps in the lower triangle, and
     nVis = count of such entries (diagonal once, off-diagonal twice).
-    src/eigensolver.cpp:148-166."""
+    src/eigensolver.cpp:148-166. |s|^2 is std::norm's re*re + im*im in the precision
+    of s (pass s in the working precision for the reference's exact threshold)."""
     s = np.asarray(s)
-    n = s.shape[0]
-    low = np.tril(np.abs(s) ** 2 > eps)
+    low = np.tril(s.real * s.real + s.imag * s.imag > s.real.dtype.type(eps))
     flags = low.any(axis=0) | low.any(axis=1)
     diag = np.diag(low).sum()
     nvis = int(diag + 2 * (low.sum() - diag))
@@ -47,7 +47,8 @@ def flag_nonzero_gram(s, eps):
 def flag_nonzero_std(s, eps):
     """Flag test of bipp::eigh: |Re| >= eps or |Im| >= eps (src/eigensolver.cpp:57-76)."""
     s = np.asarray(s)
-    low = np.tril((np.abs(s.real) >= eps) | (np.abs(s.imag) >= eps))
+    e = s.real.dtype.type(eps)
+    low = np.tril((np.abs(s.real) >= e) | (np.abs(s.imag) >= e))
     flags = low.any(axis=0) | low.any(axis=1)
     diag = np.diag(low).sum()
     nvis = int(diag + 2 * (low.sum() - diag))
@@ -77,10 +78,10 @@ def eigh_gram(wl, s, w, xyz, dtype=np.float64):
     rt = np.dtype(dtype)
     ct = np.complex64 if rt == np.float32 else np.complex128
     eps = float(np.finfo(rt).eps)
+    idx, nvis = flag_nonzero_gram(np.asarray(s, dtype=ct), eps)
     s = np.asarray(s, dtype=np.complex128)
     w = np.asarray(w, dtype=np.complex128)
     n_ant, n_beam = w.shape
-    idx, nvis = flag_nonzero_gram(s, eps)
     nred = len(idx)
     d = np.zeros(n_beam, dtype=rt)
     v = np.zeros((n_ant, n_beam), dtype=ct)
@@ -105,10 +106,10 @@ def eigh(wl, s, w, dtype=np.float64):
     rt = np.dtype(dtype)
     ct = np.complex64 if rt == np.float32 else np.complex128
     eps = float(np.finfo(rt).eps)
+    idx, nvis = flag_nonzero_std(np.asarray(s, dtype=ct), eps)
     s = np.asarray(s, dtype=np.complex128)
     w = np.asarray(w, dtype=np.complex128)
     n_ant, n_beam = w.shape
-    idx, nvis = flag_nonzero_std(s, eps)
     nred = len(idx)
     d = np.zeros(n_beam, dtype=rt)
     v = np.zeros((n_ant, n_beam), dtype=ct)

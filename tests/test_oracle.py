@@ -273,3 +273,33 @@ def test_lofar_image_oracle_vs_compiled_reference():
     for lv in range(len(intervals)):
         assert np.abs(want[:, lv]).max() > 0
         assert np.abs(got[:, lv] - want[:, lv]).max() <= 1e-9 * np.abs(want[:, lv]).max()
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_flag_threshold_matches_compiled_reference(dtype):
+    """Antennas whose only entries sit at the flag threshold (|s|^2 vs eps for eigh_gram,
+    |Re|, |Im| vs eps for eigh; eps of the working precision, src/eigensolver.cpp:57-76,
+    148-166): kept or dropped exactly as by the reference, with the same 1/nVis."""
+    rng = np.random.default_rng(3)
+    n = 16
+    eps = float(np.finfo(dtype).eps)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    s = a @ a.conj().T / n
+    xyz = rng.uniform(-30, 30, (n, 3))
+    factors = (0.5, 0.999, 1.0, 1.001, 2.0)
+    sg, se = s.copy(), s.copy()
+    for k, f in zip(range(3, 3 + len(factors)), factors):
+        sg[k, :] = sg[:, k] = 0
+        sg[k, 0] = np.sqrt(f * eps)          # |s|^2 = f eps (up to rounding in the precision)
+        sg[0, k] = np.conj(sg[k, 0])
+        se[k, :] = se[:, k] = 0
+        se[k, 1] = complex(0.0, f * eps)     # |Im| = f eps
+        se[1, k] = np.conj(se[k, 1])
+    r = ref.eigh_gram(2.0, sg, np.eye(n), xyz, dtype=dtype)
+    o = bb.eigh_gram(2.0, sg, np.eye(n), xyz, dtype=dtype)
+    assert r[2] == o[2] and abs(r[3] - o[3]) <= 1e-6 * r[3]
+    r = ref.eigh(2.0, se, np.eye(n), dtype=dtype)
+    o = bb.eigh(2.0, se, np.eye(n), dtype=dtype)
+    assert r[2] == o[2] and abs(r[3] - o[3]) <= 1e-6 * r[3]
+    assert n - len(factors) < o[2] < n
