@@ -85,6 +85,10 @@ template <typename C> __host__ __device__ __forceinline__ void cfma_cj(C& acc, C
   acc.y = fma(a.x, b.y, fma(-a.y, b.x, acc.y));
 }
 template <typename C> __host__ __device__ __forceinline__ auto cabs2(C a) { return a.x * a.x + a.y * a.y; }
+// |s|^2 of the flag test as the reference's std::norm: both products and the sum rounded
+// separately (no fused multiply-add), so that keep/drop matches it bit for bit
+__device__ __forceinline__ float flag_norm(float2 a) { return __fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)); }
+__device__ __forceinline__ double flag_norm(double2 a) { return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y)); }
 
 __device__ __forceinline__ float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
 __device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }

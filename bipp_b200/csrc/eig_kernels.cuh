@@ -54,7 +54,7 @@ prep_kernel(int nBeam, const typename Cplx<T>::type* __restrict__ S, long long s
       for (int row = col + lane; row < nBeam; row += 32) {
         C v = Sb[row + (long long)col * lds];
         if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
-        bool nz = (mode == 0) ? (cabs2(v) > eps) : (fabs(v.x) >= eps || fabs(v.y) >= eps);
+        bool nz = (mode == 0) ? (flag_norm(v) > eps) : (fabs(v.x) >= eps || fabs(v.y) >= eps);
         if (nz) {
           flags[row] = 1;
           flags[col] = 1;
