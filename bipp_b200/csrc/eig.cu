@@ -423,6 +423,15 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   require(!gram || (xyz && ldxyz >= nAntenna), "invalid xyz");
   require(!v || ldv >= nAntenna, "invalid ldv");
   require(nBeam <= 4096, "nBeam above the supported maximum of 4096");
+  if (sizeof(T) == 8) {
+    // complex<double>: the tridiagonalisation keeps 5 rows of nBeam elements and the
+    // back-transform 5 nBeam + kBtThreads elements in shared memory
+    const size_t cb = sizeof(C), smem = ctx->maxSmemOptin;
+    const size_t lim = std::min(smem / (5 * cb), (smem / cb - kBtThreads) / 5);
+    if (nBeam > lim)
+      throw Error(BIPP_INVALID_PARAMETER_ERROR,
+                  "nBeam above the FP64 maximum of " + std::to_string(lim) + " set by this device's shared memory");
+  }
   const CS* sp = static_cast<const CS*>(s);
   const CS* wp = static_cast<const CS*>(w);
   // identity beamforming?

@@ -71,7 +71,9 @@ BIPP_B200_EXPORT BippError bipp_ctx_stream(bipp_ctx_t ctx, void** stream);
  * EigensolverError): BIPP_EIGENSOLVER_ERROR when G is not positive definite or when a
  * NaN/Inf entry of S's lower triangle lies in a kept row and column. A NaN/Inf entry fails
  * the flag test like a zero, so an antenna whose entries are all NaN is dropped, and
- * entries above the diagonal are never read. */
+ * entries above the diagonal are never read. nBeam is at most 4096 for the _s entry
+ * points and, for _d, at most the FP64 limit set by the device's shared memory per block
+ * (2854 on B200); larger problems fail with BIPP_INVALID_PARAMETER_ERROR. */
 BIPP_B200_EXPORT BippError bipp_eigh_gram_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam,
                                             const void* s, size_t lds, const void* w, size_t ldw,
                                             const float* xyz, size_t ldxyz, float* d, void* v, size_t ldv,
