@@ -245,7 +245,7 @@ def test_restatement_vs_compiled_reference_beamformed(seed):
 
 @pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
 def test_lofar_image_oracle_vs_compiled_reference():
-    """The FP64 image oracle (bb.image_synthesis, the checker of the GPU image tests)
+    """The FP64 image oracle (bb.image_synthesis, which the GPU image tests compare against)
     against the compiled reference's own pieces on the reference's LOFAR test input, in
     the flow of tests/test_nufft_synthesis_lofar.cpp:86-233: eigh_gram<float> per sample,
     the level mask with its index cut at n_eig_int (:112-124), virtual_vis<double>, the
