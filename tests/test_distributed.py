@@ -228,3 +228,29 @@ def test_gloo_image_synthesis_over_two_ranks():
     assert got[1] == {}
     for tag in ("lvl0", "lvl1"):
         assert np.abs(got[0][tag] - full[tag]).max() <= 1e-5 * np.abs(full[tag]).max()
+
+
+def test_split_selection_property():
+    """For any set of sample ids and rank count: the ranks' blocks partition the sorted
+    ids in rank order, no block is longer than ceil(n / size), and every image's block
+    carries its own eigenvalues."""
+    from hypothesis import given, settings, strategies as st
+
+    import bipp_b200 as bipp
+
+    @settings(max_examples=200, deadline=None, database=None)
+    @given(st.sets(st.integers(0, 999), min_size=1, max_size=60), st.integers(1, 9))
+    def check(ids, size):
+        sel = {"a": {i: np.full(2, i, np.float32) for i in ids}, "b": {i: np.full(2, -i, np.float32) for i in ids}}
+        got = []
+        for r in range(size):
+            local, n = bipp.split_selection(sel, 1000, r, size)
+            assert n == len(ids)
+            assert list(local["a"]) == list(local["b"])
+            assert len(local["a"]) <= -(-len(ids) // size)
+            for i in local["a"]:
+                assert local["a"][i][0] == i and local["b"][i][0] == -i
+            got += list(local["a"])
+        assert got == sorted(ids)
+
+    check()
