@@ -16,6 +16,9 @@ Outputs (compressed .npz, a few hundred KB in total):
                  seeded small problem.
   partition.npz  reference DomainPartition::grid (src/host/domain_partition.hpp:35-101) on the
                  seeded distributions of tests/test_domain_partition.cpp:102-131 (numpy RNG).
+  frame.npz      the reference's own python/bipp/frame.py (uvw_basis, make_grids,
+                 reshape_uvw: the UVW frame, the pixel grid and the baseline order) on a
+                 few field centres, grid sizes and random UVW.
   levels.npz     the reference's own Python energy-level estimator and eigenvalue filters
                  (python/bipp/parameter_estimator.py:18-105, python/bipp/filter.py:7-51)
                  on seeded eigenvalue spectra, loaded from the reference's source files.
@@ -210,6 +213,53 @@ def levels(refdir: str):
     np.savez_compressed(os.path.join(HERE, "levels.npz"), **out)
 
 
+def frame(refdir: str):
+    """frame.py loaded from the reference's source with astropy.coordinates stubbed: the
+    functions only read a field centre's lon/lat (radians) and unit vector."""
+    import importlib.util
+    import types
+
+    saved = {k: sys.modules.get(k) for k in ("astropy", "astropy.coordinates")}
+    astropy = types.ModuleType("astropy")
+    coords = types.ModuleType("astropy.coordinates")
+    coords.SkyCoord = object
+    astropy.coordinates = coords
+    sys.modules.update({"astropy": astropy, "astropy.coordinates": coords})
+    try:
+        spec = importlib.util.spec_from_file_location("bipp_reference_frame",
+                                                      os.path.join(refdir, "python", "bipp", "frame.py"))
+        fr = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(fr)
+    finally:
+        for k, m in saved.items():
+            if m is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = m
+
+    def centre(lon, lat):
+        xyz = np.array([np.cos(lat) * np.cos(lon), np.cos(lat) * np.sin(lon), np.sin(lat)])
+        return types.SimpleNamespace(data=types.SimpleNamespace(lon=types.SimpleNamespace(rad=lon),
+                                                                lat=types.SimpleNamespace(rad=lat)),
+                                     cartesian=types.SimpleNamespace(xyz=types.SimpleNamespace(value=xyz)))
+
+    out = {}
+    cases = [(0.0, -0.5235987755982988), (1.2, 0.3), (4.0, -1.1)]
+    out["centres"] = np.array(cases)
+    for k, (lon, lat) in enumerate(cases):
+        out[f"basis_{k}"] = fr.uvw_basis(centre(lon, lat))
+    grids = [(8, 0.2), (33, 0.28), (64, 0.05)]
+    out["grids"] = np.array(grids)
+    for k, (n, fov) in enumerate(grids):
+        lmn, _ = fr.make_grids(int(n), fov, centre(*cases[0]))
+        out[f"lmn_{k}"] = lmn
+    rng = np.random.default_rng(9)
+    au = rng.standard_normal((7, 3)) * 100.0     # antenna UVW coordinates
+    out["antenna_uvw"] = au
+    out["uvw_reshaped"] = fr.reshape_uvw(au[:, None, :] - au[None, :, :])   # UVW[i, j] = U_i - U_j
+    np.savez_compressed(os.path.join(HERE, "frame.npz"), **out)
+
+
 if __name__ == "__main__":
     refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     lofar(refdir)
@@ -217,6 +267,7 @@ if __name__ == "__main__":
     nuft()
     partition()
     levels(refdir)
+    frame(refdir)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -53,3 +53,23 @@ def test_bench_defaults_per_workload(monkeypatch):
     a = bench.parse()
     assert (a.time_steps, a.antennas, a.image, a.chunk_steps) == (128, 1024, 2048, 592)
     assert bench.metric_of(a) == bench.METRIC_C5
+
+
+def test_geometry_matches_reference_frame():
+    """The workload generator's UVW frame, pixel grid and baseline order against the
+    reference's own python/bipp/frame.py (uvw_basis, make_grids, reshape_uvw) run on the
+    same inputs (tests/golden/frame.npz)."""
+    import types
+
+    from conftest import golden
+
+    g = golden("frame.npz")
+    for k, (lon, lat) in enumerate(g["centres"]):
+        assert np.allclose(sim.uvw_basis(lon, lat), g[f"basis_{k}"], rtol=0, atol=1e-15)
+    for k, (n, fov) in enumerate(g["grids"]):
+        assert np.allclose(sim.make_lmn_grid(int(n), fov), g[f"lmn_{k}"].T, rtol=0, atol=1e-15)
+    # baseline k = i + j N <-> U_i - U_j, as reshape_uvw orders it (float32 output)
+    obs = types.SimpleNamespace(basis=np.eye(3))
+    got = sim.baseline_uvw(obs, g["antenna_uvw"])
+    assert got.dtype == np.float32
+    assert np.allclose(got, g["uvw_reshaped"], rtol=1e-6, atol=1e-4)
