@@ -431,6 +431,8 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
     require(cfg->intervals && cfg->pixelN && cfg->uvwBasis, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(cfg->gridA >= 2 && cfg->gridB >= 2, "pixel lattice must be at least 2 x 2");
     require(cfg->filter >= 0 && cfg->filter <= 4, "unknown filter");
+    for (size_t l = 0; l < cfg->nLevels; ++l)
+      require(cfg->intervals[2 * l] <= cfg->intervals[2 * l + 1], "energy-level interval with lo > hi or NaN bounds");
     auto p = std::make_unique<bipp_pipeline_s>();
     p->ctx = ctx;
     p->nAnt = cfg->nAntenna;

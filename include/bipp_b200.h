@@ -235,7 +235,8 @@ BIPP_B200_EXPORT BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft
 typedef struct {
   size_t nAntenna;        /* antennas per step (W = I) */
   size_t nLevels;         /* energy levels, 1 to 8 */
-  const double* intervals;/* [nLevels][2] (lo, hi) eigenvalue intervals */
+  const double* intervals;/* [nLevels][2] (lo, hi) eigenvalue intervals, lo <= hi (else
+                             BIPP_INVALID_PARAMETER_ERROR); +-inf allowed */
   int filter;             /* 0 lsq, 1 std, 2 sqrt, 3 inv, 4 inv_sqrt (python/bipp/filter.py) */
   double tolerance;       /* NUFFT tolerance */
   size_t gridA, gridB;    /* pixel lattice extents (a slow, b fast); nPixel = gridA * gridB */
