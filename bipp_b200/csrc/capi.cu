@@ -65,13 +65,15 @@ __global__ void part_group_kernel(long long n, const T* __restrict__ x, const T*
                                   unsigned long long dy, unsigned long long dz, int degx, int degy, int degz,
                                   unsigned long long* __restrict__ group) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    // same arithmetic as the reference: (size_t)(inv * (c - min)), clamped to dims - 1
+    // same arithmetic as the reference: (size_t)(inv * (c - min)), clamped to dims - 1; on
+    // an axis without extent the reference computes inf * 0 = NaN, whose conversion to
+    // size_t on x86-64 lands in the last cell, so those points go to the last cell
     const T cx = fmul_rn_t(invx, (T)(x[i] - minx));
     const T cy = fmul_rn_t(invy, (T)(y[i] - miny));
     const T cz = fmul_rn_t(invz, (T)(z[i] - minz));
-    unsigned long long gx = degx ? 0ull : (unsigned long long)cx;
-    unsigned long long gy = degy ? 0ull : (unsigned long long)cy;
-    unsigned long long gz = degz ? 0ull : (unsigned long long)cz;
+    unsigned long long gx = degx ? dx - 1 : (unsigned long long)cx;
+    unsigned long long gy = degy ? dy - 1 : (unsigned long long)cy;
+    unsigned long long gz = degz ? dz - 1 : (unsigned long long)cz;
     gx = gx < dx - 1 ? gx : dx - 1;
     gy = gy < dy - 1 ? gy : dy - 1;
     gz = gz < dz - 1 ? gz : dz - 1;

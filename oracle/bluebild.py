@@ -234,13 +234,16 @@ def partition_grid(dims, x, y, z, dtype=np.float64):
     ng = int(np.prod(dims))
     if ng <= 1:
         return np.arange(n, dtype=np.uint64), np.array([0], np.uint64), np.array([n], np.uint64)
+    if n == 0:
+        return np.zeros(0, np.uint64), np.zeros(ng, np.uint64), np.zeros(ng, np.uint64)
     gidx = np.zeros(n, dtype=np.int64)
     for dim in (2, 1, 0):
         c = coords[dim]
         cmin, cmax = c.min(), c.max()
         if not cmax > cmin:
-            # degenerate extent: every point in the first cell (the reference divides by zero)
-            gidx = gidx * dims[dim]
+            # degenerate extent: the reference's spacing is dims / 0 = inf, inf * 0 = NaN,
+            # and its NaN -> size_t conversion (x86-64) clamps to the last cell
+            gidx = gidx * dims[dim] + (dims[dim] - 1)
             continue
         inv = rt.type(dims[dim]) / rt.type(cmax - cmin)
         cell = (inv * (c - cmin)).astype(rt)

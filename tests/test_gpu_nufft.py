@@ -43,7 +43,7 @@ def test_nuft_sum_f32_accumulates(ctx):
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-@pytest.mark.parametrize("n", [100, 4000])
+@pytest.mark.parametrize("n", [1, 100, 4000])
 def test_partition_matches_reference(ctx, n, prec):
     import bipp_b200 as bipp
 

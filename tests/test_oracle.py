@@ -68,7 +68,7 @@ def test_nuft_sum_oracle():
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-@pytest.mark.parametrize("n", [100, 4000])
+@pytest.mark.parametrize("n", [1, 100, 4000])
 def test_partition_oracle(n, prec):
     g = golden("partition.npz")
     dt = np.float32 if prec == "f32" else np.float64
@@ -303,3 +303,24 @@ def test_flag_threshold_matches_compiled_reference(dtype):
     o = bb.eigh(2.0, se, np.eye(n), dtype=dtype)
     assert r[2] == o[2] and abs(r[3] - o[3]) <= 1e-6 * r[3]
     assert n - len(factors) < o[2] < n
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+def test_partition_matches_compiled_reference_property():
+    """DomainPartition::grid of the restatement equals the compiled reference bit for bit
+    on random grids, sizes and value ranges (degenerate axes and duplicates included)."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=120, deadline=None, database=None)
+    @given(st.integers(0, 300), st.lists(st.integers(1, 5), min_size=3, max_size=3), st.integers(0, 2 ** 31),
+           st.sampled_from([np.float32, np.float64]), st.booleans())
+    def check(n, dims, seed, dt, degenerate):
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(-5, 10, n).astype(dt)
+        y = (np.full(n, 3.0) if degenerate else rng.uniform(2, 20, n)).astype(dt)
+        z = np.round(rng.uniform(100, 5000, n), 0).astype(dt)      # repeated values
+        pm_r, gb_r, gs_r = ref.partition_grid(dims, x, y, z, dtype=dt)
+        pm_o, gb_o, gs_o = bb.partition_grid(dims, x, y, z, dtype=dt)
+        assert np.array_equal(pm_r, pm_o) and np.array_equal(gb_r, gb_o) and np.array_equal(gs_r, gs_o)
+
+    check()
