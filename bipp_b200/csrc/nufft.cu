@@ -807,6 +807,7 @@ BippError bipp_nuft_sum_multi_device(bipp_ctx_t ctx, double alpha, size_t nIn, s
   return guard([&] {
     require(ctx && values && u && v && w && x && y && z && out, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(nch >= 1 && ldIn >= nIn && ldOut >= nOut, "invalid sizes");
+    if (!nOut) return;
     const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
     for (size_t c0 = 0; c0 < nch; c0 += 4) {
       const int n = (int)std::min<size_t>(4, nch - c0);
