@@ -518,6 +518,16 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   if (status & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
   if (status & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
   if (status & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
+  if (nred == 0) {
+    // every row and column flagged: the reference zeroes d and v, then hands LAPACK a
+    // 0 x 0 problem with leading dimension 0, which LAPACK rejects (info < 0), and throws
+    // EigensolverError (src/eigensolver.cpp:172-173, src/host/lapack_api.hpp:133)
+    for (size_t c = 0; c < nBeam; ++c) d[c] = T(0);
+    if (v)
+      for (size_t c = 0; c < nBeam; ++c)
+        for (size_t r = 0; r < nAntenna; ++r) static_cast<CS*>(v)[r + c * ldv] = CS(0, 0);
+    throw Error(BIPP_EIGENSOLVER_ERROR, "every row and column of S is flagged (empty eigenproblem)");
+  }
   for (size_t c = 0; c < nBeam; ++c) d[c] = (c < (size_t)nred) ? (T)lam[c] : T(0);
   if (v) {
     B2_CUDA(cudaMemcpy2DAsync(v, ldv * sizeof(C), dOut.get(), nAntenna * sizeof(C), nAntenna * sizeof(C), nBeam,
@@ -596,6 +606,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     if (stat[b] & kStatusTensorTimeout) throw Error(BIPP_GPU_ERROR, "tensor-core MMA wait timed out");
     if (stat[b] & kStatusCholeskyNotPD) throw Error(BIPP_EIGENSOLVER_ERROR, "Gram matrix is not positive definite");
     if (stat[b] & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
+    if (nredh[b] == 0) throw Error(BIPP_EIGENSOLVER_ERROR, "every row and column of S is flagged (empty eigenproblem)");
     nBeamReduced[b] = (size_t)nredh[b];
     scale[b] = nvish[b] ? 1.0f / (float)nvish[b] : 0.0f;
   }

@@ -81,8 +81,8 @@ Work carve(char* base, int N) {
 }
 
 // outputs: d (float, zero padded), v = eigenvectors scattered to the kept antenna rows,
-// nReduced, scale = 1/nVis, info (1 when the Cholesky factorisation of G failed or a
-// kept entry of S is not finite)
+// nReduced, scale = 1/nVis, info (1 when the Cholesky factorisation of G failed, a kept
+// entry of S is not finite, or every row and column is flagged)
 __global__ void noalloc_outputs_kernel(int n, const int* __restrict__ nredP, const long long* __restrict__ nvisP,
                                        const int* __restrict__ status, const double* __restrict__ lam,
                                        const float2* __restrict__ X, int Nmax, const int* __restrict__ idx,
@@ -109,7 +109,7 @@ __global__ void noalloc_outputs_kernel(int n, const int* __restrict__ nredP, con
     *nReduced = nred;
     const long long nv = *nvisP;
     *scale = nv ? 1.0f / (float)nv : 0.0f;
-    *info = (*status & (kStatusCholeskyNotPD | kStatusNonFinite)) ? 1 : 0;
+    *info = ((*status & (kStatusCholeskyNotPD | kStatusNonFinite)) || nred == 0) ? 1 : 0;
   }
 }
 

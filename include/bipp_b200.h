@@ -71,7 +71,9 @@ BIPP_B200_EXPORT BippError bipp_ctx_stream(bipp_ctx_t ctx, void** stream);
  * EigensolverError): BIPP_EIGENSOLVER_ERROR when G is not positive definite or when a
  * NaN/Inf entry of S's lower triangle lies in a kept row and column. A NaN/Inf entry fails
  * the flag test like a zero, so an antenna whose entries are all NaN is dropped, and
- * entries above the diagonal are never read. nBeam is at most 4096 for the _s entry
+ * entries above the diagonal are never read. A step whose rows and columns are all
+ * flagged fails with BIPP_EIGENSOLVER_ERROR after zeroing d and v (the reference's LAPACK
+ * call rejects the empty problem's leading dimension 0). nBeam is at most 4096 for the _s entry
  * points and, for _d, at most the FP64 limit set by the device's shared memory per block
  * (2854 on B200); larger problems fail with BIPP_INVALID_PARAMETER_ERROR. */
 BIPP_B200_EXPORT BippError bipp_eigh_gram_s(bipp_ctx_t ctx, float wl, size_t nAntenna, size_t nBeam,
@@ -118,7 +120,8 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatc
  * s (nAntenna x nAntenna complex float, lower triangle used, lds), xyz (nAntenna x 3
  * double, ldxyz); outputs d[nAntenna] (ascending, zero padded), v (nAntenna x nAntenna,
  * ldv, zero padded), *nBeamReduced, *scale (= 1/nVis) and *info (1 if the Cholesky
- * factorisation of G failed or a kept entry of S is not finite, else 0). The call is asynchronous on `stream` (a
+ * factorisation of G failed, a kept entry of S is not finite or every row and column is
+ * flagged, else 0). The call is asynchronous on `stream` (a
  * cudaStream_t). Every call on a device shares the array, so calls that overlap on the
  * GPU race; serialise them (one stream, or events). The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress) and should come before any stream

@@ -79,6 +79,8 @@ def eigh_gram(wl, s, w, xyz, dtype=np.float64):
     ct = np.complex64 if rt == np.float32 else np.complex128
     eps = float(np.finfo(rt).eps)
     idx, nvis = flag_nonzero_gram(np.asarray(s, dtype=ct), eps)
+    if len(idx) == 0:  # LAPACK rejects the 0 x 0 problem's leading dimension 0
+        raise EigensolverError("every row and column of S is flagged")
     s = np.asarray(s, dtype=np.complex128)
     w = np.asarray(w, dtype=np.complex128)
     n_ant, n_beam = w.shape
@@ -107,6 +109,8 @@ def eigh(wl, s, w, dtype=np.float64):
     ct = np.complex64 if rt == np.float32 else np.complex128
     eps = float(np.finfo(rt).eps)
     idx, nvis = flag_nonzero_std(np.asarray(s, dtype=ct), eps)
+    if len(idx) == 0:  # LAPACK rejects the 0 x 0 problem's leading dimension 0
+        raise EigensolverError("every row and column of S is flagged")
     s = np.asarray(s, dtype=np.complex128)
     w = np.asarray(w, dtype=np.complex128)
     n_ant, n_beam = w.shape

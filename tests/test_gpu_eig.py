@@ -135,11 +135,17 @@ def test_batched_eigh_gram_matches_single(ctx):
 
 
 def test_all_flagged_step(ctx):
+    """Every row and column flagged: the reference hands LAPACK a 0 x 0 problem with
+    leading dimension 0, which LAPACK rejects, and throws EigensolverError
+    (src/eigensolver.cpp:172-223, src/host/lapack_api.hpp:133); so do these entry points."""
     import bipp_b200 as bipp
 
     n = 16
-    v, d, nr, sc = bipp.eigh_gram_full(2.0, np.zeros((n, n), np.complex128), np.eye(n), np.random.rand(n, 3), ctx=ctx)
-    assert nr == 0 and sc == 0.0 and np.all(d == 0) and np.all(v == 0)
+    with pytest.raises(bipp.EigensolverError):
+        bipp.eigh_gram_full(2.0, np.zeros((n, n), np.complex128), np.eye(n), np.random.rand(n, 3), ctx=ctx)
+    # the context is still usable
+    xyz, zero_ant, _, _, _ = nonfinite_cases()
+    assert bipp.eigh_gram_full(2.0, zero_ant, np.eye(24), xyz, ctx=ctx)[2] == 23
 
 
 def test_invalid_gram_raises_eigensolver_error(ctx):

@@ -324,3 +324,23 @@ def test_partition_matches_compiled_reference_property():
         assert np.array_equal(pm_r, pm_o) and np.array_equal(gb_r, gb_o) and np.array_equal(gs_r, gs_o)
 
     check()
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_all_flagged_step_raises_like_compiled_reference(dtype):
+    """Every row and column flagged: the reference's LAPACK call gets a 0 x 0 problem with
+    leading dimension 0 and rejects it (EigensolverError); one non-zero pair keeps two."""
+    n = 6
+    xyz = np.random.default_rng(1).uniform(0, 10, (n, 3))
+    for fn_r, fn_o in ((lambda s: ref.eigh_gram(2.0, s, np.eye(n), xyz, dtype=dtype),
+                        lambda s: bb.eigh_gram(2.0, s, np.eye(n), xyz, dtype=dtype)),
+                       (lambda s: ref.eigh(2.0, s, np.eye(n), dtype=dtype),
+                        lambda s: bb.eigh(2.0, s, np.eye(n), dtype=dtype))):
+        with pytest.raises(RuntimeError, match="BippError 6"):
+            fn_r(np.zeros((n, n)))
+        with pytest.raises(bb.EigensolverError):
+            fn_o(np.zeros((n, n)))
+        s = np.zeros((n, n), complex)
+        s[2, 1] = s[1, 2] = 1.0
+        assert fn_r(s)[2] == fn_o(s)[2] == 2
