@@ -344,3 +344,50 @@ def test_all_flagged_step_raises_like_compiled_reference(dtype):
         s = np.zeros((n, n), complex)
         s[2, 1] = s[1, 2] = 1.0
         assert fn_r(s)[2] == fn_o(s)[2] == 2
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+def test_eigensolvers_match_compiled_reference_property():
+    """Random flag patterns (dropped antennas, isolated entries, entries near the flag
+    threshold, diagonal-only antennas) and both precisions: the restatement's nReduced,
+    1/nVis and eigenvalues equal the compiled reference's, eigh_gram and eigh."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=80, deadline=None, database=None)
+    @given(st.integers(2, 14), st.integers(0, 2 ** 31), st.sampled_from([np.float32, np.float64]))
+    def check(n, seed, dt):
+        rng = np.random.default_rng(seed)
+        eps = float(np.finfo(dt).eps)
+        a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        s = a @ a.conj().T / n
+        kind = rng.integers(0, 4, n)          # 0 keep, 1 drop, 2 one tiny entry, 3 diagonal only
+        for k in range(n):
+            if kind[k] == 0:
+                continue
+            s[k, :] = 0
+            s[:, k] = 0
+            if kind[k] == 2:
+                j = int(rng.integers(0, n))
+                val = np.sqrt(eps) * rng.uniform(0.5, 2.0)
+                s[max(j, k), min(j, k)] = val
+                s[min(j, k), max(j, k)] = val
+            elif kind[k] == 3:
+                s[k, k] = rng.uniform(0.5, 2.0)
+        xyz = rng.uniform(-20, 20, (n, 3))
+        for fr, fo in ((lambda m: ref.eigh_gram(2.0, m, np.eye(n), xyz, dtype=dt),
+                        lambda m: bb.eigh_gram(2.0, m, np.eye(n), xyz, dtype=dt)),
+                       (lambda m: ref.eigh(2.0, m, np.eye(n), dtype=dt),
+                        lambda m: bb.eigh(2.0, m, np.eye(n), dtype=dt))):
+            try:
+                r = fr(s)
+            except RuntimeError:
+                with pytest.raises(bb.EigensolverError):
+                    fo(s)
+                continue
+            o = fo(s)
+            assert r[2] == o[2]
+            assert abs(r[3] - o[3]) <= 1e-6 * max(r[3], 1e-30)
+            tol = 1e-10 if dt == np.float64 else 1e-4
+            assert np.abs(r[1] - o[1]).max() <= tol * max(np.abs(r[1]).max(), 1e-30)
+
+    check()
