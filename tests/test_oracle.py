@@ -391,3 +391,27 @@ def test_eigensolvers_match_compiled_reference_property():
             assert np.abs(r[1] - o[1]).max() <= tol * max(np.abs(r[1]).max(), 1e-30)
 
     check()
+
+
+@pytest.mark.skipif(not ref.available(), reason="compiled reference not built in this environment")
+def test_gram_and_virtual_vis_match_compiled_reference_property():
+    """Random beamforming matrices, positions, wavelengths and level eigenvalues (zeros,
+    negatives): Gram matrix and virtual visibilities of the restatement equal the compiled
+    reference's (FP64)."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=60, deadline=None, database=None)
+    @given(st.integers(1, 12), st.integers(1, 12), st.integers(0, 2 ** 31), st.floats(0.2, 5.0))
+    def check(n_ant, n_beam, seed, wl):
+        rng = np.random.default_rng(seed)
+        w = rng.standard_normal((n_ant, n_beam)) + 1j * rng.standard_normal((n_ant, n_beam))
+        xyz = rng.uniform(-30, 30, (n_ant, 3))
+        g_r, g_o = ref.gram_matrix(w, xyz, wl), bb.gram_matrix(w, xyz, wl)
+        assert np.abs(g_r - g_o).max() <= 1e-12 * max(np.abs(g_r).max(), 1e-300)
+        v = rng.standard_normal((n_ant, n_beam)) + 1j * rng.standard_normal((n_ant, n_beam))
+        d = rng.standard_normal(n_beam) * (rng.uniform(size=n_beam) > 0.3)
+        sc = float(rng.uniform(1e-3, 1.0))
+        vv_r, vv_o = ref.virtual_vis(sc, d, v), bb.virtual_vis(sc, d, v)
+        assert np.abs(vv_r - vv_o).max() <= 1e-12 * max(np.abs(vv_r).max(), 1e-300)
+
+    check()
