@@ -316,7 +316,8 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
       std::vector<bipp_nufft_t>& p;
       ~Cleanup() { for (auto q : p) bipp_nufft_destroy(q); }
     } cleanup{plans};
-    const double twoPi = 2.0 * 3.14159265358979323846;
+    // 2 pi rounded to float, as the reference's T(2 * pi) with T = float
+    const float twoPi = static_cast<float>(2.0 * 3.14159265358979323846);
     std::vector<float> ks(nBeam);
     for (size_t k = 0; k < nSamples; ++k) {
       const size_t id = sampleIds[order[0][k]];
@@ -325,7 +326,7 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
       ds->uvw(ds->user, id, uvw.data(), nB);
       ds->eig_vec(ds->user, id, v.data(), nAnt);
       // uvw scaled in single precision as the reference's float path
-      const float uvwScale = (float)(twoPi / wl);
+      const float uvwScale = twoPi / wl;   // float division (src/nufft_synthesis.cpp:150-154)
       for (auto& x : uvw) x *= uvwScale;
       h2d(ctx, dV.get(), v.data(), v.size() * sizeof(float2));
       for (size_t im = 0; im < nImages; ++im) {
