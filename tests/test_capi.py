@@ -108,3 +108,34 @@ def test_cxx_shell_host_checks(tmp_path):
     args = [str(exe)] + ([] if torch.cuda.is_available() else ["no-gpu"])
     r = subprocess.run(args, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
+
+
+def test_pybipp_surface():
+    """The names and members of pybipp (python/pybipp.cpp:285-493) that the reference's
+    Python pipeline uses exist with the same call shapes (no device needed)."""
+    import inspect
+
+    import bipp_b200 as bipp
+    from bipp_b200 import (Context, NufftSynthesisOptions, Partition, communicator, config,  # noqa: F401
+                           eigh, eigh_gram, gram_matrix, image_synthesis)
+
+    opt = NufftSynthesisOptions()
+    for m in ("set_tolerance", "set_sample_batch_size", "set_local_uvw_partition", "set_normalize_image",
+              "set_apply_scaling", "set_precision"):
+        assert callable(getattr(opt, m)), m
+    for a in ("tolerance", "sample_batch_size", "local_uvw_partition", "normalize_image", "apply_scaling",
+              "precision"):
+        assert hasattr(opt, a), a
+    assert opt.set_precision("double").precision == "double"
+    with pytest.raises(bipp.InvalidParameterError):
+        opt.set_precision("half")
+    assert Partition.grid([2, 3, 4]).dims == (2, 3, 4)
+    assert Partition.auto().method == "auto" and Partition.none().method == "none"
+    assert isinstance(Context.processing_unit, property)
+    assert list(inspect.signature(Context).parameters)[:2] == ["pu", "comm"]
+    assert list(inspect.signature(eigh_gram).parameters)[:4] == ["wl", "s", "w", "xyz"]
+    assert list(inspect.signature(eigh).parameters)[:3] == ["wl", "s", "w"]
+    assert list(inspect.signature(image_synthesis).parameters)[:6] == ["ctx", "opt", "dataset", "selection",
+                                                                       "image_prop", "image_file_name"]
+    assert all(hasattr(config, f) for f in ("cuda", "rocm", "umpire", "omp", "mpi"))
+    assert (communicator.local().rank, communicator.local().size) == (0, 1)
