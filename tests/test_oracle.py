@@ -228,6 +228,8 @@ def test_restatement_vs_compiled_reference_beamformed(seed):
     v2_r, d2_r, nr2_r, _ = ref.eigh(wl, s, w)
     v2_o, d2_o, nr2_o, _ = bb.eigh(wl, s, w)
     assert nr2_r == nr2_o and np.abs(d2_r - d2_o).max() <= 1e-12 * np.abs(d2_r).max()
+    p2_r, p2_o = _pair_product(v2_r, d2_r), _pair_product(v2_o, d2_o)   # v = W_red X
+    assert np.abs(p2_r - p2_o).max() <= 1e-10 * np.abs(p2_r).max()
     # one level: the upper half of the spectrum, as the reference's level mask
     dl = d_r * (d_r >= np.median(d_r[:nr_r]))
     vv_r, vv_o = ref.virtual_vis(sc_r, dl, v_r), bb.virtual_vis(sc_r, dl, v_r)
