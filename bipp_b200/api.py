@@ -82,8 +82,10 @@ class Context:
         if device is None and comm is not None and self.communicator.size > 1:
             import torch
 
-            n = torch.cuda.device_count()
-            device = self.communicator.rank % n if n else None
+            device = pick_device(self.communicator, torch.cuda.device_count())
+        # the GPU of this context (None: the CUDA device current at creation); collectives
+        # over this context's images run on it
+        self.device = device
         if device is None:
             check(self._lib.bipp_ctx_create(code, C.byref(h)))
         else:
@@ -478,7 +480,7 @@ def image_synthesis(ctx: Context, opt: NufftSynthesisOptions, dataset, selection
             images = _synthesize(ctx, opt, dataset, local, tags, lmn, False)
         else:
             images = np.zeros((len(tags), np.asarray(lmn).shape[0]), dtype=np.float32)
-        images = _reduce_images_to_root(images)
+        images = _reduce_images_to_root(images, getattr(ctx, "device", None))
         if comm.rank != 0:
             return {}
         if opt.normalize_image:
@@ -534,8 +536,15 @@ def split_selection(selection, n_dataset: int, rank: int, size: int):
     return local, n_total
 
 
-def _reduce_images_to_root(images: np.ndarray) -> np.ndarray:
-    """Sum the [nImages, nPixel] float images of all ranks into rank 0 (NCCL on GPUs)."""
+def pick_device(comm: communicator, n_devices: int) -> Optional[int]:
+    """GPU of a rank under a multi-rank communicator: rank % device count, as the
+    reference (src/context_internal.cpp:59-66); None without devices."""
+    return comm.rank % n_devices if n_devices else None
+
+
+def _reduce_images_to_root(images: np.ndarray, device: Optional[int] = None) -> np.ndarray:
+    """Sum the [nImages, nPixel] float images of all ranks into rank 0 (NCCL on GPUs, on
+    the context's device)."""
     import torch
     import torch.distributed as dist
 
@@ -545,7 +554,7 @@ def _reduce_images_to_root(images: np.ndarray) -> np.ndarray:
         raise InvalidParameterError(3, "a communicator of size > 1 needs an initialised torch.distributed group")
     t = torch.from_numpy(np.ascontiguousarray(images, dtype=np.float32))
     if dist.get_backend() == "nccl":
-        t = t.cuda()
+        t = t.cuda(device) if device is not None else t.cuda()
     reduce_images(t, dst=0)
     return t.cpu().numpy()
 

@@ -10,7 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
-#include <mutex>
+#include <climits>
 
 #include "bipp_b200.h"
 #include "context.hpp"
@@ -38,22 +38,32 @@ constexpr size_t kNoAllocScratchBytes = kOffWl + 256;
 // call's intermediates (calls that overlap on the GPU race on it).
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_mu;
-void* g_scratch[128] = {};
-
-// Device address of the scratch array on `device` (looked up once per device, with that
-// device current; the host-side symbol itself is not a device address).
-void* scratch_address(int device) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  require(device >= 0 && device < 128, "invalid device id");
-  if (!g_scratch[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) throw Error(BIPP_GPU_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch[device] = p;
-  }
-  return g_scratch[device];
+// Device address of the scratch array in the current device's context. The host-side
+// symbol is only a stand-in, not a device address; the lookup allocates nothing and is
+// repeated on every call, so a context that was re-created (cudaDeviceReset) never leaves
+// a stale address behind.
+void* scratch_address() {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) throw Error(BIPP_GPU_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  return p;
 }
+
+// makes `device` current for the call and gives the caller's current device back on
+// every exit path (the caller may be a framework with its own notion of the current GPU)
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int device) {
+    B2_CUDA(cudaGetDevice(&prev));
+    if (prev != device) B2_CUDA(cudaSetDevice(device));
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
 
 struct Work {
   float2 *A, *Linv, *T1;
@@ -129,9 +139,13 @@ extern "C" BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl
     require(nAntenna <= (size_t)kN,
             "bipp_eigh_gram_noalloc_s: nAntenna exceeds BIPP_NOALLOC_MAX_ANTENNA (use bipp_eigh_gram_s)");
     require(lds >= nAntenna && ldxyz >= nAntenna && ldv >= nAntenna, "invalid leading dimension");
-    B2_CUDA(cudaSetDevice(device));
+    require(lds <= (size_t)INT_MAX && ldxyz <= (size_t)INT_MAX, "leading dimension above INT_MAX");
+    int nDev = 0;
+    B2_CUDA(cudaGetDeviceCount(&nDev));
+    require(device >= 0 && device < nDev, "invalid device id");
+    DeviceScope scope(device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    char* base = static_cast<char*>(scratch_address(device));
+    char* base = static_cast<char*>(scratch_address());
     const int N = (int)nAntenna;
     const Work w = carve(base, N);
     int* idx = reinterpret_cast<int*>(base + kOffIdx);

@@ -123,9 +123,11 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatc
  * factorisation of G failed, a kept entry of S is not finite or every row and column is
  * flagged, else 0). The call is asynchronous on `stream` (a
  * cudaStream_t). Every call on a device shares the array, so calls that overlap on the
- * GPU race; serialise them (one stream, or events). The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) and should come before any stream
- * capture. Results agree with bipp_eigh_gram_s. */
+ * GPU race; serialise them (one stream, or events). Each call makes `device` current while
+ * it runs, gives the caller's current device back before it returns, and looks up the
+ * array's address in that device's current context (cudaGetSymbolAddress, which allocates
+ * nothing); the first call on a device may load the library's device code and should come
+ * before any stream capture. Results agree with bipp_eigh_gram_s. */
 BIPP_B200_EXPORT BippError bipp_eigh_gram_noalloc_s(int device, void* stream, float wl, size_t nAntenna,
                                                     const void* s, size_t lds, const double* xyz, size_t ldxyz,
                                                     float* d, void* v, size_t ldv, int* nBeamReduced, float* scale,

@@ -2,7 +2,7 @@
 
 Run in a container where the reference tree and oracle/_ref/libbipp_ref.so exist:
 
-    make -C oracle REF=/root/reference && python tests/golden/make_golden.py /root/reference
+    make -C oracle REF=<reference tree> && python tests/golden/make_golden.py <reference tree>
 
 Outputs (compressed .npz, a few hundred KB in total):
   lofar.npz      inputs of the reference's test data tests/data/lofar_input.json (2 samples,
@@ -261,7 +261,9 @@ def frame(refdir: str):
 
 
 if __name__ == "__main__":
-    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference tree>")
+    refdir = sys.argv[1]
     lofar(refdir)
     synth_eig()
     nuft()

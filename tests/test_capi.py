@@ -30,11 +30,15 @@ def test_library_exports_every_declared_symbol():
         assert n in _lib.SIGNATURES, n
 
 
-def test_library_is_sm100a_and_in_tree():
-    from bipp_b200 import _lib
+def test_library_in_tree_and_build_recipe_targets_only_sm100a():
+    """The library is built in the source tree, and the build recipe compiles and links
+    device code for sm_100a alone (no other -gencode target, no PTX fallback)."""
+    from bipp_b200 import _lib, build
 
     assert os.path.dirname(_lib.LIB_PATH) == os.path.join(ROOT, "bipp_b200")
     assert os.path.getsize(_lib.LIB_PATH) > 100_000
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert all("arch=" not in f and "-arch" not in f for f in build._flags() if f not in build.ARCH)
 
 
 def test_no_cpu_processing_unit():

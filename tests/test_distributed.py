@@ -144,6 +144,19 @@ def test_communicator():
     assert bipp.config.cuda and not bipp.config.mpi
 
 
+def test_rank_device_choice():
+    """Under a multi-rank communicator a rank's GPU is rank % device count, as the
+    reference's context (src/context_internal.cpp:59-66); the image reduction runs on it."""
+    from bipp_b200.api import pick_device
+
+    import bipp_b200 as bipp
+
+    for size, n_dev in ((2, 1), (4, 2), (8, 8), (3, 8)):
+        for rank in range(size):
+            assert pick_device(bipp.communicator(rank, size), n_dev) == rank % n_dev
+    assert pick_device(bipp.communicator(1, 2), 0) is None
+
+
 def _oracle_synthesize(ctx, opt, dataset, selection, tags, lmn, normalize):
     """The per-rank GPU synthesis call stood in by the FP64 oracle: VV = V diag(scale ev)
     V^H per image and sample, exact sum over the baselines, 1/nSamples if normalize."""
