@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stages", action="store_true", help="report per-stage device times")
+    ap.add_argument("--check-steps", type=int, default=256,
+                    help="entries of the FP64 image/eigenvalue check (spread over the batch); 0 skips it")
+    ap.add_argument("--check-pixels", type=int, default=512)
     ap.add_argument("--plain-steps", type=int, default=16,
                     help="time steps of the plain-GPU comparison (one NUFFT per step and level); 0 skips it")
     a = ap.parse_args()
@@ -201,13 +204,16 @@ def share_levels(intervals, device):
     return iv.cpu().numpy()
 
 
-def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, threads=None, wl=None):
-    """The reference's CPU path (compiled reference sources) on a bounded sample:
-    eigh_gram<float> + virtual_vis<float> per level on n_eig_steps entries, and the
-    reference direct sum nuft_sum<double> over all baselines of one entry for n_pix
-    pixels, extrapolated to the full image and all levels (the reference's CPU NUFFT,
-    neonufft, is not available). A time step holds cfg.n_channels entries. Returns
-    (time-steps/s, cores, sample description)."""
+def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=5, n_pix=2048, threads=None, wl=None, nufft=True):
+    """The reference's CPU path (compiled reference sources) on a bounded sample.
+
+    Measured in full: eigh_gram<float> + virtual_vis<float> for every level, per entry,
+    on n_eig_steps entries; the rate is the median over those entries (time-steps/s, a
+    time step holding cfg.n_channels entries). The NUFFT stage has no CPU counterpart here
+    (the reference's neonufft is not available): when `nufft` is set, the reference's
+    direct sum nuft_sum<double> over all baselines of one entry is timed on n_pix pixels
+    and extrapolated to the full image and all levels, reported separately and never
+    folded into the rate. Returns (time-steps/s, cores, sample description, extras)."""
     from oracle import ref
 
     from bipp_b200 import simulate as sim
@@ -218,7 +224,7 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
     obs = sim.observation(cfg)
     N = cfg.n_antenna
     w = np.eye(N, dtype=np.complex64)
-    t_eig = t_vv = 0.0
+    t_eig, t_vv = [], []
     last = None
     for k in range(n_eig_steps):
         s = S[k].transpose(0, 1).cpu().numpy().T  # logical S
@@ -230,27 +236,32 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=2, n_pix=2048, thre
         for lo, hi in intervals:
             vvs.append(ref.virtual_vis(sc, d * ((d >= lo) & (d <= hi)), v, dtype=np.float32))
         t2 = time.perf_counter()
-        t_eig += t1 - t0
-        t_vv += t2 - t1
+        t_eig.append(t1 - t0)
+        t_vv.append(t2 - t1)
         last = (vvs, xyz[k].cpu().numpy())
-    t_eig /= n_eig_steps
-    t_vv /= n_eig_steps
-    vvs, x = last
-    uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / wl)
-    rng = np.random.default_rng(0)
-    pix = rng.choice(obs.lmn.shape[0], n_pix, replace=False)
-    lmn = obs.lmn[pix]
-    vals = vvs[0].reshape(-1, order="F").astype(np.complex128)
-    t0 = time.perf_counter()
-    ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], lmn[:, 0], lmn[:, 1], lmn[:, 2], threads=threads)
-    t_pix = time.perf_counter() - t0
-    t_nuft = t_pix * (obs.lmn.shape[0] / n_pix) * len(intervals)
-    per_step = (t_eig + t_vv + t_nuft) * cfg.n_channels
-    desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} on {n_eig_steps} entries "
-            f"({t_eig:.3f}+{t_vv:.3f} s/entry); nuft_sum<double> all {N * N} baselines x {n_pix} px "
-            f"({t_pix:.2f} s) extrapolated to {obs.lmn.shape[0]} px x {len(intervals)} levels "
-            f"({t_nuft:.1f} s/entry); {cfg.n_channels} entries per time step; neonufft unavailable")
-    return 1.0 / per_step, threads, desc
+    per_entry = float(np.median(np.add(t_eig, t_vv)))
+    rate = 1.0 / (per_entry * cfg.n_channels)
+    desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} measured on {n_eig_steps} entries, median "
+            f"{per_entry:.3f} s/entry (eigh_gram {np.median(t_eig):.3f}, virtual_vis {np.median(t_vv):.4f}); "
+            f"{cfg.n_channels} entries per time step; NUFFT stage not included (neonufft unavailable)")
+    extras = {"eig_vv_s_per_entry": per_entry}
+    if nufft:
+        vvs, x = last
+        uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / wl)
+        rng = np.random.default_rng(0)
+        pix = rng.choice(obs.lmn.shape[0], n_pix, replace=False)
+        lmn = obs.lmn[pix]
+        vals = vvs[0].reshape(-1, order="F").astype(np.complex128)
+        t0 = time.perf_counter()
+        ref.nuft_sum(1.0, vals, uvw[:, 0], uvw[:, 1], uvw[:, 2], lmn[:, 0], lmn[:, 1], lmn[:, 2], threads=threads)
+        t_pix = time.perf_counter() - t0
+        t_nuft = t_pix * (obs.lmn.shape[0] / n_pix) * len(intervals)
+        extras["nufft_direct_sum_extrapolated"] = {
+            "s_per_entry": round(t_nuft, 1), "kind": "extrapolated",
+            "sample": f"nuft_sum<double> over all {N * N} baselines x {n_pix} px measured ({t_pix:.2f} s), scaled to "
+                      f"{obs.lmn.shape[0]} px x {len(intervals)} levels; an O(baselines x pixels) direct sum, not "
+                      f"the reference's NUFFT"}
+    return rate, threads, desc, extras
 
 
 def measured_peaks():
@@ -261,19 +272,11 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-def profiled_traffic_ratio():
-    """DRAM bytes per algorithmic byte of a full-size spreading launch, from the committed
-    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum of two launches of the
-    2048-step batch / their algorithmic bytes)."""
-    path = os.path.join(ROOT, "profiles", "spread_tc_kernel_c2.md")
-    try:
-        with open(path) as f:
-            for ln in f:
-                if ln.startswith("traffic_per_algorithmic_byte:"):
-                    return float(ln.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
+# spreading launch, measured with ncu on one w-slab of a 128-step batch of this workload
+# (512 antennas, 1024^2 px, 4 levels); the traffic of a full launch scales with the points
+# and grid cells it processes, as the algorithmic bytes do.
+SPREAD_TRAFFIC_PER_ALG_BYTE = None
 
 
 def spread_roofline(stats, spread_ms, n_levels):
@@ -290,7 +293,7 @@ def spread_roofline(stats, spread_ms, n_levels):
     peaks, label = measured_peaks()
     achieved = per_launch / dur_s / 1e9
     flops = stats["points"] * n_levels * 4 * stats["W"] ** 3 / slabs  # real weight x complex value: 4 flops
-    ratio = profiled_traffic_ratio()
+    ratio = SPREAD_TRAFFIC_PER_ALG_BYTE
     traffic = int(ratio * per_launch) if ratio else None
     return {"kernel": "spread_tc_kernel", "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 5),
@@ -310,7 +313,7 @@ def run_reference(args):
 
     from bipp_b200 import simulate as sim
 
-    args.time_steps = max(8, args.steps + args.warmup)
+    args.time_steps = max(8, args.steps + args.warmup)  # one entry per bench step
     cfg = workload_config(args)
     obs = sim.observation(cfg)
     masks = sim.keep_masks(cfg)
@@ -327,19 +330,27 @@ def run_reference(args):
                                    dtype=np.float32)
         d_all.append(d)
     intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, np.concatenate(d_all))
+    # each bench step: eigh_gram<float> + virtual_vis<float> per level on one entry
+    # (measured in full); the NUFFT stage is reported apart (its direct-sum
+    # extrapolation), not folded into the value
     vals = []
     for k in range(args.warmup + args.steps):
-        v, cores, desc = cpu_reference_sample(cfg, S[k:k + 1], x[k:k + 1], intervals, n_eig_steps=1, n_pix=1024,
-                                              wl=wl0)
+        v, cores, desc, _ = cpu_reference_sample(cfg, S[k:k + 1], x[k:k + 1], intervals, n_eig_steps=1, wl=wl0,
+                                                 nufft=False)
         if k >= args.warmup:
             vals.append(v)
     value = float(np.median(vals))
+    _, _, _, extra = cpu_reference_sample(cfg, S[:1], x[:1], intervals, n_eig_steps=1, n_pix=1024, wl=wl0)
+    desc = (f"eigh_gram<float>+virtual_vis<float>x{cfg.n_levels} per entry, median of {args.steps} entries "
+            f"({1.0 / value:.3f} s per time step); NUFFT stage not included (neonufft unavailable)")
     line = {"impl": "reference", "metric": metric_of(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded observation of the workload's shape)",
-            "config": {"workload": workload_text(args), "time_steps_per_batch": args.time_steps},
+            "config": {"workload": workload_text(args), "sample": "one entry (time step x channel) per bench step",
+                       "stages_timed": "eigh_gram + virtual_vis (the reference's CPU path for them)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+            "nufft_direct_sum_extrapolated": extra.get("nufft_direct_sum_extrapolated"),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -427,6 +438,24 @@ def main():
         stages["eig_kernels"] = dict(zip(["prep_gram", "cholesky_fp64", "trinv_fp64", "reduction_gemms", "hetrd",
                                           "tridiag_fp64", "backtransform", "x_gemm"], [round(float(x), 3) for x in kt]))
         roof = spread_roofline(pl.nufft_stats(), float(st[3]), cfg.n_levels)
+        # the stages the CPU baseline times in full (eigensolve + levels/virtual
+        # visibilities), as a rate of the same unit
+        stages["eig_vv_rate"] = {"value": T_steps / ((float(st[0]) + float(st[1])) / 1000.0), "unit": UNIT,
+                                 "stages": "eigensolve + levels_vv"}
+
+    # image and eigenvalue error of the timed form against FP64, on a sub-batch spread
+    # over the whole batch (every (T / check_steps)-th entry), at random pixels
+    parity = None
+    if rank == 0 and args.check_steps > 0:
+        from bipp_b200 import verify
+
+        stride = max(1, T // args.check_steps)
+        sel = torch.arange(0, T, stride, device=device)[:args.check_steps]
+        parity = verify.check_batch(ctx, S[sel].contiguous(), xyz[sel].contiguous(), wl[sel].contiguous(), obs, n,
+                                    intervals, cfg.eps, n_pix=args.check_pixels,
+                                    chunk_steps=min(args.chunk_steps, len(sel)))
+        parity["reference"] = ("FP64: bipp_eigh_gram_batched_d + FP64 V diag(d) V^H + direct sum with FP64 phase "
+                               "and trigonometry (the library's FP64 pieces pinned to the compiled reference)")
 
     # the plain GPU form of the metric on a bounded sample: the same kernels, one step at a
     # time and one NUFFT per step and level (no batching across steps or levels)
@@ -481,8 +510,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             Sc = S_h if not args.no_e2e else S  # noqa: F821
-            v, cores, desc = cpu_reference_sample(cfg, Sc, xyz, intervals, wl=float(wl[0].item()))
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+            v, cores, desc, extra = cpu_reference_sample(cfg, Sc, xyz, intervals, wl=float(wl[0].item()))
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc,
+                   "stages": "eigh_gram + virtual_vis", **extra}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -497,7 +527,9 @@ def main():
                            "parallelism": f"dp{world} (steps)",
                            "l2": f"inputs ({S_bytes / 1e9:.1f} GB/batch) larger than L2; no flush"},
                 "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,
-                "cpu_baseline": cpu, "roofline": roof, "plain_gpu": plain}
+                "cpu_baseline": cpu, "roofline": roof, "plain_gpu": plain,
+                "image_rel_l2": parity and parity["image_rel_l2"], "eig_rel_err": parity and parity["eig_rel_err_max"],
+                "parity": parity}
         print(json.dumps(line))
     pl.close()
     ctx.close()

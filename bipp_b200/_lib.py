@@ -63,6 +63,7 @@ SIGNATURES = {
     "bipp_eigh_s": [_p, _f, _sz, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _psz, _pf],
     "bipp_eigh_d": [_p, _d, _sz, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _psz, _pd],
     "bipp_eigh_gram_batched_s": [_p, _sz, _sz, _p, _p, _p, _p, _p, _p, _p],
+    "bipp_eigh_gram_batched_d": [_p, _sz, _sz, _p, _p, _p, _p, _p, _p, _p],
     "bipp_eigh_gram_noalloc_s": [_i, _p, _f, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _p, _p, _p],
     "bipp_gram_matrix_s": [_p, _sz, _sz, _p, _sz, _p, _sz, _f, _p, _sz],
     "bipp_gram_matrix_d": [_p, _sz, _sz, _p, _sz, _p, _sz, _d, _p, _sz],

@@ -203,23 +203,27 @@ def eigh(wl, s, w, ctx: Optional[Context] = None, precision: Optional[str] = Non
     return (v, d, nred.value, scale.value) if full else (v, d, scale.value)
 
 
-def eigh_gram_batched(wl, s, xyz, ctx: Optional[Context] = None):
-    """Batched eigh_gram with W = I over steps: wl [B], s [B, N, N] (complex64, s[b] is
-    the step's matrix; its lower triangle in column-major order is used), xyz [B, N, 3].
-    Returns (v [B, N, N] (v[b][:, c] eigenvector c), d [B, N], nReduced [B], scale [B])."""
+def eigh_gram_batched(wl, s, xyz, ctx: Optional[Context] = None, precision: str = "single"):
+    """Batched eigh_gram with W = I over steps: wl [B], s [B, N, N] (s[b] is the step's
+    matrix; its lower triangle in column-major order is used), xyz [B, N, 3]. Single
+    precision (complex64, bipp_eigh_gram_batched_s) or "double" (complex128,
+    bipp_eigh_gram_batched_d). Returns (v [B, N, N] (v[b][:, c] eigenvector c), d [B, N],
+    nReduced [B], scale [B])."""
     ctx = ctx or default_context()
-    wl = np.ascontiguousarray(wl, dtype=np.float32)
-    s = np.asarray(s, dtype=np.complex64)
+    dbl = precision == "double"
+    rt, ct = (np.float64, np.complex128) if dbl else (np.float32, np.complex64)
+    wl = np.ascontiguousarray(wl, dtype=rt)
+    s = np.asarray(s, dtype=ct)
     B, N = s.shape[0], s.shape[1]
     # column-major per matrix: store transposed so that memory order matches F layout
     sF = np.ascontiguousarray(np.transpose(s, (0, 2, 1)))
-    xyzF = np.ascontiguousarray(np.transpose(np.asarray(xyz, dtype=np.float32), (0, 2, 1)))
-    d = np.zeros((B, N), dtype=np.float32)
-    vF = np.zeros((B, N, N), dtype=np.complex64)
+    xyzF = np.ascontiguousarray(np.transpose(np.asarray(xyz, dtype=rt), (0, 2, 1)))
+    d = np.zeros((B, N), dtype=rt)
+    vF = np.zeros((B, N, N), dtype=ct)
     nred = np.zeros(B, dtype=np.uint64)
-    scale = np.zeros(B, dtype=np.float32)
-    check(ctx._lib.bipp_eigh_gram_batched_s(ctx.handle, B, N, _ptr(wl), _ptr(sF), _ptr(xyzF), _ptr(d), _ptr(vF),
-                                            _ptr(nred), _ptr(scale)))
+    scale = np.zeros(B, dtype=rt)
+    fn = ctx._lib.bipp_eigh_gram_batched_d if dbl else ctx._lib.bipp_eigh_gram_batched_s
+    check(fn(ctx.handle, B, N, _ptr(wl), _ptr(sF), _ptr(xyzF), _ptr(d), _ptr(vF), _ptr(nred), _ptr(scale)))
     v = np.transpose(vF, (0, 2, 1))
     return v, d, nred.astype(np.int64), scale
 
@@ -721,10 +725,11 @@ class Pipeline:
         return ms
 
     def nufft_stats(self):
-        """Last NUFFT: dict(points, slabs, grid_bytes, items, nx, ny, nw, W)."""
-        st = np.zeros(8, dtype=np.int64)
+        """Last NUFFT: dict(points, slabs, grid_bytes, items, nx, ny, nw, W, split_tiles)."""
+        st = np.zeros(9, dtype=np.int64)
         check(self.ctx._lib.bipp_pipeline_nufft_stats(self.handle, _ptr(st)))
-        return dict(zip(["points", "slabs", "grid_bytes", "items", "nx", "ny", "nw", "W"], [int(x) for x in st]))
+        return dict(zip(["points", "slabs", "grid_bytes", "items", "nx", "ny", "nw", "W", "split_tiles"],
+                        [int(x) for x in st]))
 
     def close(self):
         if getattr(self, "handle", None):

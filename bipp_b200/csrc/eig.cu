@@ -539,12 +539,21 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
 }
 
 // batched eigh_gram, W = I
-static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, const float* wl, const void* s,
-                                   const float* xyz, float* d, void* v, size_t* nBeamReduced, float* scale) {
-  using C = float2;
+template <typename T>
+static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, const T* wl, const void* s,
+                                   const T* xyz, T* d, void* v, size_t* nBeamReduced, T* scale) {
+  using C = typename Cplx<T>::type;
   require(nBatch > 0 && nAnt > 0, "empty problem");
   require(s && xyz && wl && d && nBeamReduced && scale, "null pointer", BIPP_INVALID_POINTER_ERROR);
   require(nAnt <= 4096, "nAntenna above the supported maximum of 4096");
+  if (sizeof(T) == 8) {
+    // as eigh_host: FP64 rows of the tridiagonalisation and back-transform in shared memory
+    const size_t cb = sizeof(C), smem = ctx->maxSmemOptin;
+    const size_t lim = std::min(smem / (5 * cb), (smem / cb - kBtThreads) / 5);
+    if (nAnt > lim)
+      throw Error(BIPP_INVALID_PARAMETER_ERROR,
+                  "nAntenna above the FP64 maximum of " + std::to_string(lim) + " set by this device's shared memory");
+  }
   const int Nmax = (int)nAnt;
   const size_t chunk = std::min<size_t>(nBatch, 256);
   const size_t n2 = nAnt * nAnt;
@@ -558,7 +567,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
   h2d(ctx, dX.get(), xyzh.data(), xyzh.size() * sizeof(double));
   h2d(ctx, dWl.get(), wlh.data(), nBatch * sizeof(double));
   dStatus.zero();
-  EigWork<float> work;
+  EigWork<T> work;
   work.reserve(ctx, (int)chunk, Nmax);
   std::vector<int> nredh(nBatch);
   std::vector<long long> nvish(nBatch);
@@ -567,16 +576,16 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
   for (size_t b0 = 0; b0 < nBatch; b0 += chunk) {
     const size_t nb = std::min(chunk, nBatch - b0);
     h2d(ctx, dS.get(), static_cast<const char*>(s) + b0 * n2 * sizeof(C), nb * n2 * sizeof(C));
-    EigLaunch<float> L{};
+    EigLaunch<T> L{};
     L.nBatch = (int)nb; L.nBeam = (int)nAnt; L.nAnt = (int)nAnt; L.Nmax = Nmax;
     L.S = dS.get<C>(); L.sStride = (long long)n2; L.lds = (int)nAnt;
     L.xyz = dX.get<double>(); L.xyzStride = (long long)nAnt * 3; L.ldxyz = (int)nAnt; L.wl = dWl.get<double>();
-    L.mode = 0; L.eps = std::numeric_limits<float>::epsilon();
+    L.mode = 0; L.eps = std::numeric_limits<T>::epsilon();
     L.gram = true; L.identityW = true;
     L.idx = dIdx.get<int>(); L.nred = dNred.get<int>(); L.nvis = dNvis.get<long long>();
     L.status = dStatus.get<int>(); L.lam = dLam.get<double>();
     L.doFlag = 1; L.batchOffset = (int)b0;
-    eig_launch<float>(ctx, L, work);
+    eig_launch<T>(ctx, L, work);
     // outputs for this chunk: scatter each matrix's eigenvectors to its kept antenna rows
     std::vector<int> nr(nb);
     d2h(ctx, nr.data(), dNred.get<int>() + b0, nb * sizeof(int));
@@ -596,7 +605,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     d2h(ctx, lamh.data(), dLamPad.get(), nb * nAnt * sizeof(double));
     if (v) d2h(ctx, static_cast<char*>(v) + b0 * n2 * sizeof(C), dOut.get(), nb * n2 * sizeof(C));
     sync(ctx);
-    for (size_t i = 0; i < nb * nAnt; ++i) d[b0 * nAnt + i] = (float)lamh[i];
+    for (size_t i = 0; i < nb * nAnt; ++i) d[b0 * nAnt + i] = (T)lamh[i];
   }
   d2h(ctx, nredh.data(), dNred.get(), nBatch * sizeof(int));
   d2h(ctx, nvish.data(), dNvis.get(), nBatch * sizeof(long long));
@@ -608,7 +617,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     if (stat[b] & kStatusNonFinite) throw Error(BIPP_EIGENSOLVER_ERROR, "non-finite visibility in a kept entry of S");
     if (nredh[b] == 0) throw Error(BIPP_EIGENSOLVER_ERROR, "every row and column of S is flagged (empty eigenproblem)");
     nBeamReduced[b] = (size_t)nredh[b];
-    scale[b] = nvish[b] ? 1.0f / (float)nvish[b] : 0.0f;
+    scale[b] = nvish[b] ? T(1) / (T)nvish[b] : T(0);
   }
 }
 
@@ -727,7 +736,14 @@ BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenn
                                    const float* xyz, float* d, void* v, size_t* nBeamReduced, float* scale) {
   return guard([&] {
     require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
-    eigh_gram_batched_host(ctx, nBatch, nAntenna, wl, s, xyz, d, v, nBeamReduced, scale);
+    eigh_gram_batched_host<float>(ctx, nBatch, nAntenna, wl, s, xyz, d, v, nBeamReduced, scale);
+  });
+}
+BippError bipp_eigh_gram_batched_d(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna, const double* wl, const void* s,
+                                   const double* xyz, double* d, void* v, size_t* nBeamReduced, double* scale) {
+  return guard([&] {
+    require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
+    eigh_gram_batched_host<double>(ctx, nBatch, nAntenna, wl, s, xyz, d, v, nBeamReduced, scale);
   });
 }
 BippError bipp_gram_matrix_s(bipp_ctx_t ctx, size_t nAntenna, size_t nBeam, const void* w, size_t ldw, const float* xyz,

@@ -353,9 +353,11 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   clearList_.ensure(ctx_, (size_t)std::max(1, ntiles) * sizeof(int));
   count_launch();
   tile_load_kernel<<<tb, 256, 0, ctx_->stream>>>(g_, offsets_.get<int>(), load_.get<int>());
+  splitCount_.ensure(ctx_, sizeof(int));
+  B2_CUDA(cudaMemsetAsync(splitCount_.get(), 0, sizeof(int), ctx_->stream));
   count_launch();
   tile_parts_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), kSpreadCap, parts_.get<int>(),
-                                                  clearFlag_.get<int>());
+                                                  clearFlag_.get<int>(), splitCount_.get<int>());
   B2_CHECK_LAUNCH();
   exclusive_scan(parts_.get<int>(), itemOff_.get<int>(), ntiles);
   if (tc) {
@@ -380,10 +382,12 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
                                                  items_.get<SpreadItem>());
   B2_CHECK_LAUNCH();
   {
-    int total = 0;
+    int total = 0, split = 0;
     d2h(ctx_, &total, offsets_.get<int>() + nkeys_, sizeof(int));
+    d2h(ctx_, &split, splitCount_.get<int>(), sizeof(int));
     sync(ctx_);
     lastPoints = total;
+    lastSplitTiles = split;
     lastSlabs = nslab;
     lastItems = nItemsAll;
     lastGridBytes = (long long)g_.ntw * kTW * (long long)planeBytes * nch_;
@@ -534,7 +538,7 @@ static void nufft_transform(bipp_nufft_s* p) {
     }
     B2_CHECK_LAUNCH();
     const double* ud = u64.get<double>();
-    const int blocks = (int)((p->nPixel + kDirectThreads - 1) / kDirectThreads);
+    const dim3 blocks = direct_sum_grid((long long)p->nPixel, (long long)n, ctx->smCount);
     for (size_t im = 0; im < p->nImages; ++im) {
       count_launch();
       f2d_kernel<<<256, 256, 0, ctx->stream>>>(reinterpret_cast<const float*>(p->values.get<float2>() + im * ld), 2 * n,
@@ -761,7 +765,7 @@ BippError bipp_nuft_sum_s(bipp_ctx_t ctx, float alpha, size_t nIn, const void* i
     h2d(ctx, dX.get<float>() + nOut, y, nOut * sizeof(float));
     h2d(ctx, dX.get<float>() + 2 * nOut, z, nOut * sizeof(float));
     h2d(ctx, dO.get(), out, nOut * sizeof(float));
-    const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
     count_launch();
     direct_sum_kernel<float, float2, float, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         (double)alpha, (long long)nIn, dIn.get<float2>(), (long long)nIn, dU.get<float>(), dU.get<float>() + nIn,
@@ -788,7 +792,7 @@ BippError bipp_nuft_sum_d(bipp_ctx_t ctx, double alpha, size_t nIn, const void* 
     h2d(ctx, dX.get<double>() + nOut, y, nOut * sizeof(double));
     h2d(ctx, dX.get<double>() + 2 * nOut, z, nOut * sizeof(double));
     h2d(ctx, dO.get(), out, nOut * sizeof(double));
-    const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
     count_launch();
     direct_sum_kernel<double, double2, double, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         alpha, (long long)nIn, dIn.get<double2>(), (long long)nIn, dU.get<double>(), dU.get<double>() + nIn,
@@ -808,7 +812,7 @@ BippError bipp_nuft_sum_multi_device(bipp_ctx_t ctx, double alpha, size_t nIn, s
     require(ctx && values && u && v && w && x && y && z && out, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(nch >= 1 && ldIn >= nIn && ldOut >= nOut, "invalid sizes");
     if (!nOut) return;
-    const int blocks = (int)((nOut + kDirectThreads - 1) / kDirectThreads);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
     for (size_t c0 = 0; c0 < nch; c0 += 4) {
       const int n = (int)std::min<size_t>(4, nch - c0);
       count_launch();

@@ -57,8 +57,9 @@ public:
 
   const NufftGeom& geom() const { return g_; }
   // statistics of the last execute(): points spread, slabs (spreading launches), bytes of
-  // grid written by the spreading (all slabs), work items
-  long long lastPoints = 0, lastSlabs = 0, lastGridBytes = 0, lastItems = 0;
+  // grid written by the spreading (all slabs), work items, tiles split into several
+  // parts (more than kSpreadCap points; their parts accumulate with atomics)
+  long long lastPoints = 0, lastSlabs = 0, lastGridBytes = 0, lastItems = 0, lastSplitTiles = 0;
   long long num_pixels() const { return (long long)g_.Na * g_.Nb; }
   int channels() const { return nch_; }
   bool sincos64() const { return eps_ < 1e-6; }
@@ -76,7 +77,7 @@ private:
   double su_ = 1, sv_ = 1;
   long long nkeys_ = 0, valStride_ = 0;
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
-  DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
+  DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, splitCount_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
   std::map<int, cufftHandle> plans_;
   int slabTiles_ = 1;
   cufftHandle plan_for(int batch);

@@ -450,11 +450,12 @@ static __global__ void tile_load_kernel(NufftGeom g, const int* __restrict__ off
 // spreading parts of each tile (ceil(load / cap), 0 when empty) and whether the tile has
 // to be cleared before spreading (empty, or spread in several parts that accumulate)
 static __global__ void tile_parts_kernel(int ntiles, const int* __restrict__ load, int cap, int* __restrict__ parts,
-                                         int* __restrict__ clearFlag) {
+                                         int* __restrict__ clearFlag, int* __restrict__ splitTiles) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
     const int np = (load[t] + cap - 1) / cap;
     parts[t] = np;
     clearFlag[t] = (np != 1) ? 1 : 0;
+    if (np > 1) atomicAdd(splitTiles, 1);
   }
 }
 
@@ -701,8 +702,13 @@ direct_sum_kernel(double alpha, long long nIn, const C* __restrict__ input, long
   for (int c = 0; c < CH; ++c) acc[c] = 0.0;
   const double twopi = 6.283185307179586476925286766559;
   const double inv2pi = 1.0 / twopi;
-  for (long long k0 = 0; k0 < nIn; k0 += kDirectChunk) {
-    const int nk = (nIn - k0 < (long long)kDirectChunk) ? (int)(nIn - k0) : kDirectChunk;
+  // blockIdx.y takes one slice of the inputs (whole chunks); slices add their partial
+  // sums atomically when the inputs are split
+  const long long per = ((nIn + gridDim.y - 1) / gridDim.y + kDirectChunk - 1) / kDirectChunk * kDirectChunk;
+  const long long kBegin = (long long)blockIdx.y * per;
+  const long long kEnd = (kBegin + per < nIn) ? kBegin + per : nIn;
+  for (long long k0 = kBegin; k0 < kEnd; k0 += kDirectChunk) {
+    const int nk = (kEnd - k0 < (long long)kDirectChunk) ? (int)(kEnd - k0) : kDirectChunk;
     __syncthreads();
     for (int i = threadIdx.x; i < nk; i += blockDim.x) {
       su[i] = (double)u[k0 + i];
@@ -738,9 +744,31 @@ direct_sum_kernel(double alpha, long long nIn, const C* __restrict__ input, long
   }
   if (active) {
 #pragma unroll
-    for (int c = 0; c < CH; ++c)
-      if (c < nch) out[(long long)c * ldOut + p] += (TO)acc[c];
+    for (int c = 0; c < CH; ++c) {
+      if (c < nch) {
+        if (gridDim.y > 1)
+          atomicAdd(&out[(long long)c * ldOut + p], (TO)acc[c]);
+        else
+          out[(long long)c * ldOut + p] += (TO)acc[c];
+      }
+    }
   }
+}
+
+// Grid of direct_sum_kernel: one thread per output; when the outputs fill fewer than
+// about four CTAs per SM, the inputs are split over blockIdx.y (slices of at least 4096
+// inputs) so that few pixels over many baselines still fill the GPU.
+inline dim3 direct_sum_grid(long long nOut, long long nIn, int smCount) {
+  const long long bx = (nOut + kDirectThreads - 1) / kDirectThreads;
+  const long long target = 4LL * (smCount > 0 ? smCount : 148);
+  long long by = 1;
+  if (bx < target) {
+    by = (target + bx - 1) / bx;
+    const long long maxSlices = nIn / 4096 > 1 ? nIn / 4096 : 1;
+    by = by < maxSlices ? by : maxSlices;
+    by = by < 65535 ? by : 65535;
+  }
+  return dim3((unsigned)bx, (unsigned)by, 1);
 }
 
 }  // namespace bippb200

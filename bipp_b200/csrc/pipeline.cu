@@ -541,6 +541,7 @@ BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats) {
     stats[5] = g.ny;
     stats[6] = g.nw;
     stats[7] = g.W;
+    stats[8] = pl->core.lastSplitTiles;
   });
 }
 

@@ -105,6 +105,12 @@ BIPP_B200_EXPORT BippError bipp_eigh_d(bipp_ctx_t ctx, double wl, size_t nAntenn
 BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna,
                                                     const float* wl, const void* s, const float* xyz, float* d,
                                                     void* v, size_t* nBeamReduced, float* scale);
+/* FP64 form of bipp_eigh_gram_batched_s (the reference's eigh_gram<double>, zhegv, per
+ * step): complex double s and v, double wl, xyz, d and scale; nAntenna at most the FP64
+ * limit of bipp_eigh_gram_d. */
+BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_d(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna,
+                                                    const double* wl, const void* s, const double* xyz, double* d,
+                                                    void* v, size_t* nBeamReduced, double* scale);
 
 /* Largest antenna count accepted by bipp_eigh_gram_noalloc_s. */
 #define BIPP_NOALLOC_MAX_ANTENNA 128
@@ -285,9 +291,10 @@ BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int ena
  * inverse, [3] reduction GEMMs, [4] Householder tridiagonalisation, [5] tridiagonal
  * eigenpairs, [6] back-transform, [7] Linv^H Y GEMM. */
 BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms);
-/* Statistics of the last NUFFT of the pipeline (8 values): points spread, spreading
+/* Statistics of the last NUFFT of the pipeline (9 values): points spread, spreading
  * launches (w-slabs), grid bytes written by the spreading, spreading work items, fine
- * grid sizes nx, ny, nw, kernel width W. */
+ * grid sizes nx, ny, nw, kernel width W, tiles split into several work items (more than
+ * 4096 points; their parts accumulate into the grid with atomics). */
 BIPP_B200_EXPORT BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
 

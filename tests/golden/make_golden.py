@@ -74,6 +74,13 @@ def lofar(refdir: str):
         out[f"nred_{prec}"] = np.array(nrs)
         out[f"scale_{prec}"] = np.array(scs)
         out[f"vv_{prec}"] = np.array(vvs)
+        # the same samples with identity beamforming (W = I over the 55 stations): the
+        # input of the batched eigh_gram, which takes W = I
+        eye = [ref.eigh_gram(d["wl"], ss[k], np.eye(ss[k].shape[0]), xyzs[k], dtype=dt) for k in range(len(ss))]
+        out[f"eye_v_{prec}"] = np.array([e[0] for e in eye])
+        out[f"eye_d_{prec}"] = np.array([e[1] for e in eye])
+        out[f"eye_nred_{prec}"] = np.array([e[2] for e in eye])
+        out[f"eye_scale_{prec}"] = np.array([e[3] for e in eye])
     np.savez_compressed(os.path.join(HERE, "lofar.npz"), **out)
 
 
