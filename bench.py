@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--image", type=int, default=None)
     ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
     ap.add_argument("--chunk-steps", type=int, default=None, help="entries per eigensolver/VV chunk")
+    ap.add_argument("--vv-precision", default="tf32x3", choices=["tf32x3", "bf16x3", "fp32", "fp64"],
+                    help="arithmetic of the virtual-visibility products of the batched form")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -204,7 +206,8 @@ def share_levels(intervals, device):
     return iv.cpu().numpy()
 
 
-def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=5, n_pix=2048, threads=None, wl=None, nufft=True):
+def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=5, n_pix=2048, threads=None, wl=None, nufft=True,
+                         ref_eig_errors=False):
     """The reference's CPU path (compiled reference sources) on a bounded sample.
 
     Measured in full: eigh_gram<float> + virtual_vis<float> for every level, per entry,
@@ -240,11 +243,27 @@ def cpu_reference_sample(cfg, S, xyz, intervals, n_eig_steps=5, n_pix=2048, thre
         t_vv.append(t2 - t1)
         last = (vvs, xyz[k].cpu().numpy())
     per_entry = float(np.median(np.add(t_eig, t_vv)))
+    # the reference FP32 eigenvalues' own error against its FP64 path (zhegv) on the
+    # same entries, beside which the GPU's eigenvalue error is read
+    if ref_eig_errors:
+        from bipp_b200.verify import eigenvalue_errors
+
+        d32, d64 = [], []
+        for k in range(n_eig_steps):
+            s = S[k].transpose(0, 1).cpu().numpy().T.astype(np.complex128)
+            x = xyz[k].cpu().numpy().astype(np.float32)
+            d32.append(ref.eigh_gram(wl, s.astype(np.complex64), w, x, dtype=np.float32)[1])
+            d64.append(ref.eigh_gram(wl, s, np.eye(N), x.astype(np.float64), dtype=np.float64)[1])
+        ref_err = eigenvalue_errors(np.array(d32, dtype=np.float64), np.array(d64), np.asarray(intervals))
+    else:
+        ref_err = None
     rate = 1.0 / (per_entry * cfg.n_channels)
     desc = (f"eigh_gram<float>+virtual_vis<float>x{len(intervals)} measured on {n_eig_steps} entries, median "
             f"{per_entry:.3f} s/entry (eigh_gram {np.median(t_eig):.3f}, virtual_vis {np.median(t_vv):.4f}); "
             f"{cfg.n_channels} entries per time step; NUFFT stage not included (neonufft unavailable)")
     extras = {"eig_vv_s_per_entry": per_entry}
+    if ref_err:
+        extras["reference_fp32_eig_errors"] = ref_err
     if nufft:
         vvs, x = last
         uvw = sim.baseline_uvw(obs, x).astype(np.float64) * (2 * math.pi / wl)
@@ -386,7 +405,7 @@ def main():
     n = cfg.image_size
     pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
                        tolerance=cfg.eps, chunk_steps=min(args.chunk_steps, S.shape[0]), max_steps=S.shape[0],
-                       mode=args.mode)
+                       mode=args.mode, vv_precision=args.vv_precision if args.mode == "batched" else "fp32")
     T = S.shape[0]  # entries: time steps x channels
     S_bytes = S.numel() * 8
     T_steps = cfg.n_steps
@@ -453,7 +472,7 @@ def main():
         sel = torch.arange(0, T, stride, device=device)[:args.check_steps]
         parity = verify.check_batch(ctx, S[sel].contiguous(), xyz[sel].contiguous(), wl[sel].contiguous(), obs, n,
                                     intervals, cfg.eps, n_pix=args.check_pixels,
-                                    chunk_steps=min(args.chunk_steps, len(sel)))
+                                    chunk_steps=min(args.chunk_steps, len(sel)), vv_precision=args.vv_precision)
         parity["reference"] = ("FP64: bipp_eigh_gram_batched_d + FP64 V diag(d) V^H + direct sum with FP64 phase "
                                "and trigonometry (the library's FP64 pieces pinned to the compiled reference)")
 
@@ -463,7 +482,7 @@ def main():
     if rank == 0 and args.plain_steps > 0 and args.mode == "batched":
         ns = min(args.plain_steps * cfg.n_channels, T)
         pp = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lattice_of(obs, n), obs.lmn[:, 2], obs.basis,
-                           tolerance=cfg.eps, chunk_steps=1, max_steps=ns, mode="plain")
+                           tolerance=cfg.eps, chunk_steps=1, max_steps=ns, mode="plain", vv_precision="fp32")
         pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())  # warm-up
         pp.reset()
         torch.cuda.synchronize()
@@ -510,7 +529,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             Sc = S_h if not args.no_e2e else S  # noqa: F821
-            v, cores, desc, extra = cpu_reference_sample(cfg, Sc, xyz, intervals, wl=float(wl[0].item()))
+            v, cores, desc, extra = cpu_reference_sample(cfg, Sc, xyz, intervals, wl=float(wl[0].item()),
+                                                         ref_eig_errors=True)
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc,
                    "stages": "eigh_gram + virtual_vis", **extra}
         except Exception as e:  # reported, not fatal
@@ -524,6 +544,7 @@ def main():
                 "data": "synthetic (seeded observation of the workload's shape, generated on the GPU)",
                 "config": {"workload": workload_text(args),
                            "time_steps_per_batch": T_steps, "entries_per_batch": T, "mode": args.mode,
+                           "vv_precision": args.vv_precision if args.mode == "batched" else "fp32",
                            "parallelism": f"dp{world} (steps)",
                            "l2": f"inputs ({S_bytes / 1e9:.1f} GB/batch) larger than L2; no flush"},
                 "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,

@@ -46,7 +46,7 @@ class DatasetCallbacks(C.Structure):
 class PipelineConfig(C.Structure):
     _fields_ = [("nAntenna", _sz), ("nLevels", _sz), ("intervals", _pd), ("filter", _i), ("tolerance", _d),
                 ("gridA", _sz), ("gridB", _sz), ("lattice", _d * 6), ("pixelN", _pd), ("uvwBasis", _pd),
-                ("chunkSteps", _sz), ("maxSteps", _sz), ("mode", _i)]
+                ("chunkSteps", _sz), ("maxSteps", _sz), ("mode", _i), ("vvPrecision", _i)]
 
 
 # symbol -> argtypes (all return BippError as int unless listed in _RESTYPE)

@@ -631,6 +631,8 @@ def _synthesize(ctx: Context, opt: NufftSynthesisOptions, dataset, selection, ta
 # --- batched pipeline ---------------------------------------------------------------------
 
 _FILTERS = {"lsq": 0, "std": 1, "sqrt": 2, "inv": 3, "inv_sqrt": 4}
+# arithmetic of the virtual-visibility products (bipp_pipeline_config.vvPrecision)
+VV_PRECISION = {"tf32x3": 0, "bf16x3": 1, "fp32": 2, "fp64": 3}
 
 
 class Pipeline:
@@ -641,10 +643,12 @@ class Pipeline:
     l = l0 + a A_l + b B_l, m = m0 + a A_m + b B_m; pixel_n: [gridA * gridB] FP64;
     uvw_basis: 3x3 (columns U, V, W in the frame of the positions);
     intervals: [nLevels, 2]; mode "batched" (one NUFFT per call) or "plain" (one NUFFT
-    per step and level)."""
+    per step and level); vv_precision: arithmetic of VV = X diag(s) X^H, "tf32x3" or
+    "bf16x3" (tensor cores, split operands, FP32 accumulation), "fp32" (CUDA cores) or
+    "fp64"."""
 
     def __init__(self, ctx: Context, n_antenna: int, intervals, lattice, pixel_n, uvw_basis, tolerance=1e-5,
-                 filter="lsq", chunk_steps=256, max_steps=0, mode="batched"):
+                 filter="lsq", chunk_steps=256, max_steps=0, mode="batched", vv_precision="tf32x3"):
         self.ctx = ctx
         self.n_antenna = int(n_antenna)
         self.intervals = np.ascontiguousarray(intervals, dtype=np.float64).reshape(-1, 2)
@@ -666,6 +670,7 @@ class Pipeline:
         cfg.chunkSteps = int(chunk_steps)
         cfg.maxSteps = int(max_steps)
         cfg.mode = 0 if mode == "batched" else 1
+        cfg.vvPrecision = VV_PRECISION[vv_precision]
         h = C.c_void_p()
         check(ctx._lib.bipp_pipeline_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self.handle = h

@@ -19,6 +19,7 @@
 #include "eig.hpp"
 #include "eig_kernels.cuh"
 #include "nufft.hpp"
+#include "vv_tc.cuh"
 
 namespace bippb200 {
 
@@ -117,7 +118,7 @@ using namespace bippb200;
 struct bipp_pipeline_s {
   bipp_ctx_s* ctx = nullptr;
   size_t nAnt = 0, nLevels = 0, chunk = 256, maxSteps = 0;
-  int filter = 0, mode = 0;
+  int filter = 0, mode = 0, vvPrecision = 0;
   double tol = 1e-5;
   long long P = 0;
   std::vector<double> intervals;
@@ -200,16 +201,42 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
                                                p->kend.get<int>() + s0 * L);
     B2_CHECK_LAUNCH();
     // VV[b][l] lower triangle = X diag(kscale) X^H over the level's eigenvalue range
-    GemmArgs<float2> g{};
-    g.A = X; g.strideA = n2; g.lda = N; g.opA = 0;
-    g.B = X; g.strideB = n2; g.ldb = N; g.opB = 1;
-    g.Cm = p->vv.get<float2>(); g.strideC = n2 * L; g.ldc = N; g.strideCLevel = n2;
-    g.n = p->nred.get<int>() + s0; g.outMode = 2; g.levels = L;
-    g.kscale = p->kscale.get<float>() + (long long)s0 * N; g.strideK = N;
-    g.kbeg = p->kbeg.get<int>() + s0 * L; g.kend = p->kend.get<int>() + s0 * L;
-    const int tiles = (N + kGemmBM - 1) / kGemmBM;
-    count_launch();
-    gemm_kernel<float2, float><<<dim3(tiles, tiles, nb * L), kGemmThreads, 0, ctx->stream>>>(g);
+    if (p->vvPrecision == 2) {
+      GemmArgs<float2> g{};
+      g.A = X; g.strideA = n2; g.lda = N; g.opA = 0;
+      g.B = X; g.strideB = n2; g.ldb = N; g.opB = 1;
+      g.Cm = p->vv.get<float2>(); g.strideC = n2 * L; g.ldc = N; g.strideCLevel = n2;
+      g.n = p->nred.get<int>() + s0; g.outMode = 2; g.levels = L;
+      g.kscale = p->kscale.get<float>() + (long long)s0 * N; g.strideK = N;
+      g.kbeg = p->kbeg.get<int>() + s0 * L; g.kend = p->kend.get<int>() + s0 * L;
+      const int tiles = (N + kGemmBM - 1) / kGemmBM;
+      count_launch();
+      gemm_kernel<float2, float><<<dim3(tiles, tiles, nb * L), kGemmThreads, 0, ctx->stream>>>(g);
+    } else {
+      VvArgs v{};
+      v.X = X; v.strideX = n2; v.ldx = N;
+      v.kscale = p->kscale.get<float>() + (long long)s0 * N; v.strideK = N;
+      v.kbeg = p->kbeg.get<int>() + s0 * L; v.kend = p->kend.get<int>() + s0 * L;
+      v.n = p->nred.get<int>() + s0;
+      v.VV = p->vv.get<float2>(); v.strideStep = n2 * L; v.strideLevel = n2; v.ldv = N;
+      v.nSteps = nb; v.nLevels = L;
+      v.status = p->status.get<int>() + s0;
+      if (p->vvPrecision == 3) {
+        const int tiles = (N + kVv64Tile - 1) / kVv64Tile;
+        v.tilesI = v.tilesJ = tiles;
+        count_launch();
+        vv_fp64_kernel<<<dim3(tiles, tiles, nb * L), kVv64Threads, 0, ctx->stream>>>(v);
+      } else {
+        v.tilesI = (N + kVvM - 1) / kVvM;
+        v.tilesJ = (N + kVvNC - 1) / kVvNC;
+        const long long items = (long long)nb * L * v.tilesI * v.tilesJ;
+        const int grid = (int)std::max<long long>(1, std::min<long long>(items, 3LL * ctx->smCount));
+        auto k = p->vvPrecision == 0 ? vv_tc_kernel<1> : vv_tc_kernel<2>;
+        smem_optin(k, VvShape<1>::Smem);
+        count_launch();
+        k<<<grid, kVvThreads, VvShape<1>::Smem, ctx->stream>>>(v);
+      }
+    }
     B2_CHECK_LAUNCH();
   }
   // zero baselines (r == s) of the levels in this transform
@@ -440,6 +467,8 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
     p->chunk = cfg->chunkSteps ? cfg->chunkSteps : 256;
     p->filter = cfg->filter;
     p->mode = cfg->mode;
+    require(cfg->vvPrecision >= 0 && cfg->vvPrecision <= 3, "unknown virtual-visibility precision");
+    p->vvPrecision = cfg->vvPrecision;
     p->tol = cfg->tolerance > 0 ? cfg->tolerance : 1e-5;
     p->intervals.assign(cfg->intervals, cfg->intervals + 2 * cfg->nLevels);
     Lattice lat;

@@ -78,11 +78,15 @@ def fp64_level_images(ctx, s_logical, xyz, wl, basis, intervals, lmn_pix, chunk=
 
 def eigenvalue_errors(d_pipe, d64, intervals):
     """Errors of the pipeline's eigenvalues inside the level range [min lo, max hi]
-    against the FP64 ones: (max per-eigenvalue relative error, max normwise error,
-    number of eigenvalues compared). Eigenvalues within 1e-6 max|d| of a range edge are
-    left out (FP32 may place them on the other side)."""
+    against the FP64 ones: max per-eigenvalue relative error |d - d64| / |d64| over all of
+    them and over those with |d64| >= 1e-2 max|d64| of their step, the max normwise error
+    |d - d64| / max|d64|, and the number compared. An FP32 solver's eigenvalue error is of
+    the order of eps32 times the norm, so the relative error of the smallest eigenvalues
+    is larger by max|d| / |d| (the reference's own FP32 path, chegv, shows the same).
+    Eigenvalues within 1e-6 max|d| of a range edge are left out (FP32 may place them on
+    the other side)."""
     lo, hi = float(intervals[:, 0].min()), float(intervals[:, 1].max())
-    per, norm, n = 0.0, 0.0, 0
+    per, large, norm, n = 0.0, 0.0, 0.0, 0
     for b in range(d64.shape[0]):
         ref = d64[b]
         scale = np.abs(ref).max()
@@ -93,14 +97,19 @@ def eigenvalue_errors(d_pipe, d64, intervals):
         if not sel.any():
             continue
         diff = np.abs(d_pipe[b][sel] - ref[sel])
-        per = max(per, float((diff / np.abs(ref[sel])).max()))
+        rel = diff / np.abs(ref[sel])
+        per = max(per, float(rel.max()))
+        big = np.abs(ref[sel]) >= 1e-2 * scale
+        if big.any():
+            large = max(large, float(rel[big].max()))
         norm = max(norm, float(diff.max() / scale))
         n += int(sel.sum())
-    return per, norm, n
+    return {"eig_rel_err_max": per, "eig_rel_err_max_above_1e-2": large, "eig_rel_err_normwise": norm,
+            "eigenvalues_compared": n}
 
 
 def check_batch(ctx, S_cm, xyz, wl, obs, image_size, intervals, tolerance, n_pix=512, seed=33, chunk_steps=None,
-                filter="lsq"):
+                filter="lsq", vv_precision="tf32x3"):
     """Image the steps of S_cm (torch device tensor [B, N, N], each step's S in
     column-major order, complex64), xyz (torch [B, N, 3] float64), wl (torch [B] float64)
     with the FP32 pipeline and with the FP64 pieces; returns a dict of errors and the
@@ -114,7 +123,7 @@ def check_batch(ctx, S_cm, xyz, wl, obs, image_size, intervals, tolerance, n_pix
     B, N = S_cm.shape[0], S_cm.shape[1]
     n = image_size
     pl = Pipeline(ctx, N, intervals, _lattice(obs.lmn, n), obs.lmn[:, 2], obs.basis, tolerance=tolerance,
-                  chunk_steps=chunk_steps or B, max_steps=B)
+                  chunk_steps=chunk_steps or B, max_steps=B, vv_precision=vv_precision)
     pl.process_device(B, S_cm.data_ptr(), xyz.data_ptr(), wl.data_ptr())
     img = pl.images()
     stats = pl.nufft_stats()
@@ -127,7 +136,8 @@ def check_batch(ctx, S_cm, xyz, wl, obs, image_size, intervals, tolerance, n_pix
                                  obs.lmn[pix])
     got = img[:, pix].astype(np.float64)
     err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    per, norm, n_eig = eigenvalue_errors(d_pipe, d64, np.asarray(intervals))
-    return {"image_rel_l2": err, "eig_rel_err_max": per, "eig_rel_err_normwise": norm, "eigenvalues_compared": n_eig,
-            "steps": int(B), "pixels": int(n_pix), "split_tiles": stats["split_tiles"], "slabs": stats["slabs"],
-            "points": stats["points"]}
+    out = {"image_rel_l2": err}
+    out.update(eigenvalue_errors(d_pipe, d64, np.asarray(intervals)))
+    out.update({"steps": int(B), "pixels": int(n_pix), "split_tiles": stats["split_tiles"], "slabs": stats["slabs"],
+                "points": stats["points"]})
+    return out

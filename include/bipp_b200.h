@@ -257,6 +257,10 @@ typedef struct {
   size_t chunkSteps;      /* steps per eigensolver launch sequence (0 = 256) */
   size_t maxSteps;        /* maximum steps per process() call */
   int mode;               /* 0 batched (one NUFFT per call), 1 plain (one NUFFT per step and level) */
+  int vvPrecision;        /* arithmetic of the virtual-visibility products VV = X diag(s) X^H
+                             (src/host/virtual_vis.cpp:52-68): 0 3xTF32 and 1 BF16x3 (tensor
+                             cores, split operands, FP32 accumulation), 2 FP32 (CUDA cores),
+                             3 FP64 (CUDA cores; for precision studies) */
 } bipp_pipeline_config;
 
 BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg,

@@ -26,8 +26,10 @@ from oracle import ref
 pytestmark = pytest.mark.gpu
 
 
-def _image_error(ctx, cfg, entries, n_pix, chunk):
-    """entries: (time step, channel) pairs, all imaged in one pipeline batch."""
+def _image_error(ctx, cfg, entries, n_pix, chunk, modes=None):
+    """entries: (time step, channel) pairs, all imaged in one pipeline batch. With
+    `modes` (virtual-visibility precisions) the error of each mode is returned as a dict,
+    the oracle computed once."""
     import bipp_b200 as bipp
     from bipp_b200 import simulate as sim
 
@@ -53,10 +55,13 @@ def _image_error(ctx, cfg, entries, n_pix, chunk):
     l = lmn[:, 0].reshape(n, n)
     m = lmn[:, 1].reshape(n, n)
     lattice = (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
-    pl = bipp.Pipeline(ctx, N, intervals, lattice, lmn[:, 2], obs.basis, tolerance=cfg.eps, chunk_steps=chunk)
-    pl.process(s, xyz, wl)
-    img = pl.images()
-    pl.close()
+    imgs = {}
+    for mode in (modes or ("tf32x3",)):
+        pl = bipp.Pipeline(ctx, N, intervals, lattice, lmn[:, 2], obs.basis, tolerance=cfg.eps, chunk_steps=chunk,
+                           vv_precision=mode)
+        pl.process(s, xyz, wl)
+        imgs[mode] = pl.images()
+        pl.close()
     # oracle on a pixel subset
     pix = np.random.default_rng(33).choice(lmn.shape[0], n_pix, replace=False)
     x, y, z = lmn[pix, 0], lmn[pix, 1], lmn[pix, 2]
@@ -69,8 +74,8 @@ def _image_error(ctx, cfg, entries, n_pix, chunk):
             vv = bb.virtual_vis(sc, dl, v).reshape(-1, order="F")
             ref.nuft_sum(1.0, vv, b[:, 0], b[:, 1], b[:, 2], x, y, z, out=out[lv])
     out /= len(entries)
-    got = img[:, pix].astype(np.float64)
-    return np.linalg.norm(got - out) / np.linalg.norm(out)
+    errs = {m: np.linalg.norm(img[:, pix].astype(np.float64) - out) / np.linalg.norm(out) for m, img in imgs.items()}
+    return errs if modes else errs["tf32x3"]
 
 
 @pytest.mark.skipif(not ref.available(), reason="compiled reference oracle not built")
@@ -83,10 +88,19 @@ def test_pipeline_image_error_at_benchmark_shape(ctx):
 
 @pytest.mark.skipif(not ref.available(), reason="compiled reference oracle not built")
 def test_pipeline_image_error_precision_study(ctx):
+    """The precision study (550 antennas, 8 levels, 4096^2 px, tolerance 1e-6, 16,384
+    random pixels, seed 33): the virtual-visibility products in FP64, 3xTF32 and BF16x3 on
+    the tensor cores, and FP32 on the CUDA cores; every mode's image within 1e-4 relative
+    L2 of the FP64 oracle, and the split tensor-core modes within 2x of the FP64 mode's
+    error (what the rest of the FP32 pipeline leaves) plus 1e-5."""
     from bipp_b200 import simulate as sim
 
-    err = _image_error(ctx, sim.config_c3(), [(0, 0)], 16384, 1)
-    assert err <= 1e-4, err
+    errs = _image_error(ctx, sim.config_c3(), [(0, 0)], 16384, 1, modes=("fp64", "tf32x3", "bf16x3", "fp32"))
+    print("precision study image errors:", {m: f"{e:.3e}" for m, e in errs.items()})
+    for m, e in errs.items():
+        assert e <= 1e-4, (m, errs)
+    for m in ("tf32x3", "bf16x3"):
+        assert errs[m] <= 2 * errs["fp64"] + 1e-5, errs
 
 
 @pytest.mark.skipif(not ref.available(), reason="compiled reference oracle not built")
@@ -156,8 +170,10 @@ def test_pipeline_image_error_benchmark_batch(ctx):
     imaged as one batch, as the benchmark does: the NUFFT splits heavy tiles into parts
     that accumulate with atomics and processes the w axis in several slabs (both asserted
     from the pipeline's statistics); image error at 512 random pixels <= 1e-4 relative
-    L2 against the FP64 check, and the eigenvalues inside the level range within 1e-4
-    (per eigenvalue, relative) and 1e-5 (normwise) of FP64."""
+    L2 against the FP64 check; the eigenvalues inside the level range within 1e-5 of FP64
+    normwise and, for those above 1e-2 of their step's largest, per eigenvalue (relative;
+    the smaller ones carry the FP32 solver's absolute error, as the reference's own FP32
+    path does, and are covered by the normwise bound)."""
     import bipp_b200 as bipp
     from bipp_b200 import simulate as sim
     from bipp_b200 import verify
@@ -173,4 +189,4 @@ def test_pipeline_image_error_benchmark_batch(ctx):
     assert r["split_tiles"] > 0 and r["slabs"] > 1, r
     assert r["image_rel_l2"] <= 1e-4, r
     assert r["eig_rel_err_normwise"] <= 1e-5, r
-    assert r["eig_rel_err_max"] <= 1e-4, r
+    assert r["eig_rel_err_max_above_1e-2"] <= 1e-5, r
