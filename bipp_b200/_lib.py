@@ -64,6 +64,12 @@ SIGNATURES = {
     "bipp_eigh_d": [_p, _d, _sz, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _psz, _pd],
     "bipp_eigh_gram_batched_s": [_p, _sz, _sz, _p, _p, _p, _p, _p, _p, _p],
     "bipp_eigh_gram_batched_d": [_p, _sz, _sz, _p, _p, _p, _p, _p, _p, _p],
+    "bipp_eigh_gram_batched_ranked_s": [_p, _sz, _sz, _p, _p, _p, _d, _i, _p, _i, _d, _p, _p, _p, _p, _p, _p, _p],
+    "bipp_rank_features_s": [_p, _sz, _sz, _p, _p, _p, _d, _p, _p],
+    "bipp_rank_mlp_num_params": [],
+    "bipp_rank_mlp_forward": [_p, _p, _p, _sz, _p],
+    "bipp_rank_mlp_gradient": [_p, _p, _p, _p, _sz, _p, _p],
+    "bipp_rank_mlp_train": [_p, _p, _p, _p, _sz, _i, _f, _p],
     "bipp_eigh_gram_noalloc_s": [_i, _p, _f, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _p, _p, _p],
     "bipp_gram_matrix_s": [_p, _sz, _sz, _p, _sz, _p, _sz, _f, _p, _sz],
     "bipp_gram_matrix_d": [_p, _sz, _sz, _p, _sz, _p, _sz, _d, _p, _sz],

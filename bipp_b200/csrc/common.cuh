@@ -43,6 +43,8 @@ enum StatusBits : int {
   kStatusNonFinite = 2,       // NaN/Inf in an entry of S that enters the reduced matrix
   kStatusClusterFix = 4,      // eigenvector cluster re-orthogonalised (informational)
   kStatusTensorTimeout = 8,   // a tensor-core MMA completion wait ran out (GPU error)
+  kStatusRankFallback = 16,   // predicted partial solve fell back to the full solve (informational)
+  kStatusResidual = 32,       // an eigenpair residual above the requested tolerance
 };
 
 // ---- complex helpers --------------------------------------------------------------

@@ -8,6 +8,7 @@
 
 #include "context.hpp"
 #include "eig.hpp"
+#include "rank_mlp.cuh"
 #include "eig_kernels.cuh"
 #include "gemm_tc.cuh"
 
@@ -299,6 +300,23 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     }
     B2_CHECK_LAUNCH();
   }
+  // rank predictor: features of the whitened matrix, MLP, predicted counts
+  if (L.features) {
+    const size_t smem = 2 * (size_t)Nmax * sizeof(float);
+    auto k = rank_features_kernel<C>;
+    smem_optin(k, smem);
+    count_launch();
+    k<<<nb, kFeatThreads, smem, st>>>(A, Nmax, nred, L.featThreshold, L.features);
+    B2_CHECK_LAUNCH();
+    if (L.mlpModel) {
+      count_launch();
+      mlp_forward_kernel<<<(nb + kMlpTile - 1) / kMlpTile, kMlpThreads, 0, st>>>(L.mlpModel, L.features, nb,
+                                                                               L.mlpOut, nullptr, nullptr);
+      count_launch();
+      rank_predk_kernel<<<(nb + 255) / 256, 256, 0, st>>>(nb, L.mlpOut, nred, L.predK);
+      B2_CHECK_LAUNCH();
+    }
+  }
   // 3. tridiagonalisation
   mark(4);
   {
@@ -325,7 +343,8 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     count_launch();
     k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
-                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues, sizeOrder);
+                                     L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues, sizeOrder,
+                                     L.mlpModel ? L.predK : nullptr, L.predMargin, L.resTol);
     B2_CHECK_LAUNCH();
   }
   // 5. back-transform Y = Q Z -> T1
@@ -538,10 +557,23 @@ static void eigh_host(bipp_ctx_s* ctx, bool gram, T wl, size_t nAntenna, size_t 
   *scale = nvis ? T(1) / T(nvis) : T(0);
 }
 
-// batched eigh_gram, W = I
+// columns of v (nAnt x nAnt) outside the computed eigenvector range [kLo, kHi) of the
+// matrix (the ranked solves compute part of the eigenpairs) set to zero
+__global__ void zero_outside_range_kernel(int nAnt, const int* __restrict__ krange, float2* __restrict__ v) {
+  const int kLo = krange[0], kHi = krange[1];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)nAnt * nAnt;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / nAnt);
+    if (c < kLo || c >= kHi) v[e] = make_float2(0.f, 0.f);
+  }
+}
+
+// batched eigh_gram, W = I; with `ro` (single precision) the ranked forms: the full solve,
+// the exact range above a threshold (Sturm counts) or the predicted partial solve
 template <typename T>
 static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, const T* wl, const void* s,
-                                   const T* xyz, T* d, void* v, size_t* nBeamReduced, T* scale) {
+                                   const T* xyz, T* d, void* v, size_t* nBeamReduced, T* scale,
+                                   const RankOpts* ro = nullptr) {
   using C = typename Cplx<T>::type;
   require(nBatch > 0 && nAnt > 0, "empty problem");
   require(s && xyz && wl && d && nBeamReduced && scale, "null pointer", BIPP_INVALID_POINTER_ERROR);
@@ -563,12 +595,32 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
   DevBuf dS(ctx, chunk * n2 * sizeof(C)), dX(ctx, xyzh.size() * sizeof(double)), dWl(ctx, nBatch * sizeof(double));
   DevBuf dIdx(ctx, nBatch * Nmax * sizeof(int)), dNred(ctx, nBatch * sizeof(int)), dNvis(ctx, nBatch * sizeof(long long));
   DevBuf dStatus(ctx, nBatch * sizeof(int)), dLam(ctx, nBatch * Nmax * sizeof(double)), dLamPad(ctx, chunk * nAnt * sizeof(double));
-  DevBuf dOut(ctx, chunk * n2 * sizeof(C));
+  DevBuf dV(ctx, chunk * n2 * sizeof(C));
   h2d(ctx, dX.get(), xyzh.data(), xyzh.size() * sizeof(double));
   h2d(ctx, dWl.get(), wlh.data(), nBatch * sizeof(double));
   dStatus.zero();
   EigWork<T> work;
   work.reserve(ctx, (int)chunk, Nmax);
+  DevBuf dModel, dFeat, dOut, dPredK;
+  if (ro) {
+    require(ro->mode >= 0 && ro->mode <= 2, "unknown rank mode");
+    require(ro->mode != 2 || ro->modelHost, "the predicted partial solve needs a model", BIPP_INVALID_POINTER_ERROR);
+    require(ro->margin >= 0, "negative margin");
+    if (ro->mode == 2) {
+      dModel.alloc(ctx, kMlpParams * sizeof(float));
+      h2d(ctx, dModel.get(), ro->modelHost, kMlpParams * sizeof(float));
+      dOut.alloc(ctx, chunk * sizeof(float));
+      dPredK.alloc(ctx, chunk * sizeof(int));
+    }
+    if (ro->mode == 2 || ro->features) dFeat.alloc(ctx, chunk * kRankFeatures * sizeof(float));
+  }
+  std::vector<int> kr(2 * chunk);
+  cudaEvent_t evA = nullptr, evB = nullptr;
+  if (ro && ro->ms) {
+    B2_CUDA(cudaEventCreate(&evA));
+    B2_CUDA(cudaEventCreate(&evB));
+    *ro->ms = 0.0;
+  }
   std::vector<int> nredh(nBatch);
   std::vector<long long> nvish(nBatch);
   std::vector<int> stat(nBatch);
@@ -585,7 +637,37 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     L.idx = dIdx.get<int>(); L.nred = dNred.get<int>(); L.nvis = dNvis.get<long long>();
     L.status = dStatus.get<int>(); L.lam = dLam.get<double>();
     L.doFlag = 1; L.batchOffset = (int)b0;
+    if (ro) {
+      if (ro->mode >= 1) {
+        L.allValues = 0;
+        L.vecLo = ro->threshold;
+        L.vecHi = INFINITY;
+      }
+      if (ro->mode == 2 || ro->features) {
+        L.features = dFeat.get<float>();
+        L.featThreshold = ro->threshold;
+      }
+      if (ro->mode == 2) {
+        L.mlpModel = dModel.get<float>();
+        L.mlpOut = dOut.get<float>();
+        L.predK = dPredK.get<int>();
+        L.predMargin = ro->margin;
+        L.resTol = ro->resTol;
+      }
+      if (evA) B2_CUDA(cudaEventRecord(evA, ctx->stream));
+    }
     eig_launch<T>(ctx, L, work);
+    if (ro) {
+      if (evB) {
+        B2_CUDA(cudaEventRecord(evB, ctx->stream));
+        B2_CUDA(cudaEventSynchronize(evB));
+        float t = 0.f;
+        B2_CUDA(cudaEventElapsedTime(&t, evA, evB));
+        *ro->ms += t;
+      }
+      if (ro->features) d2h(ctx, ro->features + b0 * kRankFeatures, dFeat.get(), nb * kRankFeatures * sizeof(float));
+      d2h(ctx, kr.data(), work.krange.get(), 2 * nb * sizeof(int));
+    }
     // outputs for this chunk: scatter each matrix's eigenvectors to its kept antenna rows
     std::vector<int> nr(nb);
     d2h(ctx, nr.data(), dNred.get<int>() + b0, nb * sizeof(int));
@@ -595,7 +677,14 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
       unbeam_kernel<C><<<128, 256, 0, ctx->stream>>>((int)nAnt, (int)nAnt, nr[b],
                                                      work.X(true) + (long long)b * Nmax * Nmax, Nmax,
                                                      dIdx.get<int>() + (b0 + b) * Nmax, nullptr, 0, 1,
-                                                     dOut.get<C>() + b * n2);
+                                                     dV.get<C>() + b * n2);
+      if constexpr (sizeof(T) == 4) {
+        if (ro && ro->mode >= 1) {
+          count_launch();
+          zero_outside_range_kernel<<<128, 256, 0, ctx->stream>>>((int)nAnt, work.krange.template get<int>() + 2 * b,
+                                                                  dV.get<float2>() + b * n2);
+        }
+      }
     }
     B2_CHECK_LAUNCH();
     count_launch();
@@ -603,10 +692,14 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
                                                         dLam.get<double>() + b0 * Nmax, Nmax, dLamPad.get<double>());
     B2_CHECK_LAUNCH();
     d2h(ctx, lamh.data(), dLamPad.get(), nb * nAnt * sizeof(double));
-    if (v) d2h(ctx, static_cast<char*>(v) + b0 * n2 * sizeof(C), dOut.get(), nb * n2 * sizeof(C));
+    if (v) d2h(ctx, static_cast<char*>(v) + b0 * n2 * sizeof(C), dV.get(), nb * n2 * sizeof(C));
     sync(ctx);
     for (size_t i = 0; i < nb * nAnt; ++i) d[b0 * nAnt + i] = (T)lamh[i];
+    if (ro && ro->kComputed)
+      for (size_t b = 0; b < nb; ++b) ro->kComputed[b0 + b] = nr[b] ? kr[2 * b + 1] - kr[2 * b] : 0;
   }
+  if (evA) cudaEventDestroy(evA);
+  if (evB) cudaEventDestroy(evB);
   d2h(ctx, nredh.data(), dNred.get(), nBatch * sizeof(int));
   d2h(ctx, nvish.data(), dNvis.get(), nBatch * sizeof(long long));
   d2h(ctx, stat.data(), dStatus.get(), nBatch * sizeof(int));
@@ -618,6 +711,7 @@ static void eigh_gram_batched_host(bipp_ctx_s* ctx, size_t nBatch, size_t nAnt, 
     if (nredh[b] == 0) throw Error(BIPP_EIGENSOLVER_ERROR, "every row and column of S is flagged (empty eigenproblem)");
     nBeamReduced[b] = (size_t)nredh[b];
     scale[b] = nvish[b] ? T(1) / (T)nvish[b] : T(0);
+    if (ro && ro->fallback) ro->fallback[b] = (stat[b] & kStatusRankFallback) ? 1 : 0;
   }
 }
 
@@ -744,6 +838,44 @@ BippError bipp_eigh_gram_batched_d(bipp_ctx_t ctx, size_t nBatch, size_t nAntenn
   return guard([&] {
     require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
     eigh_gram_batched_host<double>(ctx, nBatch, nAntenna, wl, s, xyz, d, v, nBeamReduced, scale);
+  });
+}
+BippError bipp_eigh_gram_batched_ranked_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna, const float* wl,
+                                          const void* s, const float* xyz, double threshold, int mode,
+                                          const float* model, int margin, double residualTol, float* d, void* v,
+                                          size_t* nBeamReduced, float* scale, int* kComputed, int* fallback,
+                                          double* ms) {
+  return guard([&] {
+    require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
+    RankOpts ro;
+    ro.mode = mode;
+    ro.threshold = threshold;
+    ro.modelHost = model;
+    ro.margin = margin;
+    ro.resTol = residualTol;
+    ro.kComputed = kComputed;
+    ro.fallback = fallback;
+    ro.ms = ms;
+    eigh_gram_batched_host<float>(ctx, nBatch, nAntenna, wl, s, xyz, d, v, nBeamReduced, scale, &ro);
+  });
+}
+BippError bipp_rank_features_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna, const float* wl, const void* s,
+                               const float* xyz, double threshold, float* features, int* counts) {
+  return guard([&] {
+    require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
+    require(features && counts, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    RankOpts ro;
+    ro.mode = 0;
+    ro.threshold = threshold;
+    ro.features = features;
+    std::vector<float> d(nBatch * nAntenna), sc(nBatch);
+    std::vector<size_t> nr(nBatch);
+    eigh_gram_batched_host<float>(ctx, nBatch, nAntenna, wl, s, xyz, d.data(), nullptr, nr.data(), sc.data(), &ro);
+    for (size_t b = 0; b < nBatch; ++b) {
+      int c = 0;
+      for (size_t i = 0; i < nr[b]; ++i) c += (d[b * nAntenna + i] > threshold) ? 1 : 0;
+      counts[b] = c;
+    }
   });
 }
 BippError bipp_gram_matrix_s(bipp_ctx_t ctx, size_t nAntenna, size_t nBeam, const void* w, size_t ldw, const float* xyz,

@@ -53,9 +53,40 @@ struct EigLaunch {
   // optional per-kernel device time accumulation (ms): prep, cholesky, trinv, reduction
   // GEMMs, hetrd, tridiagonal eigenpairs, back-transform, Linv^H Y GEMM
   double* kernelMs = nullptr;
+  // rank predictor (optional): the features ([batch][64], device) of the whitened matrix,
+  // formed after the reduction with featThreshold as the energy threshold; with mlpModel
+  // (device) the MLP predicts the count of eigenvalues above vecLo (mlpOut [batch]
+  // fractions, predK [batch] counts) and the tridiagonal stage computes the largest
+  // predK + predMargin eigenpairs, falling back to all of them when the smallest computed
+  // value is still above vecLo or (resTol >= 0) a residual exceeds resTol |T|
+  float* features = nullptr;
+  double featThreshold = 0.0;
+  const float* mlpModel = nullptr;
+  float* mlpOut = nullptr;
+  int* predK = nullptr;
+  int predMargin = 16;
+  double resTol = -1.0;
 };
 
 constexpr int kEigTimers = 8;
+
+// options of the ranked batched eigh_gram (single precision): mode 0 computes every
+// eigenpair, 1 those above `threshold` (exact index range by Sturm counts), 2 the largest
+// k + margin with k predicted by the MLP `modelHost` (host, kMlpParams floats), falling
+// back to every eigenpair when needed; optional outputs per step: the features
+// ([nBatch][64]), the number of eigenvectors computed, the fallback flag, and the
+// device time of the eigensolver launches
+struct RankOpts {
+  int mode = 0;
+  double threshold = 0.0;
+  const float* modelHost = nullptr;
+  int margin = 16;
+  double resTol = -1.0;
+  float* features = nullptr;
+  int* kComputed = nullptr;
+  int* fallback = nullptr;
+  double* ms = nullptr;
+};
 
 template <typename T>
 void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w);

@@ -1230,7 +1230,8 @@ __global__ void __launch_bounds__(kTriThreads)
 tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, const int* __restrict__ nred,
                int Nmax, double* __restrict__ lamOut, R* __restrict__ Z, double* __restrict__ work,
                int* __restrict__ status, double vecLo = -INFINITY, double vecHi = INFINITY,
-               int* __restrict__ krange = nullptr, int allValues = 1, const int* __restrict__ order = nullptr) {
+               int* __restrict__ krange = nullptr, int allValues = 1, const int* __restrict__ order = nullptr,
+               const int* __restrict__ predK = nullptr, int predMargin = 16, double resTol = -1.0) {
   const int b = order ? order[blockIdx.x] : blockIdx.x;
   const int n = nred[b];
   if (n <= 0) return;
@@ -1267,11 +1268,15 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
   const double pivmin = 2.2250738585072014e-308 * fmax(1.0, emax);
   lo -= 2.0 * eps * tnorm + 4.0 * pivmin;
   hi += 2.0 * eps * tnorm + 4.0 * pivmin;
-  // index range of the eigenvalues to compute
+  // index range of the eigenvalues to compute: all; those in [vecLo, vecHi] (two Sturm
+  // counts); or, with a predicted count predK of eigenvalues above vecLo, the largest
+  // predK + predMargin (a partial solve sized by the rank predictor, no Sturm count)
   __shared__ int s_vlo, s_vhi;
   if (threadIdx.x == 0) {
     int a = 0, c = n;
-    if (!allValues) {
+    if (predK) {
+      a = max(0, n - max(0, predK[b]) - predMargin);
+    } else if (!allValues) {
       if (vecLo > lo) a = min(n, sturm_count(d, e2, n, vecLo, pivmin));
       if (vecHi < hi) c = max(a, min(n, sturm_count(d, e2, n, vecHi, pivmin)));
     }
@@ -1279,8 +1284,11 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
     s_vhi = c;
   }
   __syncthreads();
-  const int vLo = s_vlo, vHi = s_vhi;
-  if (!allValues) {
+  int vLo = s_vlo;
+  const int vHi = s_vhi;
+  if (predK) {
+    for (int i = threadIdx.x; i < vLo; i += blockDim.x) lam[i] = 0.0;
+  } else if (!allValues) {
     if (vecLo > lo) lo = vecLo - (2.0 * eps * fabs(vecLo) + 4.0 * pivmin);
     if (vecHi < hi) hi = vecHi + (2.0 * eps * fabs(vecHi) + 4.0 * pivmin);
     for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -1298,13 +1306,31 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
     lam[i] = 0.5 * (a + c);
   }
   __syncthreads();
+  if (predK && vLo > 0 && lam[vLo] >= vecLo) {
+    // the smallest computed (last Ritz) value is still above the threshold, so
+    // eigenvalues above it may be missing: fall back to the full solve (all eigenpairs)
+    if (threadIdx.x == 0) atomicOr(status + b, (int)kStatusRankFallback);
+    for (int i = threadIdx.x; i < vLo; i += blockDim.x) {
+      double a = lo, c = hi;
+      for (int it = 0; it < 128; ++it) {
+        const double mid = 0.5 * (a + c);
+        if (mid <= a || mid >= c) break;
+        if (c - a <= fmax(2.0 * eps * fmax(fabs(a), fabs(c)), eps * tnorm) + pivmin) break;
+        if (sturm_count(d, e2, n, mid, pivmin) > i) c = mid; else a = mid;
+      }
+      lam[i] = 0.5 * (a + c);
+    }
+    vLo = 0;
+    __syncthreads();
+  }
   for (int i = threadIdx.x; i < n; i += blockDim.x) lamOut[(long long)b * Nmax + i] = lam[i];
-  // eigenvalue index range of the requested eigenvectors (lam ascending)
+  // eigenvalue index range of the requested eigenvectors (lam ascending); the partial
+  // solve returns the vectors of every value it computed
   __shared__ int s_klo, s_khi;
   if (threadIdx.x == 0) {
     int a = vLo, c = vHi;
-    while (a < c && lam[a] < vecLo) ++a;
-    while (c > a && lam[c - 1] > vecHi) --c;
+    while (!predK && a < c && lam[a] < vecLo) ++a;
+    while (!predK && c > a && lam[c - 1] > vecHi) --c;
     s_klo = a;
     s_khi = c;
     if (krange) {
@@ -1313,7 +1339,8 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
     }
   }
   __syncthreads();
-  const int kLo = s_klo, kHi = s_khi;
+  int kLo = s_klo;
+  const int kHi = s_khi;
 
   // twisted factorisation eigenvectors
   double* Lp = work + (long long)b * 2 * Nmax * Nmax;
@@ -1323,7 +1350,8 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
     if (i >= kLo && i < kHi) continue;
     for (int k = 0; k < n; ++k) Zb[(long long)k * Nmax + i] = R(0);
   }
-  for (int i = kLo + threadIdx.x; i < kHi; i += blockDim.x) {
+  auto twisted = [&](int iBeg, int iEnd) {
+  for (int i = iBeg + threadIdx.x; i < iEnd; i += blockDim.x) {
     const double l = lam[i];
     // top-down stationary factorisation T - l = L+ D+ L+^T
     double dp = d[0] - l;
@@ -1399,7 +1427,49 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
       Zb[(long long)k * Nmax + i] = (R)(zk * inv);
     }
   }
+  };
+  twisted(kLo, kHi);
   __syncthreads();
+  // partial solve: residual check of the computed pairs, |T z - lam z|_inf <= resTol |T|
+  // |z|_inf; a larger residual falls back to the full solve (the remaining pairs, which
+  // the full solve computes the same way)
+  if (predK && resTol >= 0.0 && kLo > 0) {
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    for (int i = kLo + threadIdx.x; i < kHi; i += blockDim.x) {
+      double res = 0.0, zmax = 0.0;
+      for (int k = 0; k < n; ++k) {
+        const double zk = (double)Zb[(long long)k * Nmax + i];
+        double tz = d[k] * zk;
+        if (k > 0) tz += e[k - 1] * (double)Zb[(long long)(k - 1) * Nmax + i];
+        if (k < n - 1) tz += e[k] * (double)Zb[(long long)(k + 1) * Nmax + i];
+        res = fmax(res, fabs(tz - lam[i] * zk));
+        zmax = fmax(zmax, fabs(zk));
+      }
+      if (!(res <= resTol * tnorm * zmax)) atomicOr(&s_bad, 1);
+    }
+    __syncthreads();
+    if (s_bad) {
+      if (threadIdx.x == 0) atomicOr(status + b, (int)(kStatusResidual | kStatusRankFallback));
+      for (int i = threadIdx.x; i < kLo; i += blockDim.x) {
+        double a = lo, c = hi;
+        for (int it = 0; it < 128; ++it) {
+          const double mid = 0.5 * (a + c);
+          if (mid <= a || mid >= c) break;
+          if (c - a <= fmax(2.0 * eps * fmax(fabs(a), fabs(c)), eps * tnorm) + pivmin) break;
+          if (sturm_count(d, e2, n, mid, pivmin) > i) c = mid; else a = mid;
+        }
+        lam[i] = 0.5 * (a + c);
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < kLo; i += blockDim.x) lamOut[(long long)b * Nmax + i] = lam[i];
+      twisted(0, kLo);
+      kLo = 0;
+      if (threadIdx.x == 0 && krange) krange[2 * b] = 0;
+      __syncthreads();
+    }
+  }
   // re-orthogonalise tight clusters (relative gap below 1e-10 of |T|): modified
   // Gram-Schmidt inside each cluster, in eigenvalue order.
   const double ctol = 1e-10 * fmax(tnorm, 1e-300);

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kVvThreads, 3) vv_tc_kernel(VvArgs a) {
 // threads with 4 x 4 outputs each, k staged 16 at a time in shared memory.
 constexpr int kVv64Tile = 64, kVv64K = 16, kVv64Threads = 256;
 
-__global__ void __launch_bounds__(kVv64Threads) vv_fp64_kernel(VvArgs a) {
+static __global__ void __launch_bounds__(kVv64Threads) vv_fp64_kernel(VvArgs a) {
   const int z = blockIdx.z;
   const int b = z / a.nLevels, lvl = z % a.nLevels;
   const int n = a.n[b];

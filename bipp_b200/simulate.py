@@ -103,6 +103,69 @@ def config_c5(**kw) -> SimConfig:
     return dataclasses.replace(c, **kw)
 
 
+def config_c4(**kw) -> SimConfig:
+    """Learned rank predictor: 256 antennas in a 10 km disc, 10,000 time steps, each with
+    its own sky of 5-200 sources (0.01-10 Jy) within 8 deg and its own noise level,
+    log-uniform in 0.001-0.1 (c4_step_sky); n_src is the largest source count."""
+    c = SimConfig(name="c4_n256_rank", n_antenna=256, layout="disc", extent_m=10000.0,
+                  z_spread_m=10.0, wl=2.0, n_steps=10000, dt_s=8.0, n_src=200, flux=(0.01, 10.0),
+                  src_radius_deg=8.0, noise_sigma=0.01, n_levels=4, image_size=256,
+                  fov_deg=16.0, eps=1e-5, keep=None, seed=4, double=False)
+    return dataclasses.replace(c, **kw)
+
+
+C4_SOURCES = (5, 200)
+C4_SIGMA = (0.001, 0.1)
+
+
+def c4_step_sky(obs: "Observation", step: int):
+    """Sky and noise level of one step of the rank-predictor workload: Q ~ U{5..200}
+    sources uniform on the cap of radius src_radius_deg, log-uniform fluxes, and sigma
+    log-uniform in [0.001, 0.1]. Returns (directions (Q, 3), fluxes (Q,), sigma)."""
+    cfg = obs.cfg
+    rng = np.random.default_rng([cfg.seed, 4000, int(step)])
+    q = int(rng.integers(C4_SOURCES[0], C4_SOURCES[1] + 1))
+    cos_rho = math.cos(math.radians(cfg.src_radius_deg))
+    ca = rng.uniform(cos_rho, 1.0, q)
+    sa = np.sqrt(1 - ca ** 2)
+    az = rng.uniform(0, 2 * np.pi, q)
+    dirs = np.stack([sa * np.cos(az), sa * np.sin(az), ca], axis=1) @ obs.basis.T
+    flux = np.exp(rng.uniform(np.log(cfg.flux[0]), np.log(cfg.flux[1]), q))
+    sigma = float(np.exp(rng.uniform(np.log(C4_SIGMA[0]), np.log(C4_SIGMA[1]))))
+    return dirs, flux, sigma
+
+
+def visibilities_c4(obs: "Observation", steps: Sequence[int], device="cpu",
+                    dtype=torch.complex64) -> Tuple[torch.Tensor, torch.Tensor]:
+    """S (len(steps), N, N) and positions (len(steps), N, 3) of rank-predictor steps, each
+    with its own sky and noise level (c4_step_sky); otherwise as visibilities()."""
+    cfg = obs.cfg
+    n, B, qmax = cfg.n_antenna, len(steps), C4_SOURCES[1]
+    dirs = np.zeros((B, qmax, 3))
+    flux = np.zeros((B, qmax))
+    sig = np.zeros(B)
+    for i, st in enumerate(steps):
+        d, f, sg = c4_step_sky(obs, st)
+        dirs[i, :len(f)] = d
+        flux[i, :len(f)] = f
+        sig[i] = sg
+    xyz = np.stack([obs.positions(s) for s in steps])
+    xyz_t = torch.from_numpy(xyz).to(device)
+    ph = (2 * math.pi / cfg.wl) * torch.einsum("bqc,bnc->bqn", torch.from_numpy(dirs).to(device), xyz_t)
+    a = torch.polar(torch.ones_like(ph), ph)
+    fl = torch.from_numpy(flux).to(device).to(a.dtype)
+    s = torch.einsum("bqi,bq,bqj->bij", a.conj(), fl, a)
+    g = torch.Generator(device=device)
+    g.manual_seed(cfg.seed * 1000003 + int(steps[0]) + 104729)
+    sg = torch.from_numpy(sig / math.sqrt(2.0)).to(device)[:, None, None]
+    xr = torch.randn((B, n, n), generator=g, device=device, dtype=torch.float64) * sg
+    xi = torch.randn((B, n, n), generator=g, device=device, dtype=torch.float64) * sg
+    x = torch.complex(xr, xi)
+    s = s + 0.5 * (x + x.conj().transpose(1, 2))
+    s.diagonal(dim1=1, dim2=2).zero_()
+    return s.to(dtype), xyz_t
+
+
 # --- geometry -----------------------------------------------------------------------
 
 def antenna_layout_enu(cfg: SimConfig) -> np.ndarray:

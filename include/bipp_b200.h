@@ -112,6 +112,50 @@ BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_d(bipp_ctx_t ctx, size_t nBatc
                                                     const double* wl, const void* s, const double* xyz, double* d,
                                                     void* v, size_t* nBeamReduced, double* scale);
 
+/* ---- learned rank predictor --------------------------------------------------------- */
+/* No counterpart in the reference, which computes every eigenpair (LAPACK ?hegv,
+ * src/eigensolver.cpp:188-216) and keeps those inside the energy levels afterwards.
+ *
+ * Ranked form of bipp_eigh_gram_batched_s (same inputs and outputs): mode 0 computes every
+ * eigenpair (the reference's full solve); mode 1 the eigenpairs above `threshold`, their
+ * index range found exactly by Sturm counts of the tridiagonal matrix; mode 2 the largest
+ * k + margin, with k, the count above the threshold, predicted per step by the MLP `model`
+ * (host, bipp_rank_mlp_num_params() floats) from the features of the whitened matrix. Mode
+ * 2 falls back to every eigenpair of a step when its smallest computed eigenvalue is still
+ * above the threshold (eigenvalues above it may be missing) or, with residualTol >= 0, when
+ * a computed pair has |T z - d z|_inf > residualTol |T| |z|_inf (T the tridiagonal matrix).
+ * Eigenvalues and eigenvectors not computed are returned as zero. Optional outputs per
+ * step: kComputed (eigenvectors computed), fallback (1 if the step fell back); ms: device
+ * time of the eigensolver kernels. */
+BIPP_B200_EXPORT BippError bipp_eigh_gram_batched_ranked_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna,
+                                                           const float* wl, const void* s, const float* xyz,
+                                                           double threshold, int mode, const float* model, int margin,
+                                                           double residualTol, float* d, void* v,
+                                                           size_t* nBeamReduced, float* scale, int* kComputed,
+                                                           int* fallback, double* ms);
+/* Training data of the predictor from the method itself: the full solve of each step (as
+ * bipp_eigh_gram_batched_s) with the 64 features of its whitened matrix L^-1 S L^-H
+ * (features [nBatch][64]) and the count of eigenvalues above `threshold` (counts [nBatch]). */
+BIPP_B200_EXPORT BippError bipp_rank_features_s(bipp_ctx_t ctx, size_t nBatch, size_t nAntenna, const float* wl,
+                                                const void* s, const float* xyz, double threshold, float* features,
+                                                int* counts);
+/* Floats of an MLP model (64 -> 128 -> 128 -> 1, ReLU): feature mean [64], standard
+ * deviation [64], W1 [64][128], b1 [128], W2 [128][128], b2 [128], W3 [128], b3. */
+BIPP_B200_EXPORT int bipp_rank_mlp_num_params(void);
+/* out[i] = MLP((features[i] - mean) / sd), features [n][64] (host pointers). */
+BIPP_B200_EXPORT BippError bipp_rank_mlp_forward(bipp_ctx_t ctx, const float* model, const float* features, size_t n,
+                                                 float* out);
+/* Gradient of the loss (1/n) sum_i (out_i - targets_i)^2 with respect to every model
+ * float (zero for the fixed mean and sd), and the loss. */
+BIPP_B200_EXPORT BippError bipp_rank_mlp_gradient(bipp_ctx_t ctx, const float* model, const float* features,
+                                                  const float* targets, size_t n, float* grad, float* loss);
+/* Train the model in place on the device: `iterations` full-batch Adam steps (beta 0.9,
+ * 0.999, eps 1e-8) on the loss above; lossHistory [iterations] (optional) gets the loss
+ * before each step. The mean and sd stay as given. */
+BIPP_B200_EXPORT BippError bipp_rank_mlp_train(bipp_ctx_t ctx, float* model, const float* features,
+                                               const float* targets, size_t n, int iterations, float learningRate,
+                                               float* lossHistory);
+
 /* Largest antenna count accepted by bipp_eigh_gram_noalloc_s. */
 #define BIPP_NOALLOC_MAX_ANTENNA 128
 

@@ -417,3 +417,47 @@ def test_gram_and_virtual_vis_match_compiled_reference_property():
         assert np.abs(vv_r - vv_o).max() <= 1e-12 * max(np.abs(vv_r).max(), 1e-300)
 
     check()
+
+
+def test_mlp_oracle_gradient_by_finite_differences():
+    """The numpy statement of the rank predictor's network (oracle/mlp.py): its
+    backpropagated gradient equals central differences of its loss (FP64) on random
+    parameters of every layer."""
+    from oracle import mlp as om
+
+    rng = np.random.default_rng(5)
+    n = 37
+    X = rng.standard_normal((n, om.F))
+    y = rng.uniform(0, 1, n)
+    model = np.concatenate([rng.standard_normal(om.F) * 0.1, rng.uniform(0.5, 2.0, om.F),
+                            rng.standard_normal(om.N_PARAMS - 2 * om.F) * 0.2])
+    loss, g = om.loss_and_gradient(model, X, y)
+    assert np.all(g[:om.OFF["W1"]] == 0)
+    idx = np.concatenate([rng.choice(np.arange(lo, hi), 6, replace=False) for lo, hi in
+                          ((om.OFF["W1"], om.OFF["b1"]), (om.OFF["b1"], om.OFF["W2"]), (om.OFF["W2"], om.OFF["b2"]),
+                           (om.OFF["b2"], om.OFF["W3"]), (om.OFF["W3"], om.OFF["b3"]))] + [[om.OFF["b3"]]])
+    h = 1e-6
+    for i in idx:
+        mp, mm = model.copy(), model.copy()
+        mp[i] += h
+        mm[i] -= h
+        fd = (om.loss_and_gradient(mp, X, y)[0] - om.loss_and_gradient(mm, X, y)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
+
+
+def test_mlp_oracle_features_statement():
+    """The numpy feature statement on a small Hermitian matrix: scale-free (a scaled
+    matrix gives the same features except the threshold), the largest diagonal
+    magnitudes and row norms first, and the 16 largest rows' share of the Frobenius norm
+    equal to the sum of their squared features."""
+    from oracle import mlp as om
+
+    rng = np.random.default_rng(6)
+    a = rng.standard_normal((40, 40)) + 1j * rng.standard_normal((40, 40))
+    C = (a + a.conj().T) / 2
+    f = om.features(C, 0.0)
+    f2 = om.features(7.0 * C, 0.0)
+    assert np.allclose(f, f2)
+    assert np.all(np.diff(f[:32]) <= 0) and np.all(np.diff(f[32:48]) <= 0)
+    assert np.isclose(f[63], np.sum(f[32:48] ** 2)) and f[63] <= 1.0
+    assert np.isclose(f[51], np.count_nonzero(C.diagonal().real > 0) / 40)
