@@ -69,7 +69,14 @@ SIGNATURES = {
     "bipp_rank_mlp_num_params": [],
     "bipp_rank_mlp_forward": [_p, _p, _p, _sz, _p],
     "bipp_rank_mlp_gradient": [_p, _p, _p, _p, _sz, _p, _p],
-    "bipp_rank_mlp_train": [_p, _p, _p, _p, _sz, _i, _f, _p],
+    "bipp_rank_mlp_train": [_p, _p, _p, _p, _sz, _p, _p, _sz, _i, _f, _f, _i, _p, _p],
+    "bipp_autotune_pipeline": [_p, _sz, _p, _p, _p, _i, _i, _p, _sz],
+    "bipp_tuning_get": [C.c_char_p, C.POINTER(_i)],
+    "bipp_tuning_set": [C.c_char_p, _i],
+    "bipp_tuning_describe": [_p, _sz],
+    "bipp_tuning_save": [C.c_char_p],
+    "bipp_tuning_load": [C.c_char_p],
+    "bipp_tuning_reset": [],
     "bipp_eigh_gram_noalloc_s": [_i, _p, _f, _sz, _p, _sz, _p, _sz, _p, _p, _sz, _p, _p, _p],
     "bipp_gram_matrix_s": [_p, _sz, _sz, _p, _sz, _p, _sz, _f, _p, _sz],
     "bipp_gram_matrix_d": [_p, _sz, _sz, _p, _sz, _p, _sz, _d, _p, _sz],

@@ -736,6 +736,19 @@ class Pipeline:
         return dict(zip(["points", "slabs", "grid_bytes", "items", "nx", "ny", "nw", "W", "split_tiles"],
                         [int(x) for x in st]))
 
+    def autotune(self, n_steps, s_ptr, xyz_ptr, wl_ptr, on_device=True, repeats=1):
+        """Time the candidate launch parameters on these steps (pointers as
+        process_device / process_host_ptr), keep the fastest in the process-wide tuning
+        table, and return the per-candidate times (ms per call) with the choices. The
+        images are left as they were."""
+        import json
+
+        buf = C.create_string_buffer(8192)
+        check(self.ctx._lib.bipp_autotune_pipeline(self.handle, int(n_steps), C.c_void_p(s_ptr), C.c_void_p(xyz_ptr),
+                                                   C.c_void_p(wl_ptr), 1 if on_device else 0, int(repeats), buf,
+                                                   len(buf)))
+        return json.loads(buf.value.decode())
+
     def close(self):
         if getattr(self, "handle", None):
             self.ctx._lib.bipp_pipeline_destroy(self.handle)
@@ -746,3 +759,39 @@ class Pipeline:
             self.close()
         except Exception:
             pass
+
+
+# --- tuning table of launch parameters ------------------------------------------------------
+
+def tuning_get(name: str) -> int:
+    v = C.c_int()
+    check(_lib.load().bipp_tuning_get(name.encode(), C.byref(v)))
+    return v.value
+
+
+def tuning_set(name: str, value: int) -> None:
+    check(_lib.load().bipp_tuning_set(name.encode(), int(value)))
+
+
+def tuning_describe() -> dict:
+    """{name: {"value", "candidates", "meaning"}} of every tunable launch parameter."""
+    buf = C.create_string_buffer(8192)
+    check(_lib.load().bipp_tuning_describe(buf, len(buf)))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, value, rest = line.split(" ", 2)
+        cands, meaning = rest[1:].split("] ", 1)
+        out[name] = {"value": int(value), "candidates": [int(c) for c in cands.split()], "meaning": meaning}
+    return out
+
+
+def tuning_save(path: str) -> None:
+    check(_lib.load().bipp_tuning_save(str(path).encode()))
+
+
+def tuning_load(path: str) -> None:
+    check(_lib.load().bipp_tuning_load(str(path).encode()))
+
+
+def tuning_reset() -> None:
+    check(_lib.load().bipp_tuning_reset())

@@ -9,6 +9,7 @@
 #include "context.hpp"
 #include "eig.hpp"
 #include "rank_mlp.cuh"
+#include "tune.hpp"
 #include "eig_kernels.cuh"
 #include "gemm_tc.cuh"
 
@@ -302,8 +303,9 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
   }
   // rank predictor: features of the whitened matrix, MLP, predicted counts
   if (L.features) {
-    const size_t smem = 2 * (size_t)Nmax * sizeof(float);
-    auto k = rank_features_kernel<C>;
+    const size_t smem = rank_features_smem(Nmax);
+    const int np = rank_probes(Nmax);
+    auto k = np == 8 ? rank_features_kernel<C, 8> : np == 4 ? rank_features_kernel<C, 4> : rank_features_kernel<C, 0>;
     smem_optin(k, smem);
     count_launch();
     k<<<nb, kFeatThreads, smem, st>>>(A, Nmax, nred, L.featThreshold, L.features);
@@ -330,8 +332,10 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     }
     smem_optin(k, smem);
     count_launch();
-    k<<<nb, trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(), w.e.template get<double>(),
-                                     w.tau.template get<C>(), sizeOrder);
+    // threads per matrix: by size, unless the tuning table fixes them
+    const int tt = tuned("hetrd.threads");
+    k<<<nb, tt > 0 ? tt : trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(),
+                                                        w.e.template get<double>(), w.tau.template get<C>(), sizeOrder);
     B2_CHECK_LAUNCH();
   }
   // 4. tridiagonal eigenpairs (FP64); workspace aliases W64 (free after trinv)

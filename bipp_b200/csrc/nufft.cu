@@ -11,6 +11,7 @@
 
 #include "context.hpp"
 #include "nufft.hpp"
+#include "tune.hpp"
 #include "spread_tc.cuh"
 
 namespace bippb200 {
@@ -287,7 +288,7 @@ static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, co
   B2_CUDA(cudaGetDevice(&dev));
   B2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   smem_optin(spread_tc_kernel<CH>, S::Smem);
-  const int grid = std::max(1, std::min(nItems, sms * S::MinBlocks));
+  const int grid = std::max(1, std::min(nItems, sms * std::min(S::MinBlocks, tuned("spread.ctas_per_sm"))));
   count_launch();
   spread_tc_kernel<CH><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0,
                                                            slabPlanes, out, errFlag);
@@ -300,9 +301,6 @@ static bool use_tensor_core_spread(int nch) {
   return nch <= kTcMaxChan;
 }
 
-// points per spreading part: heavier tiles are split so that no CTA serialises the
-// dense core of the uv plane (short baselines)
-constexpr int kSpreadCap = 4096;
 
 // exclusive scan of n ints on the stream; out[n] = total
 void NufftCore::exclusive_scan(const int* in, int* out, long long n) {
@@ -356,7 +354,10 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   splitCount_.ensure(ctx_, sizeof(int));
   B2_CUDA(cudaMemsetAsync(splitCount_.get(), 0, sizeof(int), ctx_->stream));
   count_launch();
-  tile_parts_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), kSpreadCap, parts_.get<int>(),
+  // points per spreading work item (tunable): heavier tiles are split so that no CTA
+  // serialises the dense core of the uv plane (short baselines)
+  const int spreadCap = tuned("spread.items_cap");
+  tile_parts_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), spreadCap, parts_.get<int>(),
                                                   clearFlag_.get<int>(), splitCount_.get<int>());
   B2_CHECK_LAUNCH();
   exclusive_scan(parts_.get<int>(), itemOff_.get<int>(), ntiles);
@@ -538,7 +539,7 @@ static void nufft_transform(bipp_nufft_s* p) {
     }
     B2_CHECK_LAUNCH();
     const double* ud = u64.get<double>();
-    const dim3 blocks = direct_sum_grid((long long)p->nPixel, (long long)n, ctx->smCount);
+    const dim3 blocks = direct_sum_grid((long long)p->nPixel, (long long)n, ctx->smCount, tuned("direct.ctas_per_sm"));
     for (size_t im = 0; im < p->nImages; ++im) {
       count_launch();
       f2d_kernel<<<256, 256, 0, ctx->stream>>>(reinterpret_cast<const float*>(p->values.get<float2>() + im * ld), 2 * n,
@@ -765,7 +766,7 @@ BippError bipp_nuft_sum_s(bipp_ctx_t ctx, float alpha, size_t nIn, const void* i
     h2d(ctx, dX.get<float>() + nOut, y, nOut * sizeof(float));
     h2d(ctx, dX.get<float>() + 2 * nOut, z, nOut * sizeof(float));
     h2d(ctx, dO.get(), out, nOut * sizeof(float));
-    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount, tuned("direct.ctas_per_sm"));
     count_launch();
     direct_sum_kernel<float, float2, float, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         (double)alpha, (long long)nIn, dIn.get<float2>(), (long long)nIn, dU.get<float>(), dU.get<float>() + nIn,
@@ -792,7 +793,7 @@ BippError bipp_nuft_sum_d(bipp_ctx_t ctx, double alpha, size_t nIn, const void* 
     h2d(ctx, dX.get<double>() + nOut, y, nOut * sizeof(double));
     h2d(ctx, dX.get<double>() + 2 * nOut, z, nOut * sizeof(double));
     h2d(ctx, dO.get(), out, nOut * sizeof(double));
-    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount, tuned("direct.ctas_per_sm"));
     count_launch();
     direct_sum_kernel<double, double2, double, 1><<<blocks, kDirectThreads, 0, ctx->stream>>>(
         alpha, (long long)nIn, dIn.get<double2>(), (long long)nIn, dU.get<double>(), dU.get<double>() + nIn,
@@ -812,7 +813,7 @@ BippError bipp_nuft_sum_multi_device(bipp_ctx_t ctx, double alpha, size_t nIn, s
     require(ctx && values && u && v && w && x && y && z && out, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(nch >= 1 && ldIn >= nIn && ldOut >= nOut, "invalid sizes");
     if (!nOut) return;
-    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount);
+    const dim3 blocks = direct_sum_grid((long long)nOut, (long long)nIn, ctx->smCount, tuned("direct.ctas_per_sm"));
     for (size_t c0 = 0; c0 < nch; c0 += 4) {
       const int n = (int)std::min<size_t>(4, nch - c0);
       count_launch();

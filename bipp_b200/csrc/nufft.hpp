@@ -58,7 +58,7 @@ public:
   const NufftGeom& geom() const { return g_; }
   // statistics of the last execute(): points spread, slabs (spreading launches), bytes of
   // grid written by the spreading (all slabs), work items, tiles split into several
-  // parts (more than kSpreadCap points; their parts accumulate with atomics)
+  // parts (more points than the spread.items_cap tunable; their parts accumulate with atomics)
   long long lastPoints = 0, lastSlabs = 0, lastGridBytes = 0, lastItems = 0, lastSplitTiles = 0;
   long long num_pixels() const { return (long long)g_.Na * g_.Nb; }
   int channels() const { return nch_; }

@@ -756,11 +756,11 @@ direct_sum_kernel(double alpha, long long nIn, const C* __restrict__ input, long
 }
 
 // Grid of direct_sum_kernel: one thread per output; when the outputs fill fewer than
-// about four CTAs per SM, the inputs are split over blockIdx.y (slices of at least 4096
+// ctasPerSm CTAs per SM, the inputs are split over blockIdx.y (slices of at least 4096
 // inputs) so that few pixels over many baselines still fill the GPU.
-inline dim3 direct_sum_grid(long long nOut, long long nIn, int smCount) {
+inline dim3 direct_sum_grid(long long nOut, long long nIn, int smCount, int ctasPerSm) {
   const long long bx = (nOut + kDirectThreads - 1) / kDirectThreads;
-  const long long target = 4LL * (smCount > 0 ? smCount : 148);
+  const long long target = (long long)ctasPerSm * (smCount > 0 ? smCount : 148);
   long long by = 1;
   if (bx < target) {
     by = (target + bx - 1) / bx;

@@ -10,6 +10,9 @@
 // mode) or run one step and one level at a time ("plain" mode, the straightforward GPU
 // form used as the comparison point).
 #include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
 #include <cmath>
 #include <memory>
 #include <numeric>
@@ -19,6 +22,7 @@
 #include "eig.hpp"
 #include "eig_kernels.cuh"
 #include "nufft.hpp"
+#include "tune.hpp"
 #include "vv_tc.cuh"
 
 namespace bippb200 {
@@ -230,7 +234,8 @@ static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector
         v.tilesI = (N + kVvM - 1) / kVvM;
         v.tilesJ = (N + kVvNC - 1) / kVvNC;
         const long long items = (long long)nb * L * v.tilesI * v.tilesJ;
-        const int grid = (int)std::max<long long>(1, std::min<long long>(items, 3LL * ctx->smCount));
+        const int grid = (int)std::max<long long>(
+            1, std::min<long long>(items, (long long)tuned("vv.ctas_per_sm") * ctx->smCount));
         auto k = p->vvPrecision == 0 ? vv_tc_kernel<1> : vv_tc_kernel<2>;
         smem_optin(k, VvShape<1>::Smem);
         count_launch();
@@ -521,6 +526,90 @@ BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize,
       }
     } else {
       sync(ctx);
+    }
+  });
+}
+
+BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz,
+                                 const double* wl, int onDevice, int repeats, char* report, size_t reportLen) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    require(repeats >= 1 && repeats <= 100, "repeats must be in [1, 100]");
+    bipp_ctx_s* ctx = pl->ctx;
+    // the caller's images, step count and timers are kept aside and restored afterwards
+    const size_t imgBytes = (size_t)pl->nLevels * pl->P * sizeof(float);
+    DevBuf saved(ctx, imgBytes);
+    B2_CUDA(cudaMemcpyAsync(saved.get(), pl->images.get(), imgBytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    const long long stepsDone = pl->stepsDone;
+    double stage[7], eigt[kEigTimers];
+    std::copy(pl->stageMs, pl->stageMs + 7, stage);
+    std::copy(pl->eigMs, pl->eigMs + kEigTimers, eigt);
+    const bool timing = pl->timing;
+    pl->timing = false;
+    cudaEvent_t e0, e1;
+    B2_CUDA(cudaEventCreate(&e0));
+    B2_CUDA(cudaEventCreate(&e1));
+    std::string rep = "{";
+    const char* params[] = {"spread.items_cap", "spread.ctas_per_sm", "hetrd.threads", "vv.ctas_per_sm"};
+    auto body = [&] {
+      pipeline_process(pl, nSteps, s, xyz, wl, onDevice);   // warm-up (allocations, first-use costs)
+      bool first = true;
+      for (const char* name : params) {
+        if (!std::strcmp(name, "vv.ctas_per_sm") && (pl->vvPrecision == 2 || pl->vvPrecision == 3)) continue;
+        int best = tuned(name);
+        float bestMs = 0.f;
+        bool firstBest = true;
+        rep += std::string(first ? "" : ", ") + "\"" + name + "\": {";
+        first = false;
+        bool firstC = true;
+        for (const int c : tuning_candidates(name)) {
+          set_tuned(name, c);
+          B2_CUDA(cudaEventRecord(e0, ctx->stream));
+          for (int r = 0; r < repeats; ++r) pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
+          B2_CUDA(cudaEventRecord(e1, ctx->stream));
+          B2_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          B2_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms /= (float)repeats;
+          char buf[64];
+          std::snprintf(buf, sizeof(buf), "%s\"%d\": %.3f", firstC ? "" : ", ", c, ms);
+          rep += buf;
+          firstC = false;
+          if (firstBest || ms < bestMs) {
+            bestMs = ms;
+            best = c;
+            firstBest = false;
+          }
+        }
+        set_tuned(name, best);
+        char buf[64];
+        std::snprintf(buf, sizeof(buf), ", \"chosen\": %d}", best);
+        rep += buf;
+      }
+    };
+    // the caller's state comes back on every exit path
+    auto restore = [&] {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaMemcpyAsync(pl->images.get(), saved.get(), imgBytes, cudaMemcpyDeviceToDevice, ctx->stream);
+      pl->stepsDone = stepsDone;
+      std::copy(stage, stage + 7, pl->stageMs);
+      std::copy(eigt, eigt + kEigTimers, pl->eigMs);
+      pl->timing = timing;
+      cudaStreamSynchronize(ctx->stream);
+    };
+    try {
+      body();
+    } catch (...) {
+      restore();
+      throw;
+    }
+    restore();
+    rep += "}";
+    if (report && reportLen) {
+      const size_t n = std::min(reportLen - 1, rep.size());
+      std::memcpy(report, rep.data(), n);
+      report[n] = '\0';
     }
   });
 }

@@ -4,7 +4,9 @@
 // every eigenpair (LAPACK ?hegv, src/eigensolver.cpp:188-216).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "bipp_b200.h"
 #include "context.hpp"
@@ -88,20 +90,36 @@ BippError bipp_rank_mlp_gradient(bipp_ctx_t ctx, const float* model, const float
 }
 
 BippError bipp_rank_mlp_train(bipp_ctx_t ctx, float* model, const float* features, const float* targets, size_t n,
-                              int iterations, float learningRate, float* lossHistory) {
+                              const float* valFeatures, const float* valTargets, size_t nVal, int iterations,
+                              float learningRate, float weightDecay, int evalEvery, float* lossHistory,
+                              float* valHistory) {
   return guard([&] {
     require(ctx != nullptr, "null context", BIPP_INVALID_HANDLE_ERROR);
     require(model && features && targets, "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(n >= 1 && n <= (1u << 24), "sample count must be in [1, 2^24]");
+    require(nVal <= (1u << 24), "validation sample count above 2^24");
+    require(!nVal || (valFeatures && valTargets), "null pointer", BIPP_INVALID_POINTER_ERROR);
     require(iterations >= 1 && iterations <= (1 << 24), "iterations must be in [1, 2^24]");
     require(std::isfinite(learningRate) && learningRate > 0.f, "learning rate must be positive");
+    require(std::isfinite(weightDecay) && weightDecay >= 0.f, "weight decay must be non-negative");
+    require(!nVal || evalEvery >= 1, "evalEvery must be positive with a validation set");
     check_model(model);
     MlpBuffers b(ctx, model, features, targets, (int)n, iterations);
     DevBuf m(ctx, kMlpParams * sizeof(float)), v(ctx, kMlpParams * sizeof(float)), step(ctx, sizeof(int));
+    DevBuf best(ctx, kMlpParams * sizeof(float)), vX, vOut;
     m.zero();
     v.zero();
     step.zero();
     b.loss.zero();
+    std::vector<float> vy(nVal), vo(nVal);
+    if (nVal) {
+      vX.alloc(ctx, nVal * kRankFeatures * sizeof(float));
+      vOut.alloc(ctx, nVal * sizeof(float));
+      h2d(ctx, vX.get(), valFeatures, nVal * kRankFeatures * sizeof(float));
+      std::copy(valTargets, valTargets + nVal, vy.begin());
+    }
+    B2_CUDA(cudaMemcpyAsync(best.get(), b.model.get(), kMlpParams * sizeof(float), cudaMemcpyDeviceToDevice,
+                            ctx->stream));
     const int grid = (int)((n + kMlpTile - 1) / kMlpTile);
     const int ag = (kMlpParams + 255) / 256;
     cudaStream_t st = ctx->stream;
@@ -117,21 +135,51 @@ BippError bipp_rank_mlp_train(bipp_ctx_t ctx, float* model, const float* feature
                                                     (int)n, b.H1.get<float>(), b.H2.get<float>(), b.out.get<float>(),
                                                     b.grad.get<float>(), b.loss.get<float>(), step.get<int>());
     mlp_adam_kernel<<<ag, 256, 0, st>>>(b.model.get<float>(), b.grad.get<float>(), m.get<float>(), v.get<float>(),
-                                        learningRate, 0.9f, 0.999f, 1e-8f, step.get<int>());
+                                        learningRate, 0.9f, 0.999f, 1e-8f, weightDecay, step.get<int>());
     mlp_step_kernel<<<1, 1, 0, st>>>(step.get<int>());
     const cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (ce != cudaSuccess) throw Error(BIPP_GPU_ERROR, std::string("stream capture: ") + cudaGetErrorString(ce));
     cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) throw Error(BIPP_GPU_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    // validation loss of the current model (host), every evalEvery iterations; the model
+    // with the lowest one is kept
+    auto val_loss = [&]() {
+      count_launch();
+      mlp_forward_kernel<<<(int)((nVal + kMlpTile - 1) / kMlpTile), kMlpThreads, 0, st>>>(
+          b.model.get<float>(), vX.get<float>(), (int)nVal, vOut.get<float>(), nullptr, nullptr);
+      B2_CHECK_LAUNCH();
+      d2h(ctx, vo.data(), vOut.get(), nVal * sizeof(float));
+      sync(ctx);
+      double l = 0;
+      for (size_t i = 0; i < nVal; ++i) l += ((double)vo[i] - vy[i]) * ((double)vo[i] - vy[i]);
+      return l / (double)nVal;
+    };
+    double bestVal = nVal ? val_loss() : 0.0;
+    int evals = 0;
     cudaError_t le = cudaSuccess;
-    for (int it = 0; it < iterations && le == cudaSuccess; ++it) {
-      for (int k = 0; k < 4; ++k) count_launch();
-      le = cudaGraphLaunch(exec, st);
+    try {
+      for (int it = 0; it < iterations && le == cudaSuccess; ++it) {
+        for (int k = 0; k < 4; ++k) count_launch();
+        le = cudaGraphLaunch(exec, st);
+        if (le == cudaSuccess && nVal && ((it + 1) % evalEvery == 0 || it + 1 == iterations)) {
+          const double l = val_loss();
+          if (valHistory) valHistory[evals] = (float)l;
+          ++evals;
+          if (l < bestVal) {
+            bestVal = l;
+            B2_CUDA(cudaMemcpyAsync(best.get(), b.model.get(), kMlpParams * sizeof(float), cudaMemcpyDeviceToDevice,
+                                    st));
+          }
+        }
+      }
+    } catch (...) {
+      cudaGraphExecDestroy(exec);
+      throw;
     }
     cudaGraphExecDestroy(exec);
     if (le != cudaSuccess) throw Error(BIPP_GPU_ERROR, std::string("graph launch: ") + cudaGetErrorString(le));
-    d2h(ctx, model, b.model.get(), kMlpParams * sizeof(float));
+    d2h(ctx, model, nVal ? best.get() : b.model.get(), kMlpParams * sizeof(float));
     if (lossHistory) d2h(ctx, lossHistory, b.loss.get(), (size_t)iterations * sizeof(float));
     sync(ctx);
   });

@@ -24,16 +24,79 @@ constexpr int kOffMu = 0, kOffSd = kRankFeatures, kOffW1 = 2 * kRankFeatures;
 constexpr int kOffB1 = kOffW1 + kRankFeatures * kMlpH, kOffW2 = kOffB1 + kMlpH, kOffB2 = kOffW2 + kMlpH * kMlpH;
 constexpr int kOffW3 = kOffB2 + kMlpH, kOffB3 = kOffW3 + kMlpH, kMlpParams = kOffB3 + 1;
 
+// Probe vectors of the trace estimates: Rademacher entries from a hash of (row, probe)
+__device__ __forceinline__ float probe_sign(int i, int p) {
+  unsigned h = (unsigned)i * 0x9E3779B1u ^ ((unsigned)p * 0x85EBCA77u + 0x165667B1u);
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  return (h & 1u) ? 1.f : -1.f;
+}
+
+// probes of the trace estimates for matrices of up to nmax rows (their two n x P complex
+// work arrays live in shared memory)
+inline int rank_probes(int nmax) { return nmax <= 1024 ? 8 : nmax <= 2048 ? 4 : 0; }
+// rows of the diagonal / row-norm arrays, even so that the probe arrays after them are
+// 8-byte aligned
+inline __host__ __device__ int rank_rows(int nmax) { return (nmax + 1) & ~1; }
+inline size_t rank_features_smem(int nmax) {
+  return 2 * (size_t)rank_rows(nmax) * sizeof(float) + 2 * (size_t)nmax * rank_probes(nmax) * sizeof(float2);
+}
+
+// Y = C X for the n x P block X (row-major [n][P] complex in shared memory), C Hermitian
+// with its lower triangle at Ab (ld Nmax); Y zeroed by the caller. Column j of the lower
+// triangle gives y_i += C_ij x_j (i > j, shared-memory atomics) and y_j += sum_i
+// conj(C_ij) x_i (a warp reduction).
+template <typename C, int P>
+__device__ void herm_block_mv(const C* __restrict__ Ab, int Nmax, int n, const float2* X, float2* Y) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int j = warp; j < n; j += nwarp) {
+    float2 xj[P], acc[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      xj[p] = X[j * P + p];
+      acc[p] = make_float2(0.f, 0.f);
+    }
+    for (int i = j + lane; i < n; i += 32) {
+      const C v = Ab[i + (long long)j * Nmax];
+      const float cr = (float)v.x, ci = (i == j) ? 0.f : (float)v.y;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const float2 xi = X[i * P + p];
+        // conj(C_ij) x_i
+        acc[p].x += cr * xi.x + ci * xi.y;
+        acc[p].y += cr * xi.y - ci * xi.x;
+        if (i != j) {
+          atomicAdd(&Y[i * P + p].x, cr * xj[p].x - ci * xj[p].y);
+          atomicAdd(&Y[i * P + p].y, cr * xj[p].y + ci * xj[p].x);
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const float ax = warp_sum(acc[p].x), ay = warp_sum(acc[p].y);
+      if (lane == 0) {
+        atomicAdd(&Y[j * P + p].x, ax);
+        atomicAdd(&Y[j * P + p].y, ay);
+      }
+    }
+  }
+}
+
 // Features of the whitened matrix C = L^-1 S L^-H (lower triangle, ld Nmax) of each step,
-// all scale-free (divided by the Frobenius norm |C|_F where they carry its unit):
-//   [0, 32)   the 32 largest |C_ii| (descending)
-//   [32, 48)  the 16 largest row norms |C_i.|
-//   48 log(n) / log(4096); 49 trace C; 50 threshold; 51 fraction of C_ii above the
-//   threshold; 52 sum |C_ii|; 53 sum C_ii^2 / |C|_F^2; 54 largest |C_i.|^2 / |C|_F^2;
-//   55 sum |C_i.|^4 / |C|_F^4; 56 trace C / (|C|_F sqrt(n)); 57 fraction of rows with
-//   |C_i.|^2 above |C|_F^2 / n; 58 sum of C_ii above the threshold; 59-62 C_ii at the
-//   ranks n/8, n/4, n/2, 3n/4 (descending); 63 share of |C|_F^2 in the 16 largest rows.
-template <typename C>
+// scale-free (divided by the power of the Frobenius norm f = |C|_F that carries C's unit):
+//   [0, 32)  the 32 largest |C_ii| (descending)
+//   32 log(n) / log(4096); 33 trace C; 34 threshold; 35 fraction of C_ii above the
+//   threshold; 36 sum |C_ii|; 37 sum C_ii^2; 38 largest squared row norm; 39 sum of
+//   row norms^4; 40 fraction of rows with squared norm above f^2 / n; 41 sum of C_ii above
+//   the threshold; 42-45 C_ii at the ranks n/8, n/4, n/2, 3n/4 (descending);
+//   46-63 spectral moments t_k = trace C^k, k = 2..6, estimated with P Rademacher probes
+//   z (t_k ~ mean z^H C^k z, from Y1 = C Z, Y2 = C Y1, Y3 = C Y2): t3, t4, t5, t6, the
+//   effective ranks f^4 / t4 and (f^6 / t6)^(1/2) (both / n), t4^2 / (t6 f^2),
+//   t3^2 / (t4 f^2), t5 / (t4 f), their logarithms / log(n), t1 t3 / f^4,
+//   t3 / (f t4^(1/2)), t5 / (t4 t6)^(1/2), t2 / f^2 (the probes' own check), and the
+//   share of f^2 in the 16 largest rows.
+template <typename C, int P>
 __global__ void __launch_bounds__(kFeatThreads)
 rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ nred, double threshold,
                      float* __restrict__ feat) {
@@ -42,11 +105,15 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
   float* f = feat + (long long)b * kRankFeatures;
   extern __shared__ float fsm[];
   float* dg = fsm;           // [Nmax] diagonal (real)
-  float* r2 = fsm + Nmax;    // [Nmax] squared row norms
+  float* r2 = fsm + rank_rows(Nmax);   // [Nmax] squared row norms
+  float2* Ya = reinterpret_cast<float2*>(fsm + 2 * rank_rows(Nmax));   // [Nmax][P]
+  float2* Yb = Ya + (long long)Nmax * P;                     // [Nmax][P]
   __shared__ double red[32];
   __shared__ float top[kRankFeatures];
+  __shared__ float rtop[16];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   for (int i = tid; i < kRankFeatures; i += blockDim.x) top[i] = 0.f;
+  if (tid < 16) rtop[tid] = 0.f;
   if (n <= 0) {
     for (int i = tid; i < kRankFeatures; i += blockDim.x) f[i] = 0.f;
     return;
@@ -117,28 +184,98 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
       rs += (sj > si || (sj == si && j < i)) ? 1 : 0;
     }
     if (ra < 32) top[ra] = (float)(ai / fro);
-    if (rr < 16) top[32 + rr] = (float)(sqrt((double)ri) / fro);
-    if (rs == q1) top[59] = (float)(si / fro);
-    if (rs == q2) top[60] = (float)(si / fro);
-    if (rs == q3) top[61] = (float)(si / fro);
-    if (rs == q4) top[62] = (float)(si / fro);
+    if (rr < 16) rtop[rr] = ri;
+    if (rs == q1) top[42] = (float)(si / fro);
+    if (rs == q2) top[43] = (float)(si / fro);
+    if (rs == q3) top[44] = (float)(si / fro);
+    if (rs == q4) top[45] = (float)(si / fro);
+  }
+  // spectral moments by probes: Ya = C Z, Yb = C Ya, then Ya = C Yb
+  double t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;
+  if constexpr (P > 0) {
+    for (int e = tid; e < n * P; e += blockDim.x) {
+      Yb[e] = make_float2(probe_sign(e / P, e % P), 0.f);   // Z in Yb
+      Ya[e] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    herm_block_mv<C, P>(Ab, Nmax, n, Yb, Ya);
+    __syncthreads();
+    double a1 = 0, a2 = 0;
+    for (int e = tid; e < n * P; e += blockDim.x) {
+      const float2 y = Ya[e];
+      a1 += (double)probe_sign(e / P, e % P) * y.x;
+      a2 += (double)y.x * y.x + (double)y.y * y.y;
+    }
+    t1 = block_sum(a1, red) / P;
+    __syncthreads();
+    t2 = block_sum(a2, red) / P;
+    __syncthreads();
+    for (int e = tid; e < n * P; e += blockDim.x) Yb[e] = make_float2(0.f, 0.f);
+    __syncthreads();
+    herm_block_mv<C, P>(Ab, Nmax, n, Ya, Yb);
+    __syncthreads();
+    double a3 = 0, a4 = 0;
+    for (int e = tid; e < n * P; e += blockDim.x) {
+      const float2 x = Ya[e], y = Yb[e];
+      a3 += (double)x.x * y.x + (double)x.y * y.y;
+      a4 += (double)y.x * y.x + (double)y.y * y.y;
+    }
+    t3 = block_sum(a3, red) / P;
+    __syncthreads();
+    t4 = block_sum(a4, red) / P;
+    __syncthreads();
+    for (int e = tid; e < n * P; e += blockDim.x) Ya[e] = make_float2(0.f, 0.f);
+    __syncthreads();
+    herm_block_mv<C, P>(Ab, Nmax, n, Yb, Ya);
+    __syncthreads();
+    double a5 = 0, a6 = 0;
+    for (int e = tid; e < n * P; e += blockDim.x) {
+      const float2 x = Yb[e], y = Ya[e];
+      a5 += (double)x.x * y.x + (double)x.y * y.y;
+      a6 += (double)y.x * y.x + (double)y.y * y.y;
+    }
+    t5 = block_sum(a5, red) / P;
+    __syncthreads();
+    t6 = block_sum(a6, red) / P;
+    __syncthreads();
   }
   __syncthreads();
   if (tid == 0) {
     double top16 = 0;
-    for (int r = 0; r < 16; ++r) top16 += (double)top[32 + r] * top[32 + r];
-    top[48] = (float)(log((double)n) / log(4096.0));
-    top[49] = (float)(tr / fro);
-    top[50] = (float)(threshold / fro);
-    top[51] = (float)(cab / n);
-    top[52] = (float)(sabs / fro);
-    top[53] = (float)(ssq / fro2);
-    top[54] = (float)(mr2 / fro2);
-    top[55] = (float)(sr4 / (fro2 * fro2));
-    top[56] = (float)(tr / (fro * sqrt((double)n)));
-    top[57] = (float)(crow / n);
-    top[58] = (float)(sab / fro);
-    top[63] = (float)top16;
+    for (int r = 0; r < 16; ++r) top16 += rtop[r];
+    const double ln = log((double)n);
+    top[32] = (float)(ln / log(4096.0));
+    top[33] = (float)(tr / fro);
+    top[34] = (float)(threshold / fro);
+    top[35] = (float)(cab / n);
+    top[36] = (float)(sabs / fro);
+    top[37] = (float)(ssq / fro2);
+    top[38] = (float)(mr2 / fro2);
+    top[39] = (float)(sr4 / (fro2 * fro2));
+    top[40] = (float)(crow / n);
+    top[41] = (float)(sab / fro);
+    if (P > 0 && t4 > 0 && t6 > 0) {
+      const double f3 = fro2 * fro, f4 = fro2 * fro2, f5 = f4 * fro, f6 = f4 * fro2;
+      const double er4 = f4 / t4, er6 = sqrt(f6 / t6);
+      top[46] = (float)(t3 / f3);
+      top[47] = (float)(t4 / f4);
+      top[48] = (float)(t5 / f5);
+      top[49] = (float)(t6 / f6);
+      top[50] = (float)(er4 / n);
+      top[51] = (float)(er6 / n);
+      top[52] = (float)(t4 * t4 / (t6 * fro2));
+      top[53] = (float)(t3 * t3 / (t4 * fro2));
+      top[54] = (float)(t5 / (t4 * fro));
+      top[55] = (float)(log(fmax(er4, 1e-30)) / ln);
+      top[56] = (float)(log(fmax(er6, 1e-30)) / ln);
+      top[57] = (float)(t1 * t3 / f4);
+      top[58] = (float)(t3 / (fro * sqrt(t4)));
+      top[59] = (float)(t5 / sqrt(t4 * t6));
+      top[60] = (float)(t2 / fro2);
+      top[61] = (float)(t1 / fro);
+      top[62] = (float)(er4 / er6);
+    }
+    top[63] = (float)(top16 / fro2);
   }
   __syncthreads();
   for (int i = tid; i < kRankFeatures; i += blockDim.x) f[i] = top[i];
@@ -283,10 +420,10 @@ mlp_backward_kernel(const float* __restrict__ model, const float* __restrict__ X
 }
 
 // Adam step number *step + 1 on the trainable parameters [kOffW1, kMlpParams) (bias
-// corrections 1 - beta^t); the step counter lives on the device so that one training
-// iteration can be captured once in a CUDA graph and replayed
+// corrections 1 - beta^t) with decoupled weight decay wd; the step counter lives on the
+// device so that one training iteration can be captured once in a CUDA graph and replayed
 static __global__ void mlp_adam_kernel(float* __restrict__ model, const float* __restrict__ grad, float* __restrict__ m,
-                                float* __restrict__ v, float lr, float beta1, float beta2, float eps,
+                                float* __restrict__ v, float lr, float beta1, float beta2, float eps, float wd,
                                 const int* __restrict__ step) {
   const float tt = (float)(*step + 1);
   const float c1 = 1.f - powf(beta1, tt), c2 = 1.f - powf(beta2, tt);
@@ -296,7 +433,8 @@ static __global__ void mlp_adam_kernel(float* __restrict__ model, const float* _
     const float vi = beta2 * v[i] + (1.f - beta2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    model[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    // decoupled weight decay (AdamW), then the Adam step
+    model[i] -= lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * model[i]);
   }
 }
 

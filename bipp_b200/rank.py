@@ -84,16 +84,23 @@ def gradient(model, feats, targets, ctx: Optional[Context] = None):
     return float(loss[0]), grad
 
 
-def train(model, feats, targets, iterations: int = 2000, lr: float = 1e-3, ctx: Optional[Context] = None):
-    """(trained model, loss history): full-batch Adam on the GPU."""
+def train(model, feats, targets, iterations: int = 2000, lr: float = 1e-3, weight_decay: float = 0.0,
+          val_feats=None, val_targets=None, eval_every: int = 100, ctx: Optional[Context] = None):
+    """(trained model, loss history, validation history): full-batch Adam on the GPU; with
+    a validation set the model of lowest validation loss is returned."""
     ctx = ctx or default_context()
     model = np.array(model, dtype=np.float32, copy=True)
     feats = np.ascontiguousarray(feats, dtype=np.float32)
     targets = np.ascontiguousarray(targets, dtype=np.float32)
     hist = np.zeros(iterations, dtype=np.float32)
+    nv = 0 if val_feats is None else len(val_feats)
+    vf = np.ascontiguousarray(val_feats, dtype=np.float32) if nv else None
+    vt = np.ascontiguousarray(val_targets, dtype=np.float32) if nv else None
+    vh = np.zeros(max(1, -(-iterations // eval_every)), dtype=np.float32)
     check(ctx._lib.bipp_rank_mlp_train(ctx.handle, _ptr(model), _ptr(feats), _ptr(targets), feats.shape[0],
-                                       int(iterations), C.c_float(lr), _ptr(hist)))
-    return model, hist
+                                       _ptr(vf) if nv else None, _ptr(vt) if nv else None, nv, int(iterations),
+                                       C.c_float(lr), C.c_float(weight_decay), int(eval_every), _ptr(hist), _ptr(vh)))
+    return model, hist, (vh if nv else None)
 
 
 def eigh_gram_ranked(wl, s, xyz, threshold: float = 0.0, mode: str = "predicted", model=None, margin: int = 16,
@@ -141,9 +148,10 @@ def c4_steps(obs, steps, chunk: int = 512):
 
 
 def study(ctx, obs, n_train: int = 2000, n_eval: int = 2000, threshold: float = 0.0, iterations: int = 3000,
-          lr: float = 1e-3, margin: int = 16, seed: int = 0, chunk: int = 512):
+          lr: float = 1e-3, margin: int = 16, seed: int = 0, chunk: int = 512, weight_decay: float = 1e-4):
     """The rank-predictor study on the workload of `obs` (config_c4): train on the first
-    n_train steps (features and labels from the full solve), then solve the next n_eval
+    n_train steps (features and labels from the full solve; the last fifth of them
+    validates, and the model of lowest validation loss is kept), then solve the next n_eval
     steps in the three modes, chunk steps per call. Reports the loss, the fallback rate, the
     count error of the prediction, the eigenvalue error of the predicted partial solve
     against the full solve (eigenvalues above the threshold), and the eigensolver device
@@ -152,7 +160,11 @@ def study(ctx, obs, n_train: int = 2000, n_eval: int = 2000, threshold: float = 
     feats, counts = features(wl, s, x, threshold, ctx=ctx)
     nred = np.count_nonzero(np.abs(s).sum(1) > 0, axis=1)
     y = counts / np.maximum(nred, 1)
-    model, hist = train(init_model(feats, seed, ctx=ctx), feats, y, iterations=iterations, lr=lr, ctx=ctx)
+    # the last fifth of the training steps is the validation set of the early stopping
+    nt = n_train - n_train // 5
+    model, hist, vhist = train(init_model(feats[:nt], seed, ctx=ctx), feats[:nt], y[:nt], iterations=iterations,
+                               lr=lr, weight_decay=weight_decay, val_feats=feats[nt:], val_targets=y[nt:],
+                               eval_every=100, ctx=ctx)
     se, xe, wle = c4_steps(obs, list(range(n_train, n_train + n_eval)))
     res = {m: [] for m in MODES}
     for i0 in range(0, n_eval, chunk):
@@ -172,7 +184,7 @@ def study(ctx, obs, n_train: int = 2000, n_eval: int = 2000, threshold: float = 
     k_pred = np.clip(np.rint(forward(model, feats_e, ctx=ctx) * nred_e), 0, nred_e).astype(int)
     return {
         "train_steps": n_train, "eval_steps": n_eval, "threshold": threshold, "margin": margin,
-        "loss_first": float(hist[0]), "loss_last": float(hist[-1]),
+        "loss_first": float(hist[0]), "loss_last": float(hist[-1]), "val_loss_best": float(vhist.min()),
         "fallback_rate": float(cat["predicted"]["fallback"].mean()),
         "count_error_mean_abs": float(np.abs(k_pred - k_true).mean()),
         "count_error_max_under": int(max(0, (k_true - k_pred).max())),

@@ -150,11 +150,16 @@ BIPP_B200_EXPORT BippError bipp_rank_mlp_forward(bipp_ctx_t ctx, const float* mo
 BIPP_B200_EXPORT BippError bipp_rank_mlp_gradient(bipp_ctx_t ctx, const float* model, const float* features,
                                                   const float* targets, size_t n, float* grad, float* loss);
 /* Train the model in place on the device: `iterations` full-batch Adam steps (beta 0.9,
- * 0.999, eps 1e-8) on the loss above; lossHistory [iterations] (optional) gets the loss
- * before each step. The mean and sd stay as given. */
+ * 0.999, eps 1e-8, decoupled weight decay) on the loss above; lossHistory [iterations]
+ * (optional) gets the loss before each step. With a validation set (nVal > 0) its loss is
+ * computed every evalEvery iterations (valHistory, optional, gets them) and the model
+ * with the lowest validation loss is returned (early stopping). The mean and sd stay as
+ * given. */
 BIPP_B200_EXPORT BippError bipp_rank_mlp_train(bipp_ctx_t ctx, float* model, const float* features,
-                                               const float* targets, size_t n, int iterations, float learningRate,
-                                               float* lossHistory);
+                                               const float* targets, size_t n, const float* valFeatures,
+                                               const float* valTargets, size_t nVal, int iterations,
+                                               float learningRate, float weightDecay, int evalEvery,
+                                               float* lossHistory, float* valHistory);
 
 /* Largest antenna count accepted by bipp_eigh_gram_noalloc_s. */
 #define BIPP_NOALLOC_MAX_ANTENNA 128
@@ -341,10 +346,35 @@ BIPP_B200_EXPORT BippError bipp_pipeline_stage_times(bipp_pipeline_t pl, int ena
 BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double* ms);
 /* Statistics of the last NUFFT of the pipeline (9 values): points spread, spreading
  * launches (w-slabs), grid bytes written by the spreading, spreading work items, fine
- * grid sizes nx, ny, nw, kernel width W, tiles split into several work items (more than
- * 4096 points; their parts accumulate into the grid with atomics). */
+ * grid sizes nx, ny, nw, kernel width W, tiles split into several work items (more points
+ * than the spread.items_cap tuning parameter, 4096 by default; their parts accumulate into
+ * the grid with atomics). */
 BIPP_B200_EXPORT BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
+
+/* ---- autotuner of launch shapes (no counterpart in the reference, whose only launch-shape
+ * logic is the fixed block-size ladder of src/gpu/kernels/nuft_sum.cu:73-84) ------------ */
+
+/* Time the candidates of the tunable launch parameters on the caller's sample steps (the
+ * arguments of bipp_pipeline_process) with the pipeline `pl`, one parameter at a time
+ * (points per spreading work item, spreading CTAs per SM, threads per matrix of the
+ * tridiagonalisation, virtual-visibility CTAs per SM), keep the fastest of each in the
+ * process-wide tuning table, and write a JSON report of the per-call times (ms) into
+ * report (reportLen bytes, truncated). The pipeline's images and step count are left as
+ * they were. Results do not depend on the chosen values beyond rounding. */
+BIPP_B200_EXPORT BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz,
+                                                  const double* wl, int onDevice, int repeats, char* report,
+                                                  size_t reportLen);
+/* The tuning table: get or set one parameter (a value outside its candidates fails with
+ * BIPP_INVALID_PARAMETER_ERROR), describe all (one line each: name, value, candidates,
+ * meaning), save to or load from a file of "name value" lines, or reset to the defaults.
+ * BIPP_B200_TUNING_FILE, when set, is loaded on first use. No device is needed. */
+BIPP_B200_EXPORT BippError bipp_tuning_get(const char* name, int* value);
+BIPP_B200_EXPORT BippError bipp_tuning_set(const char* name, int value);
+BIPP_B200_EXPORT BippError bipp_tuning_describe(char* out, size_t len);
+BIPP_B200_EXPORT BippError bipp_tuning_save(const char* path);
+BIPP_B200_EXPORT BippError bipp_tuning_load(const char* path);
+BIPP_B200_EXPORT BippError bipp_tuning_reset(void);
 
 #ifdef __cplusplus
 }

@@ -64,14 +64,29 @@ def loss_and_gradient(model, X, y):
     return loss, grad
 
 
-def features(C, threshold=0.0):
-    """The 64 features of a whitened matrix C (n x n Hermitian), as the GPU forms them
-    from its lower triangle: the 32 largest |C_ii|, the 16 largest row norms, then
-    log(n)/log(4096), trace, threshold, fraction of C_ii above the threshold, sum |C_ii|,
-    sum C_ii^2 / |C|_F^2, max row norm^2 / |C|_F^2, sum row norm^4 / |C|_F^4,
-    trace / (|C|_F sqrt(n)), fraction of rows with norm^2 above |C|_F^2 / n, sum of C_ii
-    above the threshold, C_ii at the ranks n/8, n/4, n/2, 3n/4 (descending), and the share
-    of |C|_F^2 in the 16 largest rows; quantities with the unit of C divided by |C|_F."""
+def probe_sign(i, p):
+    """Rademacher entry (row i, probe p) of the trace-estimate probes, the integer hash the
+    GPU uses (32-bit arithmetic)."""
+    m = 0xFFFFFFFF
+    h = ((i * 0x9E3779B1) & m) ^ ((p * 0x85EBCA77 + 0x165667B1) & m)
+    h ^= h >> 15
+    h = (h * 0x2C1B3C6D) & m
+    h ^= h >> 12
+    return 1.0 if (h & 1) else -1.0
+
+
+def features(C, threshold=0.0, probes=8):
+    """The 64 features of a whitened matrix C (n x n Hermitian), as the GPU forms them from
+    its lower triangle, with f = |C|_F: the 32 largest |C_ii| / f; log(n)/log(4096); trace /
+    f; threshold / f; fraction of C_ii above the threshold; sum |C_ii| / f; sum C_ii^2 /
+    f^2; largest squared row norm / f^2; sum of row norms^4 / f^4; fraction of rows with
+    squared norm above f^2 / n; sum of C_ii above the threshold / f; C_ii at the ranks n/8,
+    n/4, n/2, 3n/4 (descending) / f; then the spectral moments t_k = mean over the probes z
+    of z^H C^k z (k = 1..6) and their combinations (t3 / f^3, t4 / f^4, t5 / f^5, t6 / f^6,
+    effective ranks f^4 / t4 and (f^6 / t6)^(1/2) over n, t4^2 / (t6 f^2), t3^2 / (t4 f^2),
+    t5 / (t4 f), the effective ranks' logarithms / log(n), t1 t3 / f^4, t3 / (f t4^(1/2)),
+    t5 / (t4 t6)^(1/2), t2 / f^2, t1 / f, and their ratio); last, the 16 largest rows'
+    share of f^2."""
     C = np.asarray(C, dtype=np.complex128)
     n = C.shape[0]
     f = np.zeros(F)
@@ -83,21 +98,35 @@ def features(C, threshold=0.0):
     fro = np.sqrt(fro2)
     a = np.sort(np.abs(dg))[::-1][:32]
     f[:a.size] = a / fro
-    r = np.sqrt(np.sort(r2)[::-1][:16])
-    f[32:32 + r.size] = r / fro
-    f[48] = np.log(n) / np.log(4096.0)
-    f[49] = dg.sum() / fro
-    f[50] = threshold / fro
-    f[51] = np.count_nonzero(dg > threshold) / n
-    f[52] = np.abs(dg).sum() / fro
-    f[53] = (dg ** 2).sum() / fro2
-    f[54] = r2.max() / fro2
-    f[55] = (r2 ** 2).sum() / fro2 ** 2
-    f[56] = dg.sum() / (fro * np.sqrt(n))
-    f[57] = np.count_nonzero(r2 > fro2 / n) / n
-    f[58] = dg[dg > threshold].sum() / fro
+    ln = np.log(n)
+    f[32] = ln / np.log(4096.0)
+    f[33] = dg.sum() / fro
+    f[34] = threshold / fro
+    f[35] = np.count_nonzero(dg > threshold) / n
+    f[36] = np.abs(dg).sum() / fro
+    f[37] = (dg ** 2).sum() / fro2
+    f[38] = r2.max() / fro2
+    f[39] = (r2 ** 2).sum() / fro2 ** 2
+    f[40] = np.count_nonzero(r2 > fro2 / n) / n
+    f[41] = dg[dg > threshold].sum() / fro
     sd = np.sort(dg)[::-1]
     for k, q in enumerate((n // 8, n // 4, n // 2, (3 * n) // 4)):
-        f[59 + k] = sd[q] / fro
-    f[63] = (r[:16] ** 2).sum() / fro2
+        f[42 + k] = sd[q] / fro
+    if probes:
+        Z = np.array([[probe_sign(i, p) for p in range(probes)] for i in range(n)])
+        Y1 = C @ Z
+        Y2 = C @ Y1
+        Y3 = C @ Y2
+        t1 = np.sum(Z * Y1.real) / probes
+        t2 = np.sum(np.abs(Y1) ** 2) / probes
+        t3 = np.sum((np.conj(Y1) * Y2).real) / probes
+        t4 = np.sum(np.abs(Y2) ** 2) / probes
+        t5 = np.sum((np.conj(Y2) * Y3).real) / probes
+        t6 = np.sum(np.abs(Y3) ** 2) / probes
+        er4, er6 = fro2 ** 2 / t4, np.sqrt(fro2 ** 3 / t6)
+        f[46:63] = [t3 / fro ** 3, t4 / fro ** 4, t5 / fro ** 5, t6 / fro ** 6, er4 / n, er6 / n,
+                    t4 * t4 / (t6 * fro2), t3 * t3 / (t4 * fro2), t5 / (t4 * fro), np.log(er4) / ln,
+                    np.log(er6) / ln, t1 * t3 / fro ** 4, t3 / (fro * np.sqrt(t4)), t5 / np.sqrt(t4 * t6),
+                    t2 / fro2, t1 / fro, er4 / er6]
+    f[63] = np.sort(r2)[::-1][:16].sum() / fro2
     return f

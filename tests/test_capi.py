@@ -77,7 +77,7 @@ def test_null_handles_are_rejected_without_a_gpu():
 
     lib = _lib.load()
     for name, argtypes in _lib.SIGNATURES.items():
-        if name in ("bipp_last_error", "bipp_kernel_launch_count", "bipp_rank_mlp_num_params"):
+        if name in ("bipp_last_error", "bipp_kernel_launch_count", "bipp_rank_mlp_num_params", "bipp_tuning_reset"):
             continue
         args = []
         for t in argtypes:
@@ -143,3 +143,33 @@ def test_pybipp_surface():
                                                                        "image_prop", "image_file_name"]
     assert all(hasattr(config, f) for f in ("cuda", "rocm", "umpire", "omp", "mpi"))
     assert (communicator.local().rank, communicator.local().size) == (0, 1)
+
+
+def test_tuning_table_without_a_gpu(tmp_path):
+    """The autotuner's table of launch parameters (no device needed): defaults, candidate
+    checks, save / load round trip, the environment file, reset."""
+    import bipp_b200 as bipp
+
+    bipp.tuning_reset()
+    assert bipp.tuning_get("spread.items_cap") == 4096 and bipp.tuning_get("hetrd.threads") == 0
+    desc = bipp.tuning_describe()
+    assert set(desc) == {"spread.items_cap", "spread.ctas_per_sm", "hetrd.threads", "vv.ctas_per_sm",
+                         "direct.ctas_per_sm"}
+    assert desc["spread.items_cap"]["candidates"] == [2048, 4096, 8192]
+    with pytest.raises(bipp.InvalidParameterError):
+        bipp.tuning_set("spread.items_cap", 1000)
+    with pytest.raises(bipp.InvalidParameterError):
+        bipp.tuning_get("no.such.parameter")
+    bipp.tuning_set("spread.items_cap", 8192)
+    bipp.tuning_set("hetrd.threads", 512)
+    f = tmp_path / "tune.txt"
+    bipp.tuning_save(str(f))
+    bipp.tuning_reset()
+    assert bipp.tuning_get("spread.items_cap") == 4096
+    bipp.tuning_load(str(f))
+    assert bipp.tuning_get("spread.items_cap") == 8192 and bipp.tuning_get("hetrd.threads") == 512
+    bad = tmp_path / "bad.txt"
+    bad.write_text("vv.ctas_per_sm 7\n")
+    with pytest.raises(bipp.InvalidParameterError):
+        bipp.tuning_load(str(bad))
+    bipp.tuning_reset()

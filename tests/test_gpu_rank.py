@@ -51,17 +51,35 @@ def test_mlp_adam_step_and_training(ctx):
     model, X, _ = _random_model(2, n=512)
     y = (0.4 + 0.2 * np.tanh(X[:, 0] / 3) - 0.1 * np.tanh(X[:, 5] * X[:, 9] / 4)).astype(np.float32)
     _, g = rank.gradient(model, X, y, ctx=ctx)
-    m1, h1 = rank.train(model, X, y, iterations=1, lr=1e-3, ctx=ctx)
+    m1, h1, _ = rank.train(model, X, y, iterations=1, lr=1e-3, ctx=ctx)
     step = m1.astype(np.float64) - model
     expect = -1e-3 * g / (np.abs(g) + 1e-8)
     big = np.abs(g) > 1e-5
     assert np.all(step[:om.OFF["W1"]] == 0)
     assert np.abs(step[big] - expect[big]).max() <= 2e-6
-    trained, hist = rank.train(model, X, y, iterations=1500, lr=2e-3, ctx=ctx)
+    trained, hist, _ = rank.train(model, X, y, iterations=1500, lr=2e-3, ctx=ctx)
     print(f"loss {hist[0]:.4f} -> {hist[-1]:.5f}")
     assert hist[-1] <= 0.05 * hist[0]
     lfin, _ = om.loss_and_gradient(trained, X, y)
     assert lfin <= 0.05 * hist[0]
+
+
+def test_training_keeps_the_best_validation_model(ctx):
+    """With a validation set the returned model is the one of lowest validation loss
+    (checked with the numpy oracle), and weight decay shrinks the weights."""
+    from bipp_b200 import rank
+
+    model, X, _ = _random_model(4, n=400)
+    y = (0.5 + 0.3 * np.tanh(X[:, 1] / 2)).astype(np.float32)
+    Xv, yv = X[300:], y[300:]
+    trained, hist, vh = rank.train(model, X[:300], y[:300], iterations=600, lr=2e-3, val_feats=Xv,
+                                   val_targets=yv, eval_every=50, ctx=ctx)
+    lv, _ = om.loss_and_gradient(trained, Xv, yv)
+    assert abs(lv - vh.min()) <= 1e-4 * max(vh.min(), 1e-6) + 1e-7
+    plain, _, _ = rank.train(model, X[:300], y[:300], iterations=300, lr=2e-3, ctx=ctx)
+    decayed, _, _ = rank.train(model, X[:300], y[:300], iterations=300, lr=2e-3, weight_decay=0.5, ctx=ctx)
+    w = slice(om.OFF["W1"], om.N_PARAMS)
+    assert np.linalg.norm(decayed[w]) < np.linalg.norm(plain[w])
 
 
 def test_features_against_numpy_whitened_matrix(ctx):
@@ -97,7 +115,7 @@ def _vv(v, d, thr):
 
 
 def test_predicted_partial_solve_study(ctx):
-    """Train on 1024 method-generated steps, solve 512 others: the predicted partial
+    """Train on 2000 method-generated steps, solve 512 others: the predicted partial
     solve (k + 16 eigenpairs, fallback to full) returns the full solve's eigenvalues above
     the threshold, computes fewer eigenvectors and takes less device time than the full
     solve; the exact Sturm-count range solve is reported beside it."""
@@ -105,12 +123,12 @@ def test_predicted_partial_solve_study(ctx):
     from bipp_b200 import simulate as sim
 
     obs = sim.observation(sim.config_c4())
-    r = rank.study(ctx, obs, n_train=1024, n_eval=512, iterations=2000, lr=1e-3)
+    r = rank.study(ctx, obs, n_train=2000, n_eval=512, iterations=3000, lr=1e-3)
     r.pop("model")
     print(r)
     assert r["loss_last"] < 0.2 * r["loss_first"]
     assert r["eig_err_vs_full_normwise"] <= 1e-6
-    assert r["fallback_rate"] <= 0.25
+    assert r["fallback_rate"] <= 0.1
     v = r["vectors_per_step"]
     assert v["predicted"] < v["full"] and v["exact"] <= v["predicted"]
     assert r["eigensolver_ms"]["predicted"] < r["eigensolver_ms"]["full"]

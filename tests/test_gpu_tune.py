@@ -1,0 +1,51 @@
+"""GPU: the autotuner of launch shapes (bipp_autotune_pipeline). It times every candidate
+of the tunable parameters on a sample batch, keeps the fastest in the tuning table,
+leaves the pipeline's images untouched, and the images computed with the tuned values
+agree with those of the defaults (1e-5 relative L2 per level; only the summation order
+of the spreading and the tridiagonalisation changes)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_autotune_pipeline(ctx):
+    import torch
+
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+    from bipp_b200.parameter_estimator import infer_intervals
+
+    bipp.tuning_reset()
+    cfg = sim.config_c2(n_antenna=256, n_steps=64, image_size=256, n_src=100, keep=(200, 256))
+    obs = sim.observation(cfg)
+    dev = torch.device("cuda", 0)
+    s, x = sim.visibilities(obs, list(range(64)), device=dev, dtype=torch.complex64, masks=sim.keep_masks(cfg))
+    S = s.transpose(1, 2).contiguous()
+    wl = torch.full((64,), cfg.wl, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    _, d, _, _ = bipp.eigh_gram_batched(np.full(8, cfg.wl, np.float32), s[:8].cpu().numpy(), x[:8].cpu().numpy(),
+                                        ctx=ctx)
+    intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d)
+    n = cfg.image_size
+    l = obs.lmn[:, 0].reshape(n, n)
+    m = obs.lmn[:, 1].reshape(n, n)
+    lat = (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lat, obs.lmn[:, 2], obs.basis, tolerance=cfg.eps,
+                       chunk_steps=64, max_steps=64)
+    pl.process_device(64, S.data_ptr(), x.data_ptr(), wl.data_ptr())
+    base = pl.images().astype(np.float64)
+    rep = pl.autotune(64, S.data_ptr(), x.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
+    print(rep)
+    desc = bipp.tuning_describe()
+    for name in ("spread.items_cap", "spread.ctas_per_sm", "hetrd.threads", "vv.ctas_per_sm"):
+        assert rep[name]["chosen"] == desc[name]["value"]
+        assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
+    assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
+    pl.reset()
+    pl.process_device(64, S.data_ptr(), x.data_ptr(), wl.data_ptr())
+    tuned = pl.images().astype(np.float64)
+    for lv in range(tuned.shape[0]):
+        assert np.linalg.norm(tuned[lv] - base[lv]) <= 1e-5 * np.linalg.norm(base[lv]), lv
+    pl.close()
+    bipp.tuning_reset()
