@@ -12,6 +12,11 @@
 #include "bipp/bipp.hpp"
 #include "bipp_b200.h"
 
+namespace bippb200 {
+void tcp_reduce_sum_to_root(const char* host, int port, std::size_t rank, std::size_t size, float* data,
+                            std::size_t count, double timeoutSec);
+}  // namespace bippb200
+
 namespace bipp {
 
 [[noreturn]] static void throw_code(BippError code) {
@@ -43,10 +48,49 @@ auto Communicator::world() -> Communicator {
   const char* s = std::getenv("WORLD_SIZE");
   c.rank_ = r ? std::strtoull(r, nullptr, 10) : 0;
   c.size_ = s ? std::max<std::size_t>(1, std::strtoull(s, nullptr, 10)) : 1;
+  if (c.rank_ >= c.size_) throw InvalidParameterError("RANK must be below WORLD_SIZE");
+  if (c.size_ > 1) {
+    // images are summed into rank 0 over TCP, on MASTER_ADDR and a port of its own
+    const char* host = std::getenv("MASTER_ADDR");
+    const char* rp = std::getenv("BIPP_B200_REDUCE_PORT");
+    const char* mp = std::getenv("MASTER_PORT");
+    const char* to = std::getenv("BIPP_B200_REDUCE_TIMEOUT");
+    const std::string h = (host && *host) ? host : "127.0.0.1";
+    const int port = (rp && *rp) ? std::atoi(rp) : (mp && *mp) ? std::atoi(mp) + 17 : -1;
+    const double timeout = (to && *to) ? std::atof(to) : 300.0;
+    const std::size_t rank = c.rank_, size = c.size_;
+    c.reduce_ = [h, port, rank, size, timeout](float* data, std::size_t count) {
+      if (port <= 0 || port > 65535)
+        throw InvalidParameterError("set MASTER_PORT or BIPP_B200_REDUCE_PORT for the image reduction of world()");
+      bippb200::tcp_reduce_sum_to_root(h.c_str(), port, rank, size, data, count, timeout);
+    };
+  }
   return c;
 }
 
 auto Communicator::local() -> Communicator { return Communicator(); }
+
+auto Communicator::custom(std::size_t rank, std::size_t size, ReduceFn reduceSumToRoot) -> Communicator {
+  if (size < 1 || rank >= size) throw InvalidParameterError("communicator rank must be below its size");
+  if (size > 1 && !reduceSumToRoot) throw InvalidParameterError("a communicator of several ranks needs a reduction");
+  Communicator c;
+  c.rank_ = rank;
+  c.size_ = size;
+  c.reduce_ = std::move(reduceSumToRoot);
+  return c;
+}
+
+void Communicator::reduce_sum_to_root(float* data, std::size_t count) const {
+  if (size_ <= 1) return;
+  if (!reduce_) throw InvalidParameterError("this communicator has no reduction");
+  try {
+    reduce_(data, count);
+  } catch (const GenericError&) {
+    throw;
+  } catch (const std::exception& e) {
+    throw GenericError(e.what());
+  }
+}
 
 class ContextInternal {
 public:
@@ -182,26 +226,62 @@ void image_synthesis(Context& ctx, const NufftSynthesisOptions& opt, Dataset& da
   }
   if (tags.empty()) throw InvalidParameterError("Empty selection");
   const std::size_t nSamples = selection[tags[0]].size();
+  const Communicator& comm = ctx.communicator();
+  const std::size_t nRanks = comm.size(), rank = comm.rank();
+  // several ranks: the selection is sorted by sample id and checked as a whole, then each
+  // rank images a contiguous block of ceil(n / size) samples (src/image_synthesis.cpp:52-80;
+  // a rank whose block starts past the end images none)
+  if (nRanks > 1) {
+    for (const auto& t : tags) {
+      auto& smp = selection[t];
+      std::sort(smp.begin(), smp.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      if (std::adjacent_find(smp.begin(), smp.end(), [](const auto& a, const auto& b) { return a.first == b.first; }) !=
+          smp.end())
+        throw InvalidParameterError("Selection sample id duplicate");
+      if (smp.back().first >= dataset.num_samples())
+        throw InvalidParameterError("Selection sample id exceeds number of dataset samples");
+      if (smp.size() != nSamples)
+        throw InvalidParameterError("Selection must contain the same sample ids for all images.");
+      for (std::size_t i = 0; i < nSamples; ++i)
+        if (smp[i].first != selection[tags[0]][i].first)
+          throw InvalidParameterError("Selection must contain the same sample ids for all images.");
+    }
+  }
+  const std::size_t per = (nSamples + nRanks - 1) / nRanks;
+  const std::size_t begin = std::min(nSamples, rank * per);
+  const std::size_t nLocal = nRanks > 1 ? std::min(per, nSamples - begin) : nSamples;
   std::vector<std::size_t> ids;
   std::vector<const float*> ev;
   for (const auto& t : tags) {
     if (selection[t].size() != nSamples)
       throw InvalidParameterError("Selection must contain the same sample ids for all images.");
-    for (const auto& [id, p] : selection[t]) {
-      ids.push_back(id);
-      ev.push_back(p);
+    for (std::size_t i = begin; i < begin + nLocal; ++i) {
+      ids.push_back(selection[t][i].first);
+      ev.push_back(selection[t][i].second);
     }
   }
   const std::size_t nPixel = imageProp.width() * imageProp.height();
   std::vector<float> lmn(nPixel * 3);
   imageProp.pixel_lmn(lmn.data(), nPixel);
-  std::vector<float> images(tags.size() * nPixel);
+  std::vector<float> images(tags.size() * nPixel, 0.f);
   bipp_dataset_callbacks cb{&dataset,         &DatasetThunk::num_samples, &DatasetThunk::num_antenna,
                             &DatasetThunk::num_beam, &DatasetThunk::eig_vec, &DatasetThunk::eig_val,
                             &DatasetThunk::uvw,      &DatasetThunk::wl,      &DatasetThunk::scale};
-  const bipp_nufft_options o = to_c(opt);
-  check(bipp_image_synthesis(InternalContextAccessor::get(ctx), &o, &cb, tags.size(), nSamples, ids.data(), ev.data(),
-                             nPixel, lmn.data(), nPixel, images.data()));
+  bipp_nufft_options o = to_c(opt);
+  if (nRanks > 1) o.normalizeImage = 0;   // normalised once, on rank 0, after the sum
+  if (nLocal)
+    check(bipp_image_synthesis(InternalContextAccessor::get(ctx), &o, &cb, tags.size(), nLocal, ids.data(), ev.data(),
+                               nPixel, lmn.data(), nPixel, images.data()));
+  if (nRanks > 1) {
+    // SUM of the images into rank 0 (src/image_synthesis.cpp:140-147), normalised there by
+    // the total number of samples (:152-163); only rank 0 writes the image
+    comm.reduce_sum_to_root(images.data(), images.size());
+    if (rank != 0) return;
+    if (opt.normalizeImage) {
+      const float sc = 1.f / (float)nSamples;
+      for (float& x : images) x *= sc;
+    }
+  }
   for (std::size_t i = 0; i < tags.size(); ++i) imageData.set(tags[i], images.data() + i * nPixel);
 }
 

@@ -173,3 +173,28 @@ def test_tuning_table_without_a_gpu(tmp_path):
     with pytest.raises(bipp.InvalidParameterError):
         bipp.tuning_load(str(bad))
     bipp.tuning_reset()
+
+
+def test_cxx_shell_image_reduction_over_three_ranks(tmp_path):
+    """The C++ API's Communicator::world() sums float arrays of three ranks (processes)
+    into rank 0 over TCP, exactly; custom() runs the caller's reduction
+    (tests/cxx/reduce_check.cpp). No GPU is needed."""
+    import socket
+    import subprocess
+
+    exe = tmp_path / "reduce_check"
+    libdir = os.path.join(ROOT, "bipp_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", os.path.join(ROOT, "tests", "cxx", "reduce_check.cpp"),
+                    "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include", "-L" + libdir,
+                    "-lbipp_b200", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(3):
+        env = dict(os.environ, RANK=str(r), WORLD_SIZE="3", MASTER_ADDR="127.0.0.1", BIPP_B200_REDUCE_PORT=str(port),
+                   BIPP_B200_REDUCE_TIMEOUT="60")
+        procs.append(subprocess.Popen([str(exe)], env=env, stderr=subprocess.PIPE, text=True))
+    for p in procs:
+        _, err = p.communicate(timeout=120)
+        assert p.returncode == 0, err
