@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c5", "c4"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c5", "c4", "c2-api"],
                     help="c2: 512 antennas, 2048 steps, 1024^2 px, 4 levels (the headline); c5: 1024 antennas, "
                          "8 frequency channels, 2048^2 px, 8 levels (bounded to --time-steps time steps); c4: the "
                          "learned rank predictor study (256 antennas; eigensolver only)")
@@ -75,7 +75,8 @@ def parse():
     a = ap.parse_args()
     dflt = {"c2": dict(time_steps=2048, antennas=512, image=1024, chunk_steps=2048),
             "c5": dict(time_steps=128, antennas=1024, image=2048, chunk_steps=592),
-            "c4": dict(time_steps=10000, antennas=256, image=256, chunk_steps=2000)}[a.workload]
+            "c4": dict(time_steps=10000, antennas=256, image=256, chunk_steps=2000),
+            "c2-api": dict(time_steps=128, antennas=512, image=1024, chunk_steps=128)}[a.workload]
     for k, v in dflt.items():
         if getattr(a, k) is None:
             setattr(a, k, v)
@@ -407,6 +408,59 @@ def run_rank_study(args):
     ctx.close()
 
 
+def run_api_synthesis(args):
+    """--workload c2-api: image synthesis through the reference-facing API, the way a
+    reference caller images a dataset (bipp::image_synthesis / pybipp image_synthesis over
+    a Dataset whose samples hold eigenvectors, eigenvalues, uvw, wl and scale): an
+    in-memory dataset of --time-steps steps of the 512-antenna workload (eigenpairs from
+    the library's batched eigh_gram), 4 energy-level images of the 1024^2 lattice. Timed:
+    the whole call (dataset reads through host callbacks, uvw copies, virtual visibilities
+    on the GPU written into the collectors, NUFFT, images back to the host)."""
+    import torch
+
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    torch.cuda.set_device(0)
+    ctx = bipp.Context("GPU", device=0)
+    n_steps = args.time_steps
+    cfg = sim.config_c2(n_steps=2048)
+    obs = sim.observation(cfg)
+    masks = sim.keep_masks(cfg)
+    steps = list(range(0, 2048, max(1, 2048 // n_steps)))[:n_steps]
+    s, x = sim.visibilities(obs, steps, masks=masks)
+    s, x = s.numpy(), x.numpy()
+    wl = np.full(len(steps), cfg.wl, np.float32)
+    v, d, nred, scale = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
+    from bipp_b200.parameter_estimator import infer_intervals
+
+    intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d[:64])
+    ds = bipp.InMemoryDataset(cfg.n_antenna, cfg.n_antenna)
+    for k in range(len(steps)):
+        ds.write(k, cfg.wl, scale[k], v[k], d[k], sim.baseline_uvw(obs, x[k]))
+    sel = {f"lvl{l}": {k: d[k] * ((d[k] >= lo) & (d[k] <= hi)) for k in range(len(steps))}
+           for l, (lo, hi) in enumerate(intervals)}
+    opt = bipp.NufftSynthesisOptions().set_tolerance(cfg.eps).set_normalize_image(True)
+    lmn = obs.lmn.astype(np.float32)
+    bipp.image_synthesis(ctx, opt, ds, {t: dict(list(m.items())[:2]) for t, m in sel.items()}, lmn)   # warm-up
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        bipp.image_synthesis(ctx, opt, ds, sel, lmn)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.median(times))
+    line = {"metric": "time-steps/s of image synthesis from a dataset (reference API) at 512 antennas, 1024^2 px",
+            "value": len(steps) / sec, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded observation of the workload's shape; eigenpairs precomputed)",
+            "config": {"workload": f"c2-api: {len(steps)} samples of the 512-antenna workload in an in-memory dataset, "
+                                   "4 energy-level images, 1024^2 lattice, eps 1e-5",
+                       "api": "bipp_b200.image_synthesis -> bipp_image_synthesis (the C++ bipp::image_synthesis "
+                              "calls the same entry point)"},
+            "s_per_call": sec}
+    print(json.dumps(line))
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -414,6 +468,9 @@ def main():
         return
     if args.workload == "c4":
         run_rank_study(args)
+        return
+    if args.workload == "c2-api":
+        run_api_synthesis(args)
         return
     import torch
     import torch.distributed as dist

@@ -263,8 +263,10 @@ BippError bipp_domain_partition_grid_d(bipp_ctx_t ctx, const size_t* dims, size_
 
 // image_synthesis over a callback dataset: validation (src/image_synthesis.cpp:36-69),
 // per-sample uvw scaling by 2 pi / wl (src/nufft_synthesis.cpp:149-155), virtual
-// visibilities per image (src/nufft_synthesis.cpp:157-162) on the GPU, collect/get
-// NUFFT, normalisation by the number of samples (src/image_synthesis.cpp:336-347).
+// visibilities of all images of a sample (src/nufft_synthesis.cpp:157-162) by one GPU
+// launch per group of four images, written straight into the collectors' device staging
+// buffers (no device-host round trip), collect/get NUFFT, normalisation by the number of
+// samples (src/image_synthesis.cpp:152-163).
 BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, const bipp_dataset_callbacks* ds,
                                size_t nImages, size_t nSamples, const size_t* sampleIds, const float* const* eigvals,
                                size_t nPixel, const float* lmn, size_t ldlmn, float* images) {
@@ -293,12 +295,17 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
     const size_t nB = nAnt * nAnt;
     std::vector<std::complex<float>> v(nAnt * nBeam);
     std::vector<float> uvw(nB * 3);
-    std::vector<std::complex<float>> vvAll(nB * nImages);
-    // device buffers for virtual visibilities
-    DevBuf dV(ctx, v.size() * sizeof(float2)), dK(ctx, nBeam * sizeof(float)), dVV(ctx, nB * sizeof(float2)),
-        dn(ctx, 3 * sizeof(int));
-    int hn[3] = {(int)nAnt, 0, (int)nBeam};
-    h2d(ctx, dn.get(), hn, sizeof(hn));
+    // eigenvectors, per-image column scales and the GEMM's sizes on the device; the virtual
+    // visibilities are written straight into the collectors' staging buffers
+    DevBuf dV(ctx, v.size() * sizeof(float2)), dK(ctx, nImages * nBeam * sizeof(float)),
+        dn(ctx, 3 * 4 * sizeof(int));
+    std::vector<int> hn(12);
+    for (int i = 0; i < 4; ++i) {
+      hn[i] = (int)nAnt;          // matrix size of every image of a group
+      hn[4 + i] = 0;              // first column
+      hn[8 + i] = (int)nBeam;     // end column
+    }
+    h2d(ctx, dn.get(), hn.data(), hn.size() * sizeof(int));
     // collectors in groups of 4 images
     std::vector<bipp_nufft_t> plans;
     for (size_t g0 = 0; g0 < nImages; g0 += 4) {
@@ -318,7 +325,7 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
     } cleanup{plans};
     // 2 pi rounded to float, as the reference's T(2 * pi) with T = float
     const float twoPi = static_cast<float>(2.0 * 3.14159265358979323846);
-    std::vector<float> ks(nBeam);
+    std::vector<float> ks(nImages * nBeam);
     for (size_t k = 0; k < nSamples; ++k) {
       const size_t id = sampleIds[order[0][k]];
       const float wl = ds->wl(ds->user, id);
@@ -328,28 +335,35 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
       // uvw scaled in single precision as the reference's float path
       const float uvwScale = twoPi / wl;   // float division (src/nufft_synthesis.cpp:150-154)
       for (auto& x : uvw) x *= uvwScale;
-      h2d(ctx, dV.get(), v.data(), v.size() * sizeof(float2));
       for (size_t im = 0; im < nImages; ++im) {
         const float* d = eigvals[im * nSamples + order[im][k]];
-        for (size_t c = 0; c < nBeam; ++c) ks[c] = scale * d[c];
-        h2d(ctx, dK.get(), ks.data(), nBeam * sizeof(float));
+        for (size_t c = 0; c < nBeam; ++c) ks[im * nBeam + c] = scale * d[c];
+      }
+      h2d(ctx, dV.get(), v.data(), v.size() * sizeof(float2));
+      h2d(ctx, dK.get(), ks.data(), ks.size() * sizeof(float));
+      for (size_t g0 = 0, gi = 0; g0 < nImages; g0 += 4, ++gi) {
+        bipp_nufft_t pl = plans[gi];
+        const long long ld = nufft_stage_ld(pl);
+        float* su = nufft_stage_uvw(pl);
+        for (int c = 0; c < 3; ++c) h2d(ctx, su + c * ld, uvw.data() + c * nB, nB * sizeof(float));
+        // VV of the group's images in one launch: "matrix" b = image g0 + b, the same
+        // eigenvectors, its own column scales, output into the image's staging slot
+        const int nIm = (int)std::min<size_t>(4, nImages - g0);
         GemmArgs<float2> g{};
-        g.A = dV.get<float2>(); g.lda = (int)nAnt; g.opA = 0;
-        g.B = dV.get<float2>(); g.ldb = (int)nAnt; g.opB = 1;
-        g.Cm = dVV.get<float2>(); g.ldc = (int)nAnt;
+        g.A = dV.get<float2>(); g.strideA = 0; g.lda = (int)nAnt; g.opA = 0;
+        g.B = dV.get<float2>(); g.strideB = 0; g.ldb = (int)nAnt; g.opB = 1;
+        g.Cm = nufft_stage_values(pl, 0); g.strideC = ld; g.ldc = (int)nAnt;
         g.n = dn.get<int>(); g.outMode = 0; g.levels = 1;
-        g.kscale = dK.get(); g.kbeg = dn.get<int>() + 1; g.kend = dn.get<int>() + 2;
+        g.kscale = dK.get<float>() + g0 * nBeam; g.strideK = (long long)nBeam;
+        g.kbeg = dn.get<int>() + 4; g.kend = dn.get<int>() + 8;
         const int tiles = ((int)nAnt + kGemmBM - 1) / kGemmBM;
         count_launch();
-        gemm_kernel<float2, float><<<dim3(tiles, tiles, 1), kGemmThreads, 0, ctx->stream>>>(g);
+        gemm_kernel<float2, float><<<dim3(tiles, tiles, nIm), kGemmThreads, 0, ctx->stream>>>(g);
         B2_CHECK_LAUNCH();
-        d2h(ctx, vvAll.data() + im * nB, dVV.get(), nB * sizeof(float2));
+        nufft_commit(pl);
       }
+      // the host staging arrays are rewritten for the next sample
       sync(ctx);
-      for (size_t g0 = 0, gi = 0; g0 < nImages; g0 += 4, ++gi) {
-        const BippError e = bipp_nufft_add_s(plans[gi], uvw.data(), nB, vvAll.data() + g0 * nB, nB);
-        if (e != BIPP_SUCCESS) throw Error(e, bipp_last_error());
-      }
     }
     for (size_t im = 0; im < nImages; ++im) {
       const BippError e = bipp_nufft_get_image(plans[im / 4], im % 4, images + im * nPixel);

@@ -620,6 +620,18 @@ __global__ void d2f_kernel(const double* __restrict__ in, long long n, float* __
     out[i] = (float)in[i];
 }
 
+namespace bippb200 {
+float* nufft_stage_uvw(bipp_nufft_t p) { return p->uvw.get<float>() + p->count * p->nBaselines; }
+float2* nufft_stage_values(bipp_nufft_t p, size_t im) {
+  return p->values.get<float2>() + im * (long long)p->batch * p->nBaselines + p->count * p->nBaselines;
+}
+long long nufft_stage_ld(bipp_nufft_t p) { return (long long)p->batch * p->nBaselines; }
+void nufft_commit(bipp_nufft_t p) {
+  ++p->count;
+  if (p->count >= p->batch) nufft_transform(p);
+}
+}  // namespace bippb200
+
 extern "C" {
 
 BippError bipp_nufft_create(bipp_ctx_t ctx, const bipp_nufft_options* opt, size_t nPixel, const float* lmn,
@@ -714,6 +726,7 @@ static void nufft_add(bipp_nufft_t plan, const void* uvw, size_t lduvw, const vo
   ++p->count;
   if (p->count >= p->batch) nufft_transform(p);
 }
+
 
 BippError bipp_nufft_add_s(bipp_nufft_t plan, const float* uvw, size_t lduvw, const void* values, size_t ldvalues) {
   return guard([&] { nufft_add(plan, uvw, lduvw, values, ldvalues, false); });

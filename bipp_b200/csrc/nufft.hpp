@@ -87,6 +87,17 @@ public:
   ~NufftCore();
 };
 
+// Staging of one sample of a collect/get plan (bipp_nufft_create) in device memory: the
+// caller writes the sample's scaled uvw at nufft_stage_uvw (three coordinate arrays of
+// nBaselines floats, ld nufft_stage_ld) and the values of image im at
+// nufft_stage_values(plan, im) (nBaselines complex floats) on the plan's stream, then
+// nufft_commit adds the sample (transforming the batch when it is full), as
+// bipp_nufft_add_s does for host arrays.
+float* nufft_stage_uvw(bipp_nufft_t p);
+float2* nufft_stage_values(bipp_nufft_t p, size_t im);
+long long nufft_stage_ld(bipp_nufft_t p);
+void nufft_commit(bipp_nufft_t p);
+
 // Gauss-Legendre nodes/weights on [-1, 1]
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
 
