@@ -42,9 +42,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// bounded wait for the completion of phase `parity` of the barrier
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kTcSpin; ++i) {
+// bounded wait (at most `spins` tries) for the completion of phase `parity` of the barrier
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int spins = kTcSpin) {
+  for (int i = 0; i < spins; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"

@@ -352,6 +352,12 @@ BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double
 BIPP_B200_EXPORT BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);
 
+/* Self-test of the bounded tensor-core barrier waits (no counterpart in the reference):
+ * waits with the given spin limit (1 to 2^20) on a barrier that nothing completes; the
+ * wait gives up, *timedOut is set to 1 and the call fails with BIPP_GPU_ERROR, the way a
+ * stuck MMA reaches the caller; the context stays usable. */
+BIPP_B200_EXPORT BippError bipp_selftest_wait_timeout(bipp_ctx_t ctx, int spins, int* timedOut);
+
 /* ---- autotuner of launch shapes (no counterpart in the reference, whose only launch-shape
  * logic is the fixed block-size ladder of src/gpu/kernels/nuft_sum.cu:73-84) ------------ */
 

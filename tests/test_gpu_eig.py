@@ -77,6 +77,24 @@ def test_synthetic_eigh_standard(ctx, prec):
         assert _rel(_prod(v, d), _prod(g["sv_f64"][k], g["sd_f64"][k])) <= tol_p
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_lofar_eigh_general_w(ctx, prec):
+    """The standard eigh (no Gram matrix) with the LOFAR input's complex beamforming W:
+    eigenvalues and the beamformed V diag(d) V^H (v = W_red X) against the oracle, which
+    is pinned to the compiled reference on beamformed problems."""
+    import bipp_b200 as bipp
+
+    g = golden("lofar.npz")
+    dt, ct = (np.float64, np.complex128) if prec == "f64" else (np.float32, np.complex64)
+    tol_d, tol_p = (1e-10, 1e-9) if prec == "f64" else (1e-5, 1e-4)
+    for k in range(g["s"].shape[0]):
+        v, d, nr, sc = bipp.eigh(dt(g["wl"]), g["s"][k].astype(ct), g["w"][k].astype(ct), ctx=ctx, full=True)
+        vr, dr, nrr, scr = bb.eigh(float(dt(g["wl"])), g["s"][k].astype(ct), g["w"][k].astype(ct), dtype=dt)
+        assert nr == nrr and abs(sc - scr) <= 1e-6 * scr
+        assert _rel(d, dr) <= tol_d
+        assert _rel(_prod(v, d), _prod(vr, dr)) <= tol_p
+
+
 def test_eigenvector_g_orthonormality(ctx):
     import bipp_b200 as bipp
 
@@ -285,3 +303,23 @@ def test_virtual_vis(ctx, prec):
             ref_vv = g[f"vv_{prec}"][k][lv]
             scale = max(np.abs(ref_vv).max(), 1e-30)
             assert np.abs(vv - ref_vv).max() <= (1e-12 if prec == "f64" else 1e-5) * scale
+
+
+def test_bounded_barrier_wait_reports_timeout(ctx):
+    """The bounded wait of the tensor-core kernels on a barrier that nothing completes
+    (bipp_selftest_wait_timeout, a short spin limit): it gives up, the call fails with
+    BIPP_GPU_ERROR (GPUError), and the context still runs the tensor-core eigensolver."""
+    import ctypes as C
+
+    import bipp_b200 as bipp
+    from bipp_b200._lib import check
+
+    out = C.c_int(0)
+    with pytest.raises(bipp.GPUError):
+        check(ctx._lib.bipp_selftest_wait_timeout(ctx.handle, 2000, C.byref(out)))
+    assert out.value == 1
+    g = golden("synth_eig.npz")
+    n = g["s"].shape[1]
+    v, d, nr, sc = bipp.eigh_gram_full(np.float32(g["wl"]), g["s"][0].astype(np.complex64), np.eye(n, dtype=np.complex64),
+                                       g["xyz"][0].astype(np.float32), ctx=ctx)
+    assert _rel(d, g["d_f64"][0]) <= 1e-5

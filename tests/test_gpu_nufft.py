@@ -100,6 +100,35 @@ def test_nufft_collect_get_lattice(ctx, tol):
     plan.close()
 
 
+def test_nufft_collect_get_four_images_warp_spreader(ctx):
+    """Four images on a make_grids lattice with the first-order residual channels active:
+    12 channels, more than the tensor-core spreader takes, so the warp spreader with
+    shared-memory atomics runs; against the FP64 direct sum of the same float inputs."""
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    rng = np.random.default_rng(9)
+    lmn = sim.make_lmn_grid(48, math.radians(12.0)).astype(np.float32)
+    tol = 1e-5
+    plan = bipp.NufftSynthesis(ctx, bipp.NufftSynthesisOptions().set_tolerance(tol), lmn, 4, 600)
+    pts = []
+    for _ in range(3):
+        u, v = rng.uniform(-4000.0, 4000.0, (2, 600))
+        w = rng.uniform(-300.0, 300.0, 600)
+        uvw = np.stack([u, v, w], 1).astype(np.float32)
+        c = (rng.standard_normal((600, 4)) + 1j * rng.standard_normal((600, 4))).astype(np.complex64)
+        plan.add(uvw, c)
+        pts.append((uvw, c))
+    imgs = [plan.get_image(i) for i in range(4)]
+    uvw = np.concatenate([p[0] for p in pts]).astype(np.float64)
+    c = np.concatenate([p[1] for p in pts]).astype(np.complex128)
+    l64 = lmn.astype(np.float64)
+    for i in range(4):
+        ref_img = bb.nuft_sum(1.0, c[:, i], uvw[:, 0], uvw[:, 1], uvw[:, 2], l64[:, 0], l64[:, 1], l64[:, 2])
+        assert _rel_l2(imgs[i], ref_img) <= 20 * tol, i
+    plan.close()
+
+
 def test_nufft_collect_get_non_lattice(ctx):
     """Pixels that are not on a lattice use the direct FP64 evaluation."""
     import bipp_b200 as bipp
