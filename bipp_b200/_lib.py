@@ -72,6 +72,8 @@ SIGNATURES = {
     "bipp_rank_mlp_train": [_p, _p, _p, _p, _sz, _p, _p, _sz, _i, _f, _f, _i, _p, _p],
     "bipp_autotune_pipeline": [_p, _sz, _p, _p, _p, _i, _i, _p, _sz],
     "bipp_selftest_wait_timeout": [_p, _i, C.POINTER(_i)],
+    "bipp_pipeline_stage": [_p, _sz, _p, _p, _p],
+    "bipp_pipeline_process_staged": [_p],
     "bipp_tuning_get": [C.c_char_p, C.POINTER(_i)],
     "bipp_tuning_set": [C.c_char_p, _i],
     "bipp_tuning_describe": [_p, _sz],

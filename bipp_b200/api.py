@@ -696,6 +696,16 @@ class Pipeline:
         check(self.ctx._lib.bipp_pipeline_process(self.handle, int(n_steps), C.c_void_p(s_ptr), C.c_void_p(xyz_ptr),
                                                   C.c_void_p(wl_ptr), 0))
 
+    def stage_host_ptr(self, n_steps, s_ptr, xyz_ptr, wl_ptr):
+        """Copy a batch of host inputs (library layout, pinned for an asynchronous copy) into
+        a staging slot and return at once (bipp_pipeline_stage)."""
+        check(self.ctx._lib.bipp_pipeline_stage(self.handle, int(n_steps), C.c_void_p(s_ptr), C.c_void_p(xyz_ptr),
+                                                C.c_void_p(wl_ptr)))
+
+    def process_staged(self):
+        """Process the oldest staged batch (bipp_pipeline_process_staged)."""
+        check(self.ctx._lib.bipp_pipeline_process_staged(self.handle))
+
     def images_ptr(self, ptr, normalize=True, on_device=False):
         check(self.ctx._lib.bipp_pipeline_images(self.handle, C.c_void_p(ptr), 1 if normalize else 0,
                                                  1 if on_device else 0))

@@ -139,6 +139,24 @@ struct bipp_pipeline_s {
   double eigMs[kEigTimers] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<double> lastLam;
   std::vector<int> lastNred;
+  // staged host inputs (bipp_pipeline_stage): two slots, copied on their own stream so that
+  // the next batch's copy runs while the current one is processed
+  struct Staged {
+    DevBuf S, xyz, wl;
+    size_t steps = 0;
+    bool full = false;
+    cudaEvent_t copied = nullptr;    // the slot's copy is complete
+    cudaEvent_t consumed = nullptr;  // its processing no longer reads the slot
+  } staged[2];
+  int stageNext = 0, stageHead = 0;
+  cudaStream_t copyStream = nullptr;
+  ~bipp_pipeline_s() {
+    for (auto& st : staged) {
+      if (st.copied) cudaEventDestroy(st.copied);
+      if (st.consumed) cudaEventDestroy(st.consumed);
+    }
+    if (copyStream) cudaStreamDestroy(copyStream);
+  }
 };
 
 static void pipeline_alloc(bipp_pipeline_s* p, size_t steps) {
@@ -324,7 +342,7 @@ static void pipeline_count(bipp_pipeline_s* p, int s0, int nb, const std::vector
 // copied as blocks of 64 columns from each block's diagonal row down, one 3-D copy per
 // block over all steps (about 56 % of the bytes of the full matrices at 512 antennas).
 constexpr int kLowerCopyCols = 64;
-static void copy_lower_blocks(bipp_ctx_s* ctx, float2* dst, const float2* src, int N, int T) {
+static void copy_lower_blocks(cudaStream_t st, float2* dst, const float2* src, int N, int T) {
   for (int c0 = 0; c0 < N; c0 += kLowerCopyCols) {
     const int w = std::min(kLowerCopyCols, N - c0);
     cudaMemcpy3DParms prm = {};
@@ -334,7 +352,7 @@ static void copy_lower_blocks(bipp_ctx_s* ctx, float2* dst, const float2* src, i
     prm.dstPos = prm.srcPos;
     prm.extent = make_cudaExtent((size_t)(N - c0) * sizeof(float2), (size_t)w, (size_t)T);
     prm.kind = cudaMemcpyHostToDevice;
-    B2_CUDA(cudaMemcpy3DAsync(&prm, ctx->stream));
+    B2_CUDA(cudaMemcpy3DAsync(&prm, st));
   }
 }
 
@@ -369,7 +387,7 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   if (onDevice) {
     p->Sin = static_cast<const float2*>(s);
   } else {
-    copy_lower_blocks(ctx, p->S.get<float2>(), static_cast<const float2*>(s), N, T);
+    copy_lower_blocks(ctx->stream, p->S.get<float2>(), static_cast<const float2*>(s), N, T);
     p->Sin = p->S.get<float2>();
   }
   B2_CUDA(cudaMemcpyAsync(p->xyz.get(), xyz, (size_t)T * N * 3 * sizeof(double), kind, ctx->stream));
@@ -503,6 +521,60 @@ BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s
   return guard([&] {
     require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
     pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
+  });
+}
+
+BippError bipp_pipeline_stage(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz, const double* wl) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    require(s && xyz && wl, "null pointer", BIPP_INVALID_POINTER_ERROR);
+    require(nSteps > 0, "no steps");
+    bipp_ctx_s* ctx = pl->ctx;
+    auto& slot = pl->staged[pl->stageNext];
+    require(!slot.full, "both staging slots hold unprocessed batches; process one first");
+    const int N = (int)pl->nAnt;
+    if (!pl->copyStream) B2_CUDA(cudaStreamCreateWithFlags(&pl->copyStream, cudaStreamNonBlocking));
+    if (!slot.copied) {
+      B2_CUDA(cudaEventCreateWithFlags(&slot.copied, cudaEventDisableTiming));
+      B2_CUDA(cudaEventCreateWithFlags(&slot.consumed, cudaEventDisableTiming));
+      B2_CUDA(cudaEventRecord(slot.consumed, ctx->stream));
+    }
+    const size_t sB = nSteps * (size_t)N * N * sizeof(float2), xB = nSteps * (size_t)N * 3 * sizeof(double),
+                 wB = nSteps * sizeof(double);
+    if (slot.S.bytes() < sB || slot.xyz.bytes() < xB || slot.wl.bytes() < wB) {
+      slot.S.ensure(ctx, sB);
+      slot.xyz.ensure(ctx, xB);
+      slot.wl.ensure(ctx, wB);
+      sync(ctx);   // the slot's buffers exist before the copy stream writes them
+    }
+    // the previous batch of this slot must have been read before it is overwritten
+    B2_CUDA(cudaStreamWaitEvent(pl->copyStream, slot.consumed, 0));
+    copy_lower_blocks(pl->copyStream, slot.S.get<float2>(), static_cast<const float2*>(s), N, (int)nSteps);
+    B2_CUDA(cudaMemcpyAsync(slot.xyz.get(), xyz, nSteps * (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                            pl->copyStream));
+    B2_CUDA(cudaMemcpyAsync(slot.wl.get(), wl, nSteps * sizeof(double), cudaMemcpyHostToDevice, pl->copyStream));
+    B2_CUDA(cudaEventRecord(slot.copied, pl->copyStream));
+    slot.steps = nSteps;
+    slot.full = true;
+    pl->stageNext ^= 1;
+  });
+}
+
+BippError bipp_pipeline_process_staged(bipp_pipeline_t pl) {
+  return guard([&] {
+    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
+    auto& slot = pl->staged[pl->stageHead];
+    require(slot.full, "no staged batch (bipp_pipeline_stage)");
+    bipp_ctx_s* ctx = pl->ctx;
+    B2_CUDA(cudaStreamWaitEvent(ctx->stream, slot.copied, 0));
+    slot.full = false;
+    pl->stageHead ^= 1;
+    struct Release {
+      bipp_ctx_s* c;
+      cudaEvent_t e;
+      ~Release() { cudaEventRecord(e, c->stream); }
+    } release{ctx, slot.consumed};
+    pipeline_process(pl, slot.steps, slot.S.get(), slot.xyz.get<double>(), slot.wl.get<double>(), 1);
   });
 }
 

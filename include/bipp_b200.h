@@ -326,6 +326,16 @@ BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipel
  * BIPP_GPU_ERROR when a tensor-core completion wait runs out (a GPU fault). */
 BIPP_B200_EXPORT BippError bipp_pipeline_process(bipp_pipeline_t pl, size_t nSteps, const void* s,
                                                  const double* xyz, const double* wl, int onDevice);
+/* Double-buffered host input: bipp_pipeline_stage copies a batch (host arrays as for
+ * bipp_pipeline_process with onDevice 0; pinned memory lets the copy run asynchronously)
+ * into one of two device slots on a stream of its own and returns at once;
+ * bipp_pipeline_process_staged processes the oldest staged batch. Staging batch k + 1
+ * before processing batch k overlaps its copy with batch k's work. At most two batches
+ * wait (BIPP_INVALID_PARAMETER_ERROR otherwise); the host arrays must stay unchanged until
+ * the batch is processed. */
+BIPP_B200_EXPORT BippError bipp_pipeline_stage(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz,
+                                               const double* wl);
+BIPP_B200_EXPORT BippError bipp_pipeline_process_staged(bipp_pipeline_t pl);
 /* Images [nLevels][nPixel] (normalised by the number of processed steps if normalize),
  * to host (onDevice == 0) or device memory. */
 BIPP_B200_EXPORT BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize, int onDevice);
