@@ -294,11 +294,13 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
-# spreading launch, measured with ncu on one w-slab of a 128-step batch of this workload
-# (512 antennas, 1024^2 px, 4 levels); the traffic of a full launch scales with the points
-# and grid cells it processes, as the algorithmic bytes do.
-SPREAD_TRAFFIC_PER_ALG_BYTE = None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the
+# spreading kernel, measured with ncu over all three spreading launches of a 128-step
+# batch of this workload (512 antennas, 1024^2 px, 4 levels, 2 GB w-slabs): 4.773e9 DRAM
+# bytes for 5.493e9 algorithmic bytes. The traffic of a full launch is taken to scale with
+# the points and cells it processes, as the algorithmic bytes do (tiles without points are
+# cleared by their own kernel, so the ratio is below 1).
+SPREAD_TRAFFIC_PER_ALG_BYTE = 0.869
 
 
 def spread_roofline(stats, spread_ms, n_levels):
