@@ -36,6 +36,15 @@ struct NufftGeom {
   int ntx, nty, ntw;                // tile counts
 };
 
+// Fine-grid slab layout: cell (channel c, plane, y, x) of a slab of slabPlanes w-planes at
+// ((y nch + c) slabPlanes + plane) nx + x, i.e. [y][channel][plane][x]. With y outermost
+// the FFT's pass along y is one strided batch over every (channel, plane, x) column, and
+// its pass along x touches only the rows the pixels read, as two contiguous row blocks.
+__host__ __device__ __forceinline__ long long slab_index(const NufftGeom& g, int nch, int slabPlanes, int c, int plane,
+                                                       int y, int x) {
+  return (((long long)y * nch + c) * slabPlanes + plane) * g.nx + x;
+}
+
 // ES kernel exp(beta (sqrt(1 - z^2) - 1)), |z| < 1
 __device__ __forceinline__ float es_kernel(float z, float beta) {
   const float t = 1.0f - z * z;
@@ -564,13 +573,13 @@ spread_warp_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __
     }
   }
   __syncthreads();
-  // write the tile: grid[ch][plane][y][x], plane relative to the slab start
+  // write the tile into the slab layout (slab_index), plane relative to the slab start
   for (int i = threadIdx.x; i < nch * kTileCells; i += blockDim.x) {
     const int c = i / kTileCells, rem = i % kTileCells;
     const int lw = rem / (kTX * kTY), ly = (rem / kTX) % kTY, lx = rem % kTX;
     const int cell = tile_cell(lx, ly, lw, W);
     const float2 val = make_float2(sacc[(c * 2) * kTileCells + cell], sacc[(c * 2 + 1) * kTileCells + cell]);
-    const long long off = (((long long)c * slabPlanes + (twl * kTW + lw)) * g.ny + (y0 + ly)) * (long long)g.nx + (x0 + lx);
+    const long long off = slab_index(g, nch, slabPlanes, c, twl * kTW + lw, y0 + ly, x0 + lx);
     if (it.nparts == 1) {
       grid[off] = val;
     } else if (val.x != 0.f || val.y != 0.f) {
@@ -602,11 +611,10 @@ static __global__ void wsum_kernel(NufftGeom g, const float2* __restrict__ F, in
     for (int c = 0; c < kMaxChan; ++c) sum[c] = make_float2(0.f, 0.f);
     for (int j = 0; j < planesUsed; ++j) {
       const float fr = (float)er, fi = (float)ei;
-      const long long cell = ((long long)j * g.ny + ap) * g.nx + bp;
 #pragma unroll
       for (int c = 0; c < kMaxChan; ++c) {
         if (c < nch) {
-          const float2 f = F[(long long)c * slabPlanes * g.ny * g.nx + cell];
+          const float2 f = F[slab_index(g, nch, slabPlanes, c, j, ap, bp)];
           sum[c].x += f.x * fr - f.y * fi;
           sum[c].y += f.x * fi + f.y * fr;
         }

@@ -339,8 +339,6 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     if (!sOk) break;
     if (nvis > 0) {
       const int twl = tw - tw0;
-      const long long rowOff = (long long)(y0 + ym) * g.nx + (x0 + xm);
-      const long long planeStride = (long long)g.ny * g.nx;
       constexpr int PPB = 16 / (2 * CH);   // planes per 16-column block
 #pragma unroll
       for (int q = 0; q < S::N / 16; ++q) {
@@ -353,7 +351,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           for (int c = 0; c < CH; ++c) {
             if (c < nch) {
               const float2 v = make_float2(r[pl * 2 * CH + 2 * c], r[pl * 2 * CH + 2 * c + 1]);
-              float2* dst = grid + ((long long)c * slabPlanes + plane) * planeStride + rowOff;
+              float2* dst = grid + slab_index(g, nch, slabPlanes, c, plane, y0 + ym, x0 + xm);
               if (it.nparts == 1) {
                 *dst = v;
               } else {
@@ -390,11 +388,11 @@ clear_tiles_kernel(NufftGeom g, const int* __restrict__ list, int tw0, int slabP
   const int t = list[blockIdx.x];
   const int tx = t % g.ntx, ty = (t / g.ntx) % g.nty, tw = t / (g.ntx * g.nty);
   const int xm = threadIdx.x % kTX, ym = threadIdx.x / kTX;
-  const long long planeStride = (long long)g.ny * g.nx;
-  float2* p = grid + (long long)(tw - tw0) * kTW * planeStride + (long long)(ty * kTY + ym) * g.nx + (tx * kTX + xm);
   for (int c = 0; c < nch; ++c)
 #pragma unroll
-    for (int pl = 0; pl < kTW; ++pl) p[((long long)c * slabPlanes + pl) * planeStride] = make_float2(0.f, 0.f);
+    for (int pl = 0; pl < kTW; ++pl)
+      grid[slab_index(g, nch, slabPlanes, c, (tw - tw0) * kTW + pl, ty * kTY + ym, tx * kTX + xm)] =
+          make_float2(0.f, 0.f);
 }
 
 }  // namespace bippb200
