@@ -420,21 +420,22 @@ mlp_backward_kernel(const float* __restrict__ model, const float* __restrict__ X
 }
 
 // Adam step number *step + 1 on the trainable parameters [kOffW1, kMlpParams) (bias
-// corrections 1 - beta^t) with decoupled weight decay wd; the step counter lives on the
-// device so that one training iteration can be captured once in a CUDA graph and replayed
+// corrections 1 - beta^t) on the gradient of the loss plus the L2 penalty (l2 / 2) |W|^2
+// of the weights (not the biases); the step counter lives on the device so that one
+// training iteration can be captured once in a CUDA graph and replayed
 static __global__ void mlp_adam_kernel(float* __restrict__ model, const float* __restrict__ grad, float* __restrict__ m,
-                                float* __restrict__ v, float lr, float beta1, float beta2, float eps, float wd,
+                                float* __restrict__ v, float lr, float beta1, float beta2, float eps, float l2,
                                 const int* __restrict__ step) {
   const float tt = (float)(*step + 1);
   const float c1 = 1.f - powf(beta1, tt), c2 = 1.f - powf(beta2, tt);
   for (int i = kOffW1 + blockIdx.x * blockDim.x + threadIdx.x; i < kMlpParams; i += gridDim.x * blockDim.x) {
-    const float gi = grad[i];
+    const bool weight = i < kOffB1 || (i >= kOffW2 && i < kOffB2) || (i >= kOffW3 && i < kOffB3);
+    const float gi = grad[i] + (weight ? l2 * model[i] : 0.f);
     const float mi = beta1 * m[i] + (1.f - beta1) * gi;
     const float vi = beta2 * v[i] + (1.f - beta2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    // decoupled weight decay (AdamW), then the Adam step
-    model[i] -= lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * model[i]);
+    model[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
   }
 }
 

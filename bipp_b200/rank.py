@@ -47,13 +47,15 @@ def features(wl, s, xyz, threshold: float = 0.0, ctx: Optional[Context] = None):
 
 
 def init_model(feats, seed: int = 0, ctx: Optional[Context] = None) -> np.ndarray:
-    """A fresh model: the features' mean and standard deviation (1 for a constant
-    feature) and He-normal weights, zero biases."""
+    """A fresh model: the features' mean and standard deviation, the latter at least
+    1e-4 (every feature is scale free, and those that vary less across steps, such as
+    the diagonal of the whitened matrix, which is tiny against its norm, are dominated by
+    the FP32 rounding of that matrix and must not be magnified into noise of unit size),
+    He-normal weights, zero biases."""
     feats = np.asarray(feats, dtype=np.float64)
     rng = np.random.default_rng(seed)
     mu = feats.mean(0)
-    sd = feats.std(0)
-    sd = np.where(sd > 1e-6 * max(1.0, np.abs(mu).max()), sd, 1.0)
+    sd = np.maximum(feats.std(0), 1e-4)
     w1 = rng.standard_normal((N_FEATURES, HIDDEN)) * np.sqrt(2.0 / N_FEATURES)
     w2 = rng.standard_normal((HIDDEN, HIDDEN)) * np.sqrt(2.0 / HIDDEN)
     w3 = rng.standard_normal(HIDDEN) * np.sqrt(1.0 / HIDDEN)
@@ -86,8 +88,9 @@ def gradient(model, feats, targets, ctx: Optional[Context] = None):
 
 def train(model, feats, targets, iterations: int = 2000, lr: float = 1e-3, weight_decay: float = 0.0,
           val_feats=None, val_targets=None, eval_every: int = 100, ctx: Optional[Context] = None):
-    """(trained model, loss history, validation history): full-batch Adam on the GPU; with
-    a validation set the model of lowest validation loss is returned."""
+    """(trained model, loss history, validation history): full-batch Adam on the GPU with
+    the L2 penalty (weight_decay / 2) |W|^2 of the weights; with a validation set the
+    model of lowest validation loss is returned."""
     ctx = ctx or default_context()
     model = np.array(model, dtype=np.float32, copy=True)
     feats = np.ascontiguousarray(feats, dtype=np.float32)
@@ -148,7 +151,7 @@ def c4_steps(obs, steps, chunk: int = 512):
 
 
 def study(ctx, obs, n_train: int = 2000, n_eval: int = 2000, threshold: float = 0.0, iterations: int = 3000,
-          lr: float = 1e-3, margin: int = 16, seed: int = 0, chunk: int = 512, weight_decay: float = 1e-4):
+          lr: float = 1e-3, margin: int = 16, seed: int = 0, chunk: int = 512, weight_decay: float = 1e-3):
     """The rank-predictor study on the workload of `obs` (config_c4): train on the first
     n_train steps (features and labels from the full solve; the last fifth of them
     validates, and the model of lowest validation loss is kept), then solve the next n_eval

@@ -150,7 +150,8 @@ BIPP_B200_EXPORT BippError bipp_rank_mlp_forward(bipp_ctx_t ctx, const float* mo
 BIPP_B200_EXPORT BippError bipp_rank_mlp_gradient(bipp_ctx_t ctx, const float* model, const float* features,
                                                   const float* targets, size_t n, float* grad, float* loss);
 /* Train the model in place on the device: `iterations` full-batch Adam steps (beta 0.9,
- * 0.999, eps 1e-8, decoupled weight decay) on the loss above; lossHistory [iterations]
+ * 0.999, eps 1e-8) on the loss above plus the L2 penalty (weightDecay / 2) |W|^2 of the
+ * weights (not the biases); lossHistory [iterations]
  * (optional) gets the loss before each step. With a validation set (nVal > 0) its loss is
  * computed every evalEvery iterations (valHistory, optional, gets them) and the model
  * with the lowest validation loss is returned (early stopping). The mean and sd stay as
