@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--vv-precision", default="tf32x3", choices=["tf32x3", "bf16x3", "fp32", "fp64"],
                     help="arithmetic of the virtual-visibility products of the batched form")
     ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default launch shapes instead of tuning them on the batch first")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--stages", action="store_true", help="report per-stage device times")
@@ -509,6 +511,11 @@ def main():
     def one_step():
         pl.process_device(T, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())
 
+    # launch shapes tuned on this batch before the warm-up (the tuned values stay in the
+    # process's tuning table for the timed region)
+    tuning = None
+    if args.autotune and args.mode == "batched":
+        tuning = pl.autotune(T, S.data_ptr(), xyz.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
     for _ in range(args.warmup):
         one_step()
     pl.reset()
@@ -656,6 +663,7 @@ def main():
                            "l2": f"inputs ({S_bytes / 1e9:.1f} GB/batch) larger than L2; no flush"},
                 "clocks": clk.summary(), "gpu_launches": gpu_launches, "stages_ms": stages, "e2e": e2e,
                 "cpu_baseline": cpu, "roofline": roof, "plain_gpu": plain,
+                "tuning": tuning,
                 "image_rel_l2": parity and parity["image_rel_l2"],
                 "eig_rel_err": parity and {
                     "per_eigenvalue_above_1e-2_of_max": parity["eig_rel_err_max_above_1e-2"],

@@ -12,6 +12,8 @@
 #include "context.hpp"
 #include "nufft.hpp"
 #include "tune.hpp"
+
+#include <cub/device/device_radix_sort.cuh>
 #include "spread_tc.cuh"
 
 namespace bippb200 {
@@ -310,7 +312,7 @@ static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStrea
 template <int CH>
 static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, const int* offs, const PtRec* rec,
                              const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
-                             int slabPlanes, float2* out, int* errFlag) {
+                             int slabPlanes, float2* out, int* errFlag, int* workCounter) {
   using S = TcShape<CH>;
   int dev = 0, sms = 148;
   B2_CUDA(cudaGetDevice(&dev));
@@ -319,7 +321,7 @@ static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, co
   const int grid = std::max(1, std::min(nItems, sms * std::min(S::MinBlocks, tuned("spread.ctas_per_sm"))));
   count_launch();
   spread_tc_kernel<CH><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0,
-                                                           slabPlanes, out, errFlag);
+                                                           slabPlanes, out, errFlag, workCounter);
 }
 
 // BIPP_B200_SPREAD=warp selects the shared-memory-atomic spreader for every channel count
@@ -410,6 +412,32 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   item_fill_kernel<<<tb, 256, 0, ctx_->stream>>>(ntiles, load_.get<int>(), parts_.get<int>(), itemOff_.get<int>(),
                                                  items_.get<SpreadItem>());
   B2_CHECK_LAUNCH();
+  // load-ordered dynamic schedule (tunable): the items of every slab sorted heaviest
+  // first, handed out by a work counter per slab launch
+  const bool dynamic = tc && tuned("spread.schedule") == 1 && nItemsAll > 0;
+  if (dynamic) {
+    const int tilesPerSlab = slabTiles * g_.ntx * g_.nty;
+    itemKeys_.ensure(ctx_, 2 * (size_t)nItemsAll * sizeof(unsigned));
+    itemsAlt_.ensure(ctx_, (size_t)nItemsAll * sizeof(SpreadItem));
+    count_launch();
+    item_key_kernel<<<std::min(8192, (nItemsAll + 255) / 256), 256, 0, ctx_->stream>>>(
+        nItemsAll, items_.get<SpreadItem>(), tilesPerSlab, itemKeys_.get<unsigned>());
+    B2_CHECK_LAUNCH();
+    int endBit = 20;
+    while ((1 << (endBit - 20)) <= nslab && endBit < 32) ++endBit;
+    size_t tmpBytes = 0;
+    B2_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, itemKeys_.get<unsigned>(),
+                                            itemKeys_.get<unsigned>() + nItemsAll, items_.get<SpreadItem>(),
+                                            itemsAlt_.get<SpreadItem>(), nItemsAll, 0, endBit, ctx_->stream));
+    sortTmp_.ensure(ctx_, std::max<size_t>(tmpBytes, 16));
+    B2_CUDA(cub::DeviceRadixSort::SortPairs(sortTmp_.get(), tmpBytes, itemKeys_.get<unsigned>(),
+                                            itemKeys_.get<unsigned>() + nItemsAll, items_.get<SpreadItem>(),
+                                            itemsAlt_.get<SpreadItem>(), nItemsAll, 0, endBit, ctx_->stream));
+    B2_CUDA(cudaMemcpyAsync(items_.get(), itemsAlt_.get(), (size_t)nItemsAll * sizeof(SpreadItem),
+                            cudaMemcpyDeviceToDevice, ctx_->stream));
+    workCounters_.ensure(ctx_, (size_t)std::max(1, nslab) * sizeof(int));
+    B2_CUDA(cudaMemsetAsync(workCounters_.get(), 0, (size_t)std::max(1, nslab) * sizeof(int), ctx_->stream));
+  }
   {
     int total = 0, split = 0;
     d2h(ctx_, &total, offsets_.get<int>() + nkeys_, sizeof(int));
@@ -445,7 +473,8 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     if (nItems > 0 && tc) {
       auto launch = nch_ <= 4 ? launch_spread_tc<4> : launch_spread_tc<8>;
       launch(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(), valStride_, nch_,
-             items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes, grid_.get<float2>(), errFlag_.get<int>());
+             items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes, grid_.get<float2>(), errFlag_.get<int>(),
+             dynamic ? workCounters_.get<int>() + sl : nullptr);
       B2_CHECK_LAUNCH();
     } else if (nItems > 0) {
       const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];

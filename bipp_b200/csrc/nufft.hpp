@@ -77,6 +77,7 @@ private:
   double su_ = 1, sv_ = 1;
   long long nkeys_ = 0, valStride_ = 0;
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
+  DevBuf itemKeys_, itemsAlt_, sortTmp_, workCounters_;
   DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, splitCount_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
   // per slab size: the pass along y over every (channel, plane, x) column and the pass
   // along x over the two blocks of rows the pixels read

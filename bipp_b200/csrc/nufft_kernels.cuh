@@ -468,6 +468,20 @@ static __global__ void tile_parts_kernel(int ntiles, const int* __restrict__ loa
   }
 }
 
+// sort keys of the spreading work items for the load-ordered schedule: slab index in the
+// high bits (items of a slab stay one contiguous range), then the item's points in
+// descending order (heaviest first)
+static __global__ void item_key_kernel(int nItems, const SpreadItem* __restrict__ items, int tilesPerSlab,
+                                       unsigned* __restrict__ keys) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nItems; i += gridDim.x * blockDim.x) {
+    const SpreadItem it = items[i];
+    const long long lo = (long long)it.load * it.part / it.nparts, hi = (long long)it.load * (it.part + 1) / it.nparts;
+    const long long pts = hi - lo;
+    const unsigned n = (unsigned)(pts < 0xFFFFF ? pts : 0xFFFFF);
+    keys[i] = ((unsigned)(it.tile / tilesPerSlab) << 20) | (0xFFFFFu - n);
+  }
+}
+
 // tiles to clear, compacted in tile order (offsets from an exclusive scan of the flags)
 static __global__ void clear_list_kernel(int ntiles, const int* __restrict__ clearFlag, const int* __restrict__ off,
                                          int* __restrict__ list) {

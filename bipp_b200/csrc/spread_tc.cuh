@@ -78,18 +78,20 @@ __device__ __forceinline__ int tc_range_pair(int j) {
   return -1;
 }
 
-// Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ...
+// Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ... or, with
+// a work counter, the next item of the (load-ordered) list whenever it is free
 template <int CH>
 static __global__ void __launch_bounds__(kTcThreads, TcShape<CH>::MinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
-                 int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag) {
+                 int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag,
+                 int* __restrict__ workCounter) {
   using S = TcShape<CH>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmemSlot;
   __shared__ int rBeg[27], rPre[28];
-  __shared__ int sOk;
+  __shared__ int sOk, sItem;
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t sbase = smem_u32(sm);
   const uint32_t bar = smem_u32(&mbar);
@@ -120,7 +122,14 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   const int myPair = (lane < 27) ? tc_range_pair(lane) : -1;
   uint32_t parity = 0;
   bool pending = false;                       // a commit not yet waited for
-  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
+  for (int item = blockIdx.x;; item += gridDim.x) {
+    if (workCounter) {
+      // every thread has read the previous sItem (the item ends with a barrier)
+      if (tid == 0) sItem = atomicAdd(workCounter, 1);
+      __syncthreads();
+      item = sItem;
+    }
+    if (item >= nItems) break;
     const SpreadItem it = items[item];
     const int tx = it.tile % g.ntx, ty = (it.tile / g.ntx) % g.nty, tw = it.tile / (g.ntx * g.nty);
     const int x0 = tx * kTX, y0 = ty * kTY, w0 = tw * kTW;
