@@ -38,30 +38,35 @@ __device__ __forceinline__ int tab_sw(int row, int v) {
 }
 static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mapping assumes 16 x 8 x 8 tiles, 16 visits");
 
-// Shape of the kernel for CH channels (4 or 8): accumulator 128 x N, N = 8 planes x CH
-// channels x re/im; one K-step of B is N rows x 8 tf32; CTAs per SM bounded by TMEM.
-template <int CH>
+// Shape of the kernel for CH channels (4 or 8) and STAGES operand stages (1, or 2 so that
+// a phase's operands are built while the previous phase's MMAs run): accumulator 128 x N,
+// N = 8 planes x CH channels x re/im; one K-step of B is N rows x 8 tf32; CTAs per SM
+// bounded by TMEM (512 columns) and shared memory.
+template <int CH, int STAGES = 1>
 struct TcShape {
   static constexpr int N = kTW * 2 * CH;
   static constexpr int Cols = N;                  // tensor-memory columns per CTA
-  static constexpr int MinBlocks = 512 / Cols;    // CTAs per SM (all 512 TMEM columns)
   static constexpr int BStep = N * 8 * 4;
-  static constexpr int OffAhi = 0;
+  static constexpr int OffAhi = 0;                // operands of stage 0; stage s at + s StageBytes
   static constexpr int OffAlo = OffAhi + kTcSteps * kTcAStep;
   static constexpr int OffBhi = OffAlo + kTcSteps * kTcAStep;
   static constexpr int OffBlo = OffBhi + kTcSteps * BStep;
-  static constexpr int OffEx = OffBlo + kTcSteps * BStep;  // float [16 x][kTcVS]
+  static constexpr int StageBytes = OffBlo + kTcSteps * BStep;
+  static constexpr int OffEx = STAGES * StageBytes;        // float [16 x][kTcVS]
   static constexpr int OffEy = OffEx + kTX * kTcVS * 4;    // float [8 y][kTcVS]
   static constexpr int OffEw = OffEy + kTY * kTcVS * 4;    // float [8 w][kTcVS]
   static constexpr int OffVal = OffEw + kTW * kTcVS * 4;   // float [2 CH (channel, re/im)][kTcVS]
   static constexpr int Smem = OffVal + 2 * CH * kTcVS * 4;
+  static constexpr int BySmem = 233472 / (Smem + 512 + 1024);
+  static constexpr int MinBlocks = (512 / Cols) < BySmem ? (512 / Cols) : BySmem;   // CTAs per SM
   // instruction descriptor: D f32, A/B tf32, both K-major, N, M = 128
   static constexpr uint32_t Idesc =
       (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
   static_assert(CH == 4 || CH == 8, "4 or 8 channels");
   static_assert(N % 16 == 0 && N <= 256, "MMA N for M = 128");
   static_assert(OffEx % 1024 == 0, "operand blocks 1 KB aligned");
-  static_assert(MinBlocks * (Smem + 512 + 1024) <= 233472,
+  static_assert(STAGES == 1 || STAGES == 2, "one or two operand stages");
+  static_assert(MinBlocks >= 1 && MinBlocks * (Smem + 512 + 1024) <= 233472,
                 "shared memory (dynamic + static <= 512 B + 1 KB reserved) for MinBlocks CTAs per SM");
 };
 
@@ -80,27 +85,26 @@ __device__ __forceinline__ int tc_range_pair(int j) {
 
 // Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ... or, with
 // a work counter, the next item of the (load-ordered) list whenever it is free
-template <int CH>
-static __global__ void __launch_bounds__(kTcThreads, TcShape<CH>::MinBlocks)
+template <int CH, int STAGES>
+static __global__ void __launch_bounds__(kTcThreads, TcShape<CH, STAGES>::MinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                  int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag,
                  int* __restrict__ workCounter) {
-  using S = TcShape<CH>;
+  using S = TcShape<CH, STAGES>;
   extern __shared__ __align__(128) unsigned char sm[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[STAGES];   // MMA completion of the phases of each stage
   __shared__ uint32_t tmemSlot;
   __shared__ int rBeg[27], rPre[28];
   __shared__ int sOk, sItem;
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t sbase = smem_u32(sm);
-  const uint32_t bar = smem_u32(&mbar);
   float* ex = reinterpret_cast<float*>(sm + S::OffEx);
   float* ey = reinterpret_cast<float*>(sm + S::OffEy);
   float* ew = reinterpret_cast<float*>(sm + S::OffEw);
   float* val = reinterpret_cast<float*>(sm + S::OffVal);
   if (tid == 0) {
-    mbar_init(bar, 1);
+    for (int st = 0; st < STAGES; ++st) mbar_init(smem_u32(&mbar[st]), 1);
     sOk = 1;
   }
   __syncwarp();
@@ -120,8 +124,23 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   const int xm = tid % kTX, ym = tid / kTX;   // cell of accumulator row tid
   const int lane = tid & 31;
   const int myPair = (lane < 27) ? tc_range_pair(lane) : -1;
-  uint32_t parity = 0;
-  bool pending = false;                       // a commit not yet waited for
+  // thread 0's view of each stage's barrier: its phase parity and whether a commit of
+  // that stage has not been waited for
+  uint32_t parity[STAGES];
+  bool pending[STAGES];
+#pragma unroll
+  for (int st = 0; st < STAGES; ++st) {
+    parity[st] = 0;
+    pending[st] = false;
+  }
+  // bounded wait (thread 0) for stage st's last commit; false on timeout
+  auto wait_stage = [&](int st) {
+    if (!pending[st]) return true;
+    if (!mbar_wait(smem_u32(&mbar[st]), parity[st])) return false;
+    parity[st] ^= 1u;
+    pending[st] = false;
+    return true;
+  };
   for (int item = blockIdx.x;; item += gridDim.x) {
     if (workCounter) {
       // every thread has read the previous sItem (the item ends with a barrier)
@@ -202,6 +221,9 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     for (int v0 = 0; v0 < nvis; v0 += kTcVisits) {
       const int nk = min(kTcVisits, nvis - v0);
       const int steps = (nk + 7) >> 3;
+      // operand stage of this phase
+      const int stg = STAGES == 1 ? 0 : (v0 / kTcVisits) & 1;
+      const uint32_t sstage = sbase + (uint32_t)(stg * S::StageBytes);
       // per-visit tables from the prefetched point data (the tensor cores read only the
       // operand blocks, so the tables are rebuilt while the previous phase's MMAs run)
       {
@@ -245,15 +267,9 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
             for (int c = 2 * CPR * (pa - 6); c < 2 * CPR * (pa - 5); ++c) val[tab_sw(c, pv)] = 0.f;
         }
       }
-      // the operands of the previous phase must have been consumed before they are rewritten
-      if (tid == 0 && pending) {
-        if (mbar_wait(bar, parity)) {
-          parity ^= 1u;
-          pending = false;
-        } else {
-          sOk = 0;
-        }
-      }
+      // the operands of this stage's previous phase must have been consumed before they
+      // are rewritten (with two stages, the MMAs of the phase before run meanwhile)
+      if (tid == 0 && !wait_stage(stg)) sOk = 0;
       __syncthreads();
       if (!sOk) break;
       if (v0 + kTcVisits < nvis) fetch(v0 + kTcVisits);
@@ -278,8 +294,8 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
             l[2 * t] = lo2.x; l[2 * t + 1] = lo2.y;
           }
         }
-        const uint32_t ah = sbase + S::OffAhi + s * kTcAStep + tid * 16;
-        const uint32_t al = sbase + S::OffAlo + s * kTcAStep + tid * 16;
+        const uint32_t ah = sstage + S::OffAhi + s * kTcAStep + tid * 16;
+        const uint32_t al = sstage + S::OffAlo + s * kTcAStep + tid * 16;
         st_shared_v4(ah, h[0], h[1], h[2], h[3]);
         st_shared_v4(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
         st_shared_v4(al, l[0], l[1], l[2], l[3]);
@@ -308,8 +324,8 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
               h[0] = h0.x; h[1] = h0.y; h[2] = h1.x; h[3] = h1.y;
               l[0] = l0.x; l[1] = l0.y; l[2] = l1.x; l[3] = l1.y;
             }
-            const uint32_t bh = sbase + S::OffBhi + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
-            const uint32_t bl = sbase + S::OffBlo + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
+            const uint32_t bh = sstage + S::OffBhi + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
+            const uint32_t bl = sstage + S::OffBlo + s * S::BStep + (k0 >> 2) * (S::BStep / 2) + n * 16;
             st_shared_v4(bh, h[0], h[1], h[2], h[3]);
             st_shared_v4(bl, l[0], l[1], l[2], l[3]);
           }
@@ -321,26 +337,23 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       if (tid == 0) {
         tc_fence_after();
         for (int s = 0; s < steps; ++s) {
-          const uint64_t dAh = tc_desc(sbase + S::OffAhi + s * kTcAStep, kTcAStep / 2, 128);
-          const uint64_t dAl = tc_desc(sbase + S::OffAlo + s * kTcAStep, kTcAStep / 2, 128);
-          const uint64_t dBh = tc_desc(sbase + S::OffBhi + s * S::BStep, S::BStep / 2, 128);
-          const uint64_t dBl = tc_desc(sbase + S::OffBlo + s * S::BStep, S::BStep / 2, 128);
+          const uint64_t dAh = tc_desc(sstage + S::OffAhi + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dAl = tc_desc(sstage + S::OffAlo + s * kTcAStep, kTcAStep / 2, 128);
+          const uint64_t dBh = tc_desc(sstage + S::OffBhi + s * S::BStep, S::BStep / 2, 128);
+          const uint64_t dBl = tc_desc(sstage + S::OffBlo + s * S::BStep, S::BStep / 2, 128);
           tc_mma(tmem, dAh, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
           tc_mma(tmem, dAh, dBl, S::Idesc, 1u);
           tc_mma(tmem, dAl, dBh, S::Idesc, 1u);
         }
-        tc_commit(bar);
-        pending = true;
+        tc_commit(smem_u32(&mbar[stg]));
+        pending[stg] = true;
       }
     }
-    // accumulator complete
-    if (tid == 0 && pending) {
-      if (mbar_wait(bar, parity)) {
-        parity ^= 1u;
-        pending = false;
-      } else {
-        sOk = 0;
-      }
+    // accumulator complete (every stage's last commit waited for)
+    if (tid == 0) {
+#pragma unroll
+      for (int st = 0; st < STAGES; ++st)
+        if (sOk && !wait_stage(st)) sOk = 0;
     }
     tc_fence_before();
     __syncthreads();
@@ -378,7 +391,9 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   }
   // after a timeout: wait once more (bounded) for MMAs still in flight, then release
   if (tid == 0) {
-    if (pending) mbar_wait(bar, parity);
+#pragma unroll
+    for (int st = 0; st < STAGES; ++st)
+      if (pending[st]) mbar_wait(smem_u32(&mbar[st]), parity[st]);
     if (!sOk) atomicOr(errFlag, 1);
   }
   tc_fence_before();

@@ -44,6 +44,8 @@ std::vector<Param>& table() {
       {"spread.items_cap", 4096, {2048, 4096, 8192}, "points per spreading work item (heavier tiles are split)", 0},
       {"spread.ctas_per_sm", 8, {2, 4, 8}, "resident tensor-core spreading CTAs per SM (at most 512 / TMEM columns)",
        0},
+      {"spread.stages", 1, {1, 2},
+       "operand stages of the tensor-core spreader (2: a phase is built while the previous one's MMAs run)", 0},
       {"spread.schedule", 0, {0, 1},
        "spreading work items: 0 round-robin over the persistent CTAs, 1 heaviest first from a work counter", 0},
       {"hetrd.threads", 0, {0, 256, 512, 1024}, "threads per matrix in the tridiagonalisation (0: by matrix size)", 0},

@@ -38,7 +38,8 @@ def test_autotune_pipeline(ctx):
     rep = pl.autotune(64, S.data_ptr(), x.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
     print(rep)
     desc = bipp.tuning_describe()
-    for name in ("spread.items_cap", "spread.ctas_per_sm", "spread.schedule", "hetrd.threads", "vv.ctas_per_sm"):
+    for name in ("spread.items_cap", "spread.stages", "spread.ctas_per_sm", "spread.schedule", "hetrd.threads",
+                 "vv.ctas_per_sm"):
         assert rep[name]["chosen"] == desc[name]["value"]
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
     assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
