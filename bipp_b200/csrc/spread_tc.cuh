@@ -126,19 +126,14 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   const int myPair = (lane < 27) ? tc_range_pair(lane) : -1;
   // thread 0's view of each stage's barrier: its phase parity and whether a commit of
   // that stage has not been waited for
-  uint32_t parity[STAGES];
-  bool pending[STAGES];
-#pragma unroll
-  for (int st = 0; st < STAGES; ++st) {
-    parity[st] = 0;
-    pending[st] = false;
-  }
+  // (bit st of each word), kept in registers
+  uint32_t parityBits = 0, pendingBits = 0;
   // bounded wait (thread 0) for stage st's last commit; false on timeout
   auto wait_stage = [&](int st) {
-    if (!pending[st]) return true;
-    if (!mbar_wait(smem_u32(&mbar[st]), parity[st])) return false;
-    parity[st] ^= 1u;
-    pending[st] = false;
+    if (!((pendingBits >> st) & 1u)) return true;
+    if (!mbar_wait(smem_u32(&mbar[st]), (parityBits >> st) & 1u)) return false;
+    parityBits ^= 1u << st;
+    pendingBits &= ~(1u << st);
     return true;
   };
   for (int item = blockIdx.x;; item += gridDim.x) {
@@ -346,7 +341,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
           tc_mma(tmem, dAl, dBh, S::Idesc, 1u);
         }
         tc_commit(smem_u32(&mbar[stg]));
-        pending[stg] = true;
+        pendingBits |= 1u << stg;
       }
     }
     // accumulator complete (every stage's last commit waited for)
@@ -393,7 +388,7 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
   if (tid == 0) {
 #pragma unroll
     for (int st = 0; st < STAGES; ++st)
-      if (pending[st]) mbar_wait(smem_u32(&mbar[st]), parity[st]);
+      if ((pendingBits >> st) & 1u) mbar_wait(smem_u32(&mbar[st]), (parityBits >> st) & 1u);
     if (!sOk) atomicOr(errFlag, 1);
   }
   tc_fence_before();
