@@ -50,3 +50,50 @@ def test_autotune_pipeline(ctx):
         assert np.linalg.norm(tuned[lv] - base[lv]) <= 1e-5 * np.linalg.norm(base[lv]), lv
     pl.close()
     bipp.tuning_reset()
+
+
+def test_spreader_variants_agree(ctx):
+    """The tunable spreader variants (one or two operand stages, round-robin or
+    heaviest-first dynamic schedule, work-item caps) give the same images to 1e-6
+    relative L2 per level on a batch that splits heavy tiles."""
+    import torch
+
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+    from bipp_b200.parameter_estimator import infer_intervals
+
+    bipp.tuning_reset()
+    cfg = sim.config_c2(n_antenna=256, n_steps=96, image_size=256, n_src=100, keep=(200, 256))
+    obs = sim.observation(cfg)
+    dev = torch.device("cuda", 0)
+    s, x = sim.visibilities(obs, list(range(96)), device=dev, dtype=torch.complex64, masks=sim.keep_masks(cfg))
+    S = s.transpose(1, 2).contiguous()
+    wl = torch.full((96,), cfg.wl, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    _, d, _, _ = bipp.eigh_gram_batched(np.full(8, cfg.wl, np.float32), s[:8].cpu().numpy(), x[:8].cpu().numpy(),
+                                        ctx=ctx)
+    intervals = infer_intervals(cfg.n_levels, 1.0, "log", 0.0, np.inf, d)
+    n = cfg.image_size
+    l = obs.lmn[:, 0].reshape(n, n)
+    m = obs.lmn[:, 1].reshape(n, n)
+    lat = (n, n, l[0, 0], m[0, 0], l[1, 0] - l[0, 0], l[0, 1] - l[0, 0], m[1, 0] - m[0, 0], m[0, 1] - m[0, 0])
+    pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, lat, obs.lmn[:, 2], obs.basis, tolerance=cfg.eps,
+                       chunk_steps=96, max_steps=96)
+
+    def run():
+        pl.reset()
+        pl.process_device(96, S.data_ptr(), x.data_ptr(), wl.data_ptr())
+        return pl.images().astype(np.float64), pl.nufft_stats()
+
+    base, st = run()
+    assert st["split_tiles"] > 0 or bipp.tuning_get("spread.items_cap") > 2048
+    for settings in ({"spread.stages": 2}, {"spread.schedule": 1}, {"spread.stages": 2, "spread.schedule": 1},
+                     {"spread.items_cap": 2048, "spread.stages": 2}):
+        bipp.tuning_reset()
+        for k, v in settings.items():
+            bipp.tuning_set(k, v)
+        got, _ = run()
+        for lv in range(got.shape[0]):
+            assert np.linalg.norm(got[lv] - base[lv]) <= 1e-6 * np.linalg.norm(base[lv]), (settings, lv)
+    bipp.tuning_reset()
+    pl.close()
