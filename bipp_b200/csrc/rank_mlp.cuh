@@ -44,41 +44,53 @@ inline size_t rank_features_smem(int nmax) {
 }
 
 // Y = C X for the n x P block X (row-major [n][P] complex in shared memory), C Hermitian
-// with its lower triangle at Ab (ld Nmax); Y zeroed by the caller. Column j of the lower
-// triangle gives y_i += C_ij x_j (i > j, shared-memory atomics) and y_j += sum_i
-// conj(C_ij) x_i (a warp reduction).
+// with its lower triangle at Ab (ld Nmax), in two passes without atomics: a warp per
+// column j writes y_j = sum_{i >= j} conj(C_ij) x_i (the column below the diagonal, read
+// coalesced and reduced across the warp), then a thread per row i adds
+// sum_{j < i} C_ij x_j (the row left of the diagonal; the rows of a warp are consecutive,
+// so every column read is coalesced).
 template <typename C, int P>
 __device__ void herm_block_mv(const C* __restrict__ Ab, int Nmax, int n, const float2* X, float2* Y) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int j = warp; j < n; j += nwarp) {
-    float2 xj[P], acc[P];
+    float2 acc[P];
 #pragma unroll
-    for (int p = 0; p < P; ++p) {
-      xj[p] = X[j * P + p];
-      acc[p] = make_float2(0.f, 0.f);
-    }
+    for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
     for (int i = j + lane; i < n; i += 32) {
       const C v = Ab[i + (long long)j * Nmax];
       const float cr = (float)v.x, ci = (i == j) ? 0.f : (float)v.y;
 #pragma unroll
       for (int p = 0; p < P; ++p) {
         const float2 xi = X[i * P + p];
-        // conj(C_ij) x_i
         acc[p].x += cr * xi.x + ci * xi.y;
         acc[p].y += cr * xi.y - ci * xi.x;
-        if (i != j) {
-          atomicAdd(&Y[i * P + p].x, cr * xj[p].x - ci * xj[p].y);
-          atomicAdd(&Y[i * P + p].y, cr * xj[p].y + ci * xj[p].x);
-        }
       }
     }
 #pragma unroll
     for (int p = 0; p < P; ++p) {
       const float ax = warp_sum(acc[p].x), ay = warp_sum(acc[p].y);
-      if (lane == 0) {
-        atomicAdd(&Y[j * P + p].x, ax);
-        atomicAdd(&Y[j * P + p].y, ay);
+      if (lane == 0) Y[j * P + p] = make_float2(ax, ay);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    float2 acc[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
+    for (int j = 0; j < i; ++j) {
+      const C v = Ab[i + (long long)j * Nmax];
+      const float cr = (float)v.x, ci = (float)v.y;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const float2 xj = X[j * P + p];
+        acc[p].x += cr * xj.x - ci * xj.y;
+        acc[p].y += cr * xj.y + ci * xj.x;
       }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      Y[i * P + p].x += acc[p].x;
+      Y[i * P + p].y += acc[p].y;
     }
   }
 }
@@ -90,7 +102,7 @@ __device__ void herm_block_mv(const C* __restrict__ Ab, int Nmax, int n, const f
 //   threshold; 36 sum |C_ii|; 37 sum C_ii^2; 38 largest squared row norm; 39 sum of
 //   row norms^4; 40 fraction of rows with squared norm above f^2 / n; 41 sum of C_ii above
 //   the threshold; 42-45 C_ii at the ranks n/8, n/4, n/2, 3n/4 (descending);
-//   46-63 spectral moments t_k = trace C^k, k = 2..6, estimated with P Rademacher probes
+//   46-63 spectral moments t_k = trace C^k, k = 1..6, estimated with P Rademacher probes
 //   z (t_k ~ mean z^H C^k z, from Y1 = C Z, Y2 = C Y1, Y3 = C Y2): t3, t4, t5, t6, the
 //   effective ranks f^4 / t4 and (f^6 / t6)^(1/2) (both / n), t4^2 / (t6 f^2),
 //   t3^2 / (t4 f^2), t5 / (t4 f), their logarithms / log(n), t1 t3 / f^4,
@@ -119,22 +131,28 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
     return;
   }
   const C* Ab = A + (long long)b * Nmax * Nmax;
-  for (int i = tid; i < n; i += blockDim.x) {
-    dg[i] = (float)Ab[i + (long long)i * Nmax].x;
-    r2[i] = 0.f;
-  }
+  for (int i = tid; i < n; i += blockDim.x) dg[i] = (float)Ab[i + (long long)i * Nmax].x;
   __syncthreads();
-  // C_ij (i > j) is in row i and, as conj(C_ij) = C_ji, in row j
+  // squared row norms: row j holds its column below the diagonal (conj(C_ij) = C_ji), read
+  // by a warp and reduced, and row i holds the entries left of its diagonal, read by a
+  // thread per row (consecutive rows, coalesced)
   for (int j = warp; j < n; j += nwarp) {
     float col = 0.f;
     for (int i = j + lane; i < n; i += 32) {
       const C v = Ab[i + (long long)j * Nmax];
-      const float m = (float)v.x * (float)v.x + (float)v.y * (float)v.y;
-      col += m;
-      if (i != j) atomicAdd(&r2[i], m);
+      col += (float)v.x * (float)v.x + (float)v.y * (float)v.y;
     }
     col = warp_sum(col);
-    if (lane == 0) atomicAdd(&r2[j], col);
+    if (lane == 0) r2[j] = col;
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += blockDim.x) {
+    float row = 0.f;
+    for (int j = 0; j < i; ++j) {
+      const C v = Ab[i + (long long)j * Nmax];
+      row += (float)v.x * (float)v.x + (float)v.y * (float)v.y;
+    }
+    r2[i] += row;
   }
   __syncthreads();
   double sFro = 0, sTr = 0, sAbs = 0, sSq = 0, sR4 = 0, sAbove = 0;
@@ -193,10 +211,7 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
   // spectral moments by probes: Ya = C Z, Yb = C Ya, then Ya = C Yb
   double t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;
   if constexpr (P > 0) {
-    for (int e = tid; e < n * P; e += blockDim.x) {
-      Yb[e] = make_float2(probe_sign(e / P, e % P), 0.f);   // Z in Yb
-      Ya[e] = make_float2(0.f, 0.f);
-    }
+    for (int e = tid; e < n * P; e += blockDim.x) Yb[e] = make_float2(probe_sign(e / P, e % P), 0.f);   // Z
     __syncthreads();
     herm_block_mv<C, P>(Ab, Nmax, n, Yb, Ya);
     __syncthreads();
@@ -210,8 +225,6 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
     __syncthreads();
     t2 = block_sum(a2, red) / P;
     __syncthreads();
-    for (int e = tid; e < n * P; e += blockDim.x) Yb[e] = make_float2(0.f, 0.f);
-    __syncthreads();
     herm_block_mv<C, P>(Ab, Nmax, n, Ya, Yb);
     __syncthreads();
     double a3 = 0, a4 = 0;
@@ -223,8 +236,6 @@ rank_features_kernel(const C* __restrict__ A, int Nmax, const int* __restrict__ 
     t3 = block_sum(a3, red) / P;
     __syncthreads();
     t4 = block_sum(a4, red) / P;
-    __syncthreads();
-    for (int e = tid; e < n * P; e += blockDim.x) Ya[e] = make_float2(0.f, 0.f);
     __syncthreads();
     herm_block_mv<C, P>(Ab, Nmax, n, Yb, Ya);
     __syncthreads();
