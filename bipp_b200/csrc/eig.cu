@@ -332,10 +332,14 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     }
     smem_optin(k, smem);
     count_launch();
-    // threads per matrix: by size, unless the tuning table fixes them
+    // threads per matrix: by size, unless the tuning table fixes them; the blocked kernel
+    // may run as fewer persistent CTAs (a percentage of the SM count)
     const int tt = tuned("hetrd.threads");
-    k<<<nb, tt > 0 ? tt : trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(),
-                                                        w.e.template get<double>(), w.tau.template get<C>(), sizeOrder);
+    const int pct = blocked ? tuned("hetrd.ctas_pct") : 0;
+    const int grid = pct > 0 ? std::max(1, std::min(nb, pct * ctx->smCount / 100)) : nb;
+    k<<<grid, tt > 0 ? tt : trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(),
+                                                          w.e.template get<double>(), w.tau.template get<C>(),
+                                                          sizeOrder, nb);
     B2_CHECK_LAUNCH();
   }
   // 4. tridiagonal eigenpairs (FP64); workspace aliases W64 (free after trinv)

@@ -1013,7 +1013,8 @@ static __global__ void order_by_size_kernel(const int* __restrict__ nred, int nb
 template <typename C, typename R>
 __global__ void __launch_bounds__(kTrdThreads)
 hetrd_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
-             double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr) {
+             double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr,
+             int /* nBatch: one CTA per matrix here */ = 0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int b = order ? order[blockIdx.x] : blockIdx.x;
   hetd2_tail<C, R>(A + (long long)b * Nmax * Nmax, nred[b], Nmax, 0, dOut + (long long)b * Nmax,
@@ -1095,12 +1096,31 @@ __device__ __forceinline__ void trd_her2k(float2* __restrict__ Ab, int Nmax, int
 }
 
 template <typename C, typename R>
+__device__ __forceinline__ void hetrd_blk_matrix(C* __restrict__ A, const int* __restrict__ nred, int Nmax,
+                                                 double* __restrict__ dOut, double* __restrict__ eOut,
+                                                 C* __restrict__ tauOut, int b, unsigned char* smem_raw);
+
+// One CTA per matrix, or (nBatch > gridDim.x) persistent CTAs that take matrices
+// blockIdx.x, blockIdx.x + gridDim.x, ... of the size order: fewer matrices in flight keep
+// their trailing triangles (the per-column mat-vec passes re-read them) in L2.
+template <typename C, typename R>
 __global__ void __launch_bounds__(kTrdThreads)
 hetrd_blk_kernel(C* __restrict__ A, const int* __restrict__ nred, int Nmax, double* __restrict__ dOut,
-                 double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr) {
+                 double* __restrict__ eOut, C* __restrict__ tauOut, const int* __restrict__ order = nullptr,
+                 int nBatch = 0) {
   static_assert(sizeof(C) == 8, "single precision");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int b = order ? order[blockIdx.x] : blockIdx.x;
+  const int nb = nBatch > 0 ? nBatch : (int)gridDim.x;
+  for (int w = blockIdx.x; w < nb; w += gridDim.x) {
+    hetrd_blk_matrix<C, R>(A, nred, Nmax, dOut, eOut, tauOut, order ? order[w] : w, smem_raw);
+    __syncthreads();
+  }
+}
+
+template <typename C, typename R>
+__device__ __forceinline__ void hetrd_blk_matrix(C* __restrict__ A, const int* __restrict__ nred, int Nmax,
+                                                 double* __restrict__ dOut, double* __restrict__ eOut,
+                                                 C* __restrict__ tauOut, int b, unsigned char* smem_raw) {
   const int n = nred[b];
   C* Ab = A + (long long)b * Nmax * Nmax;
   double* d = dOut + (long long)b * Nmax;

@@ -39,7 +39,7 @@ def test_autotune_pipeline(ctx):
     print(rep)
     desc = bipp.tuning_describe()
     for name in ("spread.items_cap", "spread.stages", "spread.ctas_per_sm", "spread.schedule", "hetrd.threads",
-                 "vv.ctas_per_sm"):
+                 "hetrd.ctas_pct", "vv.ctas_per_sm"):
         assert rep[name]["chosen"] == desc[name]["value"]
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
     assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
@@ -97,3 +97,34 @@ def test_spreader_variants_agree(ctx):
             assert np.linalg.norm(got[lv] - base[lv]) <= 1e-6 * np.linalg.norm(base[lv]), (settings, lv)
     bipp.tuning_reset()
     pl.close()
+
+
+def test_persistent_tridiagonalisation_agrees(ctx):
+    """The tridiagonalisation run as persistent CTAs (fewer than the matrices, each taking
+    matrices in the size order) gives the eigenvalues and V diag(d) V^H of the default of
+    one CTA per matrix, to 1e-6 relative, on 40 steps of uneven size (100-160 of 160
+    antennas kept, so that the blocked panels run)."""
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    bipp.tuning_reset()
+    cfg = sim.config_c2(n_antenna=160, n_steps=40, image_size=64, n_src=20, keep=(100, 160))
+    obs = sim.observation(cfg)
+    s, x = sim.visibilities(obs, list(range(40)), masks=sim.keep_masks(cfg))
+    s, x = s.numpy().astype(np.complex64), x.numpy().astype(np.float32)
+    wl = np.full(40, cfg.wl, np.float32)
+    v0, d0, n0, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
+    try:
+        for pct in (50, 150):
+            bipp.tuning_set("hetrd.ctas_pct", pct)
+            v1, d1, n1, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
+            assert np.array_equal(n0, n1)
+            for b in range(40):
+                sc = np.abs(d0[b]).max()
+                assert np.abs(d1[b] - d0[b]).max() <= 1e-6 * sc, (pct, b)
+                k = int(n0[b])
+                a0 = (v0[b][:, :k] * d0[b][:k]) @ v0[b][:, :k].conj().T
+                a1 = (v1[b][:, :k] * d1[b][:k]) @ v1[b][:, :k].conj().T
+                assert np.linalg.norm(a1 - a0) <= 1e-6 * np.linalg.norm(a0), (pct, b)
+    finally:
+        bipp.tuning_reset()
