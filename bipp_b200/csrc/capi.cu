@@ -181,6 +181,15 @@ static void partition_host(bipp_ctx_s* ctx, const size_t* dims, size_t n, const 
 
 using namespace bippb200;
 
+namespace bippb200 {
+void ctx_release(bipp_ctx_s* c) {
+  if (c->refs.fetch_sub(1) != 1) return;
+  cudaStreamSynchronize(c->stream);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+}  // namespace bippb200
+
 extern "C" {
 
 const char* bipp_last_error(void) { return g_lastError; }
@@ -226,9 +235,7 @@ BippError bipp_ctx_create(BippProcessingUnit pu, bipp_ctx_t* out) {
 BippError bipp_ctx_destroy(bipp_ctx_t ctx) {
   return guard([&] {
     if (!ctx) return;
-    cudaStreamSynchronize(ctx->stream);
-    cudaStreamDestroy(ctx->stream);
-    delete ctx;
+    ctx_release(ctx);
   });
 }
 

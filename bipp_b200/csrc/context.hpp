@@ -5,6 +5,8 @@
 // synchronous on return.
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -22,11 +24,20 @@ struct bipp_ctx_s {
   cudaDeviceProp prop{};
   int smCount = 0;
   size_t maxSmemOptin = 0;
+  // references: the caller's (dropped by bipp_ctx_destroy) and one per live pipeline or
+  // NUFFT collector created on it, so that the context outlives them whatever the order
+  // of the destroy calls
+  std::atomic<int> refs{1};
 };
 
 namespace bippb200 {
 
 void set_last_error(const std::string& msg);
+
+// a pipeline or collector keeps its context alive
+inline void ctx_retain(bipp_ctx_s* c) { c->refs.fetch_add(1); }
+// drop a reference; the last one synchronises and frees the context
+void ctx_release(bipp_ctx_s* c);
 
 // RAII device buffer on the context's stream-ordered pool.
 class DevBuf {

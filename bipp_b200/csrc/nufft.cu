@@ -743,6 +743,7 @@ BippError bipp_nufft_create(bipp_ctx_t ctx, const bipp_nufft_options* opt, size_
     p->images.alloc(ctx, nImages * nPixel * sizeof(float));
     p->images.zero();
     sync(ctx);
+    ctx_retain(ctx);
     *plan = p.release();
   });
 }
@@ -818,6 +819,7 @@ BippError bipp_nufft_destroy(bipp_nufft_t plan) {
     bipp_ctx_s* ctx = plan->ctx;
     delete plan;
     sync(ctx);
+    ctx_release(ctx);
   });
 }
 

@@ -512,6 +512,7 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
     p->images.zero();
     if (cfg->maxSteps) pipeline_alloc(p.get(), cfg->maxSteps);
     sync(ctx);
+    ctx_retain(ctx);
     *out = p.release();
   });
 }
@@ -749,6 +750,7 @@ BippError bipp_pipeline_destroy(bipp_pipeline_t pl) {
     bipp_ctx_s* ctx = pl->ctx;
     delete pl;
     sync(ctx);
+    ctx_release(ctx);
   });
 }
 

@@ -53,6 +53,8 @@ BIPP_B200_EXPORT BippError bipp_ctx_create(BippProcessingUnit pu, bipp_ctx_t* ct
 /* As bipp_ctx_create on an explicit device (the reference picks rank % deviceCount,
  * src/context_internal.cpp:59-66). */
 BIPP_B200_EXPORT BippError bipp_ctx_create_on_device(BippProcessingUnit pu, int device, bipp_ctx_t* ctx);
+/* Drops the caller's reference: pipelines and NUFFT collectors created on the context
+ * keep it alive until they are destroyed, so the destroy calls may come in any order. */
 BIPP_B200_EXPORT BippError bipp_ctx_destroy(bipp_ctx_t ctx);
 /* Processing unit actually used (always BIPP_PU_GPU). Context::processing_unit(),
  * include/bipp/context.hpp:60. */

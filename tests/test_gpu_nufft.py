@@ -129,6 +129,30 @@ def test_nufft_collect_get_four_images_warp_spreader(ctx):
     plan.close()
 
 
+def test_context_destroyed_before_its_collector():
+    """A context destroyed before the NUFFT collector created on it stays alive until the
+    collector is destroyed: the collector still adds, returns its image (that of a
+    collector on a live context, to 1e-6) and is destroyed without error."""
+    import bipp_b200 as bipp
+    from bipp_b200 import simulate as sim
+
+    rng = np.random.default_rng(8)
+    lmn = sim.make_lmn_grid(32, math.radians(10.0)).astype(np.float32)
+    uvw, c = _synthetic_points(rng, 300, 3000.0, 200.0)
+    uvw, c = uvw.astype(np.float32), c.astype(np.complex64)
+    imgs = []
+    for early in (False, True):
+        own = bipp.Context("GPU")
+        plan = bipp.NufftSynthesis(own, bipp.NufftSynthesisOptions().set_tolerance(1e-5), lmn, 2, 300)
+        if early:
+            own.close()
+        plan.add(uvw, c)
+        imgs.append(plan.get_image(0))
+        plan.close()
+        own.close()
+    assert _rel_l2(imgs[1], imgs[0]) <= 1e-6
+
+
 def test_nufft_collect_get_non_lattice(ctx):
     """Pixels that are not on a lattice use the direct FP64 evaluation."""
     import bipp_b200 as bipp

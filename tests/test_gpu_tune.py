@@ -54,8 +54,10 @@ def test_autotune_pipeline(ctx):
 
 def test_spreader_variants_agree(ctx):
     """The tunable spreader variants (one or two operand stages, round-robin or
-    heaviest-first dynamic schedule, work-item caps) give the same images to 1e-6
-    relative L2 per level on a batch that splits heavy tiles."""
+    heaviest-first dynamic schedule, work-item caps) give the same images to 1e-5
+    relative L2 per level on a batch that splits heavy tiles (the cap changes which tiles
+    are split, so the FP32 sums of their parts are added in another order: differences of
+    ~2e-6 were measured)."""
     import torch
 
     import bipp_b200 as bipp
@@ -94,7 +96,7 @@ def test_spreader_variants_agree(ctx):
             bipp.tuning_set(k, v)
         got, _ = run()
         for lv in range(got.shape[0]):
-            assert np.linalg.norm(got[lv] - base[lv]) <= 1e-6 * np.linalg.norm(base[lv]), (settings, lv)
+            assert np.linalg.norm(got[lv] - base[lv]) <= 1e-5 * np.linalg.norm(base[lv]), (settings, lv)
     bipp.tuning_reset()
     pl.close()
 
