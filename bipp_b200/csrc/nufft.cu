@@ -134,46 +134,22 @@ Lattice fit_lattice(const std::vector<double>& l, const std::vector<double>& m) 
 // NufftCore
 // ---------------------------------------------------------------------------------------
 NufftCore::~NufftCore() {
-  for (auto& kv : plans_) {
-    cufftDestroy(kv.second.y);
-    cufftDestroy(kv.second.x0);
-    cufftDestroy(kv.second.x1);
-  }
+  for (auto& kv : plans_) cufftDestroy(kv.second);
 }
 
-// rows of the FFT output that the w-sum reads: y in [0, Na - Na/2) and [ny - Na/2, ny)
-// (pixel row a reads y = (a - Na/2) mod ny)
-const NufftCore::FftPlans& NufftCore::plan_for(int slabPlanes) {
-  auto it = plans_.find(slabPlanes);
-  if (it != plans_.end()) return it->second;
-  FftPlans f;
-  const long long cp = (long long)nch_ * slabPlanes;   // (channel, plane) rows per y
-  int ny = g_.ny, nx = g_.nx;
-  // along y: element k of column b = (channel, plane, x) at b + k * cp * nx
-  int emb = 0;
-  B2_CUFFT(cufftPlanMany(&f.y, 1, &ny, &emb, (int)(cp * nx), 1, &emb, (int)(cp * nx), 1, CUFFT_C2C, (int)(cp * nx)));
-  // along x: contiguous rows; rows y of one block x (channel, plane) are contiguous
-  const int r0 = g_.Na - g_.Na / 2, r1 = g_.Na / 2;
-  B2_CUFFT(cufftPlanMany(&f.x0, 1, &nx, nullptr, 1, nx, nullptr, 1, nx, CUFFT_C2C, (int)(r0 * cp)));
-  B2_CUFFT(cufftPlanMany(&f.x1, 1, &nx, nullptr, 1, nx, nullptr, 1, nx, CUFFT_C2C, (int)(std::max(1, r1) * cp)));
-  B2_CUFFT(cufftSetStream(f.y, ctx_->stream));
-  B2_CUFFT(cufftSetStream(f.x0, ctx_->stream));
-  B2_CUFFT(cufftSetStream(f.x1, ctx_->stream));
-  return plans_[slabPlanes] = f;
-}
-
-// inverse 2-D FFT of every (channel, plane) of the slab, pruned to the output rows the
-// w-sum reads: the pass along y over all columns, the pass along x over those rows only
+// batched inverse 2-D FFT of every (channel, plane) array of the slab
 void NufftCore::inverse_fft(int slabPlanes, float2* slab) {
-  const FftPlans& f = plan_for(slabPlanes);
-  const long long cp = (long long)nch_ * slabPlanes;
-  auto c = [](float2* p) { return reinterpret_cast<cufftComplex*>(p); };
-  B2_CUFFT(cufftExecC2C(f.y, c(slab), c(slab), CUFFT_INVERSE));
-  B2_CUFFT(cufftExecC2C(f.x0, c(slab), c(slab), CUFFT_INVERSE));
-  if (g_.Na / 2 > 0) {
-    float2* blk = slab + (long long)(g_.ny - g_.Na / 2) * cp * g_.nx;
-    B2_CUFFT(cufftExecC2C(f.x1, c(blk), c(blk), CUFFT_INVERSE));
+  const int batch = nch_ * slabPlanes;
+  auto it = plans_.find(batch);
+  if (it == plans_.end()) {
+    cufftHandle h;
+    int n[2] = {g_.ny, g_.nx};
+    B2_CUFFT(cufftPlanMany(&h, 2, n, nullptr, 1, g_.nx * g_.ny, nullptr, 1, g_.nx * g_.ny, CUFFT_C2C, batch));
+    B2_CUFFT(cufftSetStream(h, ctx_->stream));
+    it = plans_.emplace(batch, h).first;
   }
+  B2_CUFFT(cufftExecC2C(it->second, reinterpret_cast<cufftComplex*>(slab), reinterpret_cast<cufftComplex*>(slab),
+                        CUFFT_INVERSE));
 }
 
 void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<double>& n, double eps, int nch,

@@ -79,14 +79,9 @@ private:
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
   DevBuf itemKeys_, itemsAlt_, sortTmp_, workCounters_;
   DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, splitCount_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
-  // per slab size: the pass along y over every (channel, plane, x) column and the pass
-  // along x over the two blocks of rows the pixels read
-  struct FftPlans {
-    cufftHandle y = 0, x0 = 0, x1 = 0;
-  };
-  std::map<int, FftPlans> plans_;
+  // batched 2-D cuFFT plans by batch size (channels x slab planes)
+  std::map<int, cufftHandle> plans_;
   int slabTiles_ = 1;
-  const FftPlans& plan_for(int slabPlanes);
   void inverse_fft(int slabPlanes, float2* slab);
   void exclusive_scan(const int* in, int* out, long long n);
 

@@ -42,15 +42,20 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// suspend-time hint of one try (ns): a waiting thread is suspended until the phase
+// completes or this time passes, instead of spinning and taking issue slots from the
+// other warps of the SM
+constexpr uint32_t kTcWaitHintNs = 1000;
+
 // bounded wait (at most `spins` tries) for the completion of phase `parity` of the barrier
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int spins = kTcSpin) {
   for (int i = 0; i < spins; ++i) {
     uint32_t done;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(done)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "n"(kTcWaitHintNs)
         : "memory");
     if (done) return true;
   }
