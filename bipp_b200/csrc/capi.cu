@@ -182,6 +182,42 @@ static void partition_host(bipp_ctx_s* ctx, const size_t* dims, size_t n, const 
 using namespace bippb200;
 
 namespace bippb200 {
+// Pinned host slots for staged copies, each with an event recorded after the last copy
+// that reads it
+class PinnedSlots {
+public:
+  PinnedSlots(int n, size_t bytes) : bufs_(n, nullptr), events_(n, nullptr), recorded_(n, false) {
+    for (int i = 0; i < n; ++i) {
+      B2_CUDA(cudaMallocHost(&bufs_[i], bytes));
+      B2_CUDA(cudaEventCreateWithFlags(&events_[i], cudaEventDisableTiming));
+    }
+  }
+  PinnedSlots(const PinnedSlots&) = delete;
+  PinnedSlots& operator=(const PinnedSlots&) = delete;
+  ~PinnedSlots() {
+    for (size_t i = 0; i < bufs_.size(); ++i) {
+      if (events_[i]) {
+        cudaEventSynchronize(events_[i]);
+        cudaEventDestroy(events_[i]);
+      }
+      if (bufs_[i]) cudaFreeHost(bufs_[i]);
+    }
+  }
+  void* get(int i) const { return bufs_[i]; }
+  void record(int i, cudaStream_t st) {
+    B2_CUDA(cudaEventRecord(events_[i], st));
+    recorded_[i] = true;
+  }
+  void wait(int i) {
+    if (recorded_[i]) B2_CUDA(cudaEventSynchronize(events_[i]));
+  }
+
+private:
+  std::vector<void*> bufs_;
+  std::vector<cudaEvent_t> events_;
+  std::vector<bool> recorded_;
+};
+
 void ctx_release(bipp_ctx_s* c) {
   if (c->refs.fetch_sub(1) != 1) return;
   cudaStreamSynchronize(c->stream);
@@ -300,12 +336,14 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
         require(sampleIds[im * nSamples + order[im][k]] == sampleIds[order[0][k]],
                 "Selection must contain the same sample ids for all images.");
     const size_t nB = nAnt * nAnt;
-    std::vector<std::complex<float>> v(nAnt * nBeam);
-    std::vector<float> uvw(nB * 3);
-    // eigenvectors, per-image column scales and the GEMM's sizes on the device; the virtual
-    // visibilities are written straight into the collectors' staging buffers
-    DevBuf dV(ctx, v.size() * sizeof(float2)), dK(ctx, nImages * nBeam * sizeof(float)),
-        dn(ctx, 3 * 4 * sizeof(int));
+    // Samples are read into two pinned host slots; sample k + 1 is read (dataset callbacks)
+    // while the copies and kernels of sample k run, and a slot is rewritten only after the
+    // copies that read it have completed (its event). Eigenvectors and column scales go to
+    // two device slots as well; the uvw go straight into the collectors' staging buffers.
+    PinnedSlots host(2, nAnt * nBeam * sizeof(float2) + nB * 3 * sizeof(float) + nImages * nBeam * sizeof(float));
+    DevBuf dV[2] = {DevBuf(ctx, nAnt * nBeam * sizeof(float2)), DevBuf(ctx, nAnt * nBeam * sizeof(float2))};
+    DevBuf dK[2] = {DevBuf(ctx, nImages * nBeam * sizeof(float)), DevBuf(ctx, nImages * nBeam * sizeof(float))};
+    DevBuf dn(ctx, 3 * 4 * sizeof(int));
     std::vector<int> hn(12);
     for (int i = 0; i < 4; ++i) {
       hn[i] = (int)nAnt;          // matrix size of every image of a group
@@ -332,36 +370,41 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
     } cleanup{plans};
     // 2 pi rounded to float, as the reference's T(2 * pi) with T = float
     const float twoPi = static_cast<float>(2.0 * 3.14159265358979323846);
-    std::vector<float> ks(nImages * nBeam);
     for (size_t k = 0; k < nSamples; ++k) {
+      const int slot = (int)(k & 1);
+      host.wait(slot);   // the copies of sample k - 2 out of this slot are done
+      auto* v = reinterpret_cast<std::complex<float>*>(host.get(slot));
+      float* uvw = reinterpret_cast<float*>(v + nAnt * nBeam);
+      float* ks = uvw + nB * 3;
       const size_t id = sampleIds[order[0][k]];
       const float wl = ds->wl(ds->user, id);
       const float scale = ds->scale(ds->user, id);
-      ds->uvw(ds->user, id, uvw.data(), nB);
-      ds->eig_vec(ds->user, id, v.data(), nAnt);
+      ds->uvw(ds->user, id, uvw, nB);
+      ds->eig_vec(ds->user, id, v, nAnt);
       // uvw scaled in single precision as the reference's float path
       const float uvwScale = twoPi / wl;   // float division (src/nufft_synthesis.cpp:150-154)
-      for (auto& x : uvw) x *= uvwScale;
+      for (size_t i = 0; i < nB * 3; ++i) uvw[i] *= uvwScale;
       for (size_t im = 0; im < nImages; ++im) {
         const float* d = eigvals[im * nSamples + order[im][k]];
         for (size_t c = 0; c < nBeam; ++c) ks[im * nBeam + c] = scale * d[c];
       }
-      h2d(ctx, dV.get(), v.data(), v.size() * sizeof(float2));
-      h2d(ctx, dK.get(), ks.data(), ks.size() * sizeof(float));
+      h2d(ctx, dV[slot].get(), v, nAnt * nBeam * sizeof(float2));
+      h2d(ctx, dK[slot].get(), ks, nImages * nBeam * sizeof(float));
       for (size_t g0 = 0, gi = 0; g0 < nImages; g0 += 4, ++gi) {
         bipp_nufft_t pl = plans[gi];
         const long long ld = nufft_stage_ld(pl);
         float* su = nufft_stage_uvw(pl);
-        for (int c = 0; c < 3; ++c) h2d(ctx, su + c * ld, uvw.data() + c * nB, nB * sizeof(float));
+        for (int c = 0; c < 3; ++c) h2d(ctx, su + c * ld, uvw + c * nB, nB * sizeof(float));
+        if (g0 + 4 >= nImages) host.record(slot, ctx->stream);   // last reader of the slot
         // VV of the group's images in one launch: "matrix" b = image g0 + b, the same
         // eigenvectors, its own column scales, output into the image's staging slot
         const int nIm = (int)std::min<size_t>(4, nImages - g0);
         GemmArgs<float2> g{};
-        g.A = dV.get<float2>(); g.strideA = 0; g.lda = (int)nAnt; g.opA = 0;
-        g.B = dV.get<float2>(); g.strideB = 0; g.ldb = (int)nAnt; g.opB = 1;
+        g.A = dV[slot].get<float2>(); g.strideA = 0; g.lda = (int)nAnt; g.opA = 0;
+        g.B = dV[slot].get<float2>(); g.strideB = 0; g.ldb = (int)nAnt; g.opB = 1;
         g.Cm = nufft_stage_values(pl, 0); g.strideC = ld; g.ldc = (int)nAnt;
         g.n = dn.get<int>(); g.outMode = 0; g.levels = 1;
-        g.kscale = dK.get<float>() + g0 * nBeam; g.strideK = (long long)nBeam;
+        g.kscale = dK[slot].get<float>() + g0 * nBeam; g.strideK = (long long)nBeam;
         g.kbeg = dn.get<int>() + 4; g.kend = dn.get<int>() + 8;
         const int tiles = ((int)nAnt + kGemmBM - 1) / kGemmBM;
         count_launch();
@@ -369,9 +412,8 @@ BippError bipp_image_synthesis(bipp_ctx_t ctx, const bipp_nufft_options* opt, co
         B2_CHECK_LAUNCH();
         nufft_commit(pl);
       }
-      // the host staging arrays are rewritten for the next sample
-      sync(ctx);
     }
+    sync(ctx);
     for (size_t im = 0; im < nImages; ++im) {
       const BippError e = bipp_nufft_get_image(plans[im / 4], im % 4, images + im * nPixel);
       if (e != BIPP_SUCCESS) throw Error(e, bipp_last_error());
