@@ -515,7 +515,7 @@ def main():
     # process's tuning table for the timed region)
     tuning = None
     if args.autotune and args.mode == "batched":
-        tuning = pl.autotune(T, S.data_ptr(), xyz.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
+        tuning = pl.autotune(T, S.data_ptr(), xyz.data_ptr(), wl.data_ptr(), on_device=True, repeats=2)
     for _ in range(args.warmup):
         one_step()
     pl.reset()

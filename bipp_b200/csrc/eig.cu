@@ -337,10 +337,7 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     const int tt = tuned("hetrd.threads");
     const int pct = blocked ? tuned("hetrd.ctas_pct") : 0;
     const int grid = pct > 0 ? std::max(1, std::min(nb, pct * ctx->smCount / 100)) : nb;
-    // (the blocked kernel above 256 rows: 1024 threads, one matrix per SM, so that fewer
-    // trailing triangles compete for L2; measured faster than two 512-thread CTAs per SM)
-    const int defThreads = (blocked && Nmax > 256) ? 1024 : trd_threads(Nmax);
-    k<<<grid, tt > 0 ? tt : defThreads, smem, st>>>(A, nred, Nmax, w.d.template get<double>(),
+    k<<<grid, tt > 0 ? tt : trd_threads(Nmax), smem, st>>>(A, nred, Nmax, w.d.template get<double>(),
                                                           w.e.template get<double>(), w.tau.template get<C>(),
                                                           sizeOrder, nb);
     B2_CHECK_LAUNCH();
