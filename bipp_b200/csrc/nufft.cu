@@ -285,19 +285,21 @@ static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStrea
 
 // tensor-core spreading (4 or 8 channels): persistent CTAs, as many per SM as tensor
 // memory allows
-template <int CH, int STAGES>
+template <int CH, int STAGES, bool AT>
 static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, const int* offs, const PtRec* rec,
                              const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
                              int slabPlanes, float2* out, int* errFlag, int* workCounter) {
-  using S = TcShape<CH, STAGES>;
+  using S = TcShape<CH, STAGES, AT>;
   int dev = 0, sms = 148;
   B2_CUDA(cudaGetDevice(&dev));
   B2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  smem_optin(spread_tc_kernel<CH, STAGES>, S::Smem);
+  smem_optin(spread_tc_kernel<CH, STAGES, AT>, S::Smem);
+  // never more CTAs per SM than tensor memory holds (a CTA beyond that would wait in its
+  // allocation until another one exits)
   const int grid = std::max(1, std::min(nItems, sms * std::min(S::MinBlocks, tuned("spread.ctas_per_sm"))));
   count_launch();
-  spread_tc_kernel<CH, STAGES><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems, tw0,
-                                                           slabPlanes, out, errFlag, workCounter);
+  spread_tc_kernel<CH, STAGES, AT><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems,
+                                                                     tw0, slabPlanes, out, errFlag, workCounter);
 }
 
 // BIPP_B200_SPREAD=warp selects the shared-memory-atomic spreader for every channel count
@@ -448,8 +450,11 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
     if (nItems > 0 && tc) {
       const bool two = tuned("spread.stages") == 2;
-      auto launch = nch_ <= 4 ? (two ? launch_spread_tc<4, 2> : launch_spread_tc<4, 1>)
-                              : (two ? launch_spread_tc<8, 2> : launch_spread_tc<8, 1>);
+      const bool at = tuned("spread.a_tmem") == 1;
+      auto launch = nch_ <= 4 ? (at ? (two ? launch_spread_tc<4, 2, true> : launch_spread_tc<4, 1, true>)
+                                    : (two ? launch_spread_tc<4, 2, false> : launch_spread_tc<4, 1, false>))
+                              : (at ? (two ? launch_spread_tc<8, 2, true> : launch_spread_tc<8, 1, true>)
+                                    : (two ? launch_spread_tc<8, 2, false> : launch_spread_tc<8, 1, false>));
       launch(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(), valStride_, nch_,
              items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes, grid_.get<float2>(), errFlag_.get<int>(),
              dynamic ? workCounters_.get<int>() + sl : nullptr);

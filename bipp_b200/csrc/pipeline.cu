@@ -623,7 +623,7 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     B2_CUDA(cudaEventCreate(&e0));
     B2_CUDA(cudaEventCreate(&e1));
     std::string rep = "{";
-    const char* params[] = {"spread.items_cap", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
+    const char* params[] = {"spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                             "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"};
     auto body = [&] {
       pipeline_process(pl, nSteps, s, xyz, wl, onDevice);   // warm-up (allocations, first-use costs)

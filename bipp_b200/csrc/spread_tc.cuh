@@ -38,18 +38,24 @@ __device__ __forceinline__ int tab_sw(int row, int v) {
 }
 static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mapping assumes 16 x 8 x 8 tiles, 16 visits");
 
-// Shape of the kernel for CH channels (4 or 8) and STAGES operand stages (1, or 2 so that
-// a phase's operands are built while the previous phase's MMAs run): accumulator 128 x N,
-// N = 8 planes x CH channels x re/im; one K-step of B is N rows x 8 tf32; CTAs per SM
-// bounded by TMEM (512 columns) and shared memory.
-template <int CH, int STAGES = 1>
+// Shape of the kernel for CH channels (4 or 8), STAGES operand stages (1, or 2 so that a
+// phase's operands are built while the previous phase's MMAs run) and the place of the A
+// operand (AT: tensor memory, written by each thread into its own lane with tcgen05.st;
+// otherwise shared memory): accumulator 128 x N, N = 8 planes x CH channels x re/im; one
+// K-step of B is N rows x 8 tf32; CTAs per SM bounded by TMEM (512 columns) and shared
+// memory. With A in tensor memory the tensor cores read only B from shared memory, and
+// the threads store only B there: about half of the shared-memory traffic of a phase.
+constexpr int tc_pow2_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
+template <int CH, int STAGES = 1, bool AT = false>
 struct TcShape {
   static constexpr int N = kTW * 2 * CH;
-  static constexpr int Cols = N;                  // tensor-memory columns per CTA
+  static constexpr int AStageCols = AT ? 2 * kTcSteps * 8 : 0;   // A_hi, A_lo of a phase (K = 16 each)
+  static constexpr int AColBase = N;                             // A of stage s at AColBase + s AStageCols
+  static constexpr int Cols = tc_pow2_cols(N + STAGES * AStageCols);   // tensor-memory columns per CTA
   static constexpr int BStep = N * 8 * 4;
   static constexpr int OffAhi = 0;                // operands of stage 0; stage s at + s StageBytes
-  static constexpr int OffAlo = OffAhi + kTcSteps * kTcAStep;
-  static constexpr int OffBhi = OffAlo + kTcSteps * kTcAStep;
+  static constexpr int OffAlo = OffAhi + (AT ? 0 : kTcSteps * kTcAStep);
+  static constexpr int OffBhi = OffAlo + (AT ? 0 : kTcSteps * kTcAStep);
   static constexpr int OffBlo = OffBhi + kTcSteps * BStep;
   static constexpr int StageBytes = OffBlo + kTcSteps * BStep;
   static constexpr int OffEx = STAGES * StageBytes;        // float [16 x][kTcVS]
@@ -85,13 +91,13 @@ __device__ __forceinline__ int tc_range_pair(int j) {
 
 // Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ... or, with
 // a work counter, the next item of the (load-ordered) list whenever it is free
-template <int CH, int STAGES>
-static __global__ void __launch_bounds__(kTcThreads, TcShape<CH, STAGES>::MinBlocks)
+template <int CH, int STAGES, bool AT = false>
+static __global__ void __launch_bounds__(kTcThreads, TcShape<CH, STAGES, AT>::MinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                  int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag,
                  int* __restrict__ workCounter) {
-  using S = TcShape<CH, STAGES>;
+  using S = TcShape<CH, STAGES, AT>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar[STAGES];   // MMA completion of the phases of each stage
   __shared__ uint32_t tmemSlot;
@@ -265,7 +271,9 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       // the operands of this stage's previous phase must have been consumed before they
       // are rewritten (with two stages, the MMAs of the phase before run meanwhile)
       if (tid == 0 && !wait_stage(stg)) sOk = 0;
+      if constexpr (AT) tc_fence_before();
       __syncthreads();
+      if constexpr (AT) tc_fence_after();   // the stage's tensor memory is free to rewrite
       if (!sOk) break;
       if (v0 + kTcVisits < nvis) fetch(v0 + kTcVisits);
       // A: row tid (cell xm, ym), 8 visits per K-step
@@ -289,12 +297,19 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
             l[2 * t] = lo2.x; l[2 * t + 1] = lo2.y;
           }
         }
-        const uint32_t ah = sstage + S::OffAhi + s * kTcAStep + tid * 16;
-        const uint32_t al = sstage + S::OffAlo + s * kTcAStep + tid * 16;
-        st_shared_v4(ah, h[0], h[1], h[2], h[3]);
-        st_shared_v4(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
-        st_shared_v4(al, l[0], l[1], l[2], l[3]);
-        st_shared_v4(al + kTcAStep / 2, l[4], l[5], l[6], l[7]);
+        if constexpr (AT) {
+          // K-step s of A_hi at column +8 s, of A_lo at +16 + 8 s (row tid = lane tid)
+          const uint32_t ta = tmemWarp + (uint32_t)(S::AColBase + stg * S::AStageCols + 8 * s);
+          tmem_st8(ta, h);
+          tmem_st8(ta + 16, l);
+        } else {
+          const uint32_t ah = sstage + S::OffAhi + s * kTcAStep + tid * 16;
+          const uint32_t al = sstage + S::OffAlo + s * kTcAStep + tid * 16;
+          st_shared_v4(ah, h[0], h[1], h[2], h[3]);
+          st_shared_v4(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
+          st_shared_v4(al, l[0], l[1], l[2], l[3]);
+          st_shared_v4(al + kTcAStep / 2, l[4], l[5], l[6], l[7]);
+        }
       }
       // B: row n = plane * 2 CH + channel * 2 + (re|im); TPR threads per row, each with
       // VPT visits of the K-step
@@ -328,17 +343,28 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       }
       // make the operand writes visible to the tensor core, then one thread issues
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if constexpr (AT) {
+        tmem_st_wait();
+        tc_fence_before();
+      }
       __syncthreads();
       if (tid == 0) {
         tc_fence_after();
         for (int s = 0; s < steps; ++s) {
-          const uint64_t dAh = tc_desc(sstage + S::OffAhi + s * kTcAStep, kTcAStep / 2, 128);
-          const uint64_t dAl = tc_desc(sstage + S::OffAlo + s * kTcAStep, kTcAStep / 2, 128);
           const uint64_t dBh = tc_desc(sstage + S::OffBhi + s * S::BStep, S::BStep / 2, 128);
           const uint64_t dBl = tc_desc(sstage + S::OffBlo + s * S::BStep, S::BStep / 2, 128);
-          tc_mma(tmem, dAh, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
-          tc_mma(tmem, dAh, dBl, S::Idesc, 1u);
-          tc_mma(tmem, dAl, dBh, S::Idesc, 1u);
+          if constexpr (AT) {
+            const uint32_t aHi = tmem + (uint32_t)(S::AColBase + stg * S::AStageCols + 8 * s);
+            tc_mma_ta(tmem, aHi, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
+            tc_mma_ta(tmem, aHi, dBl, S::Idesc, 1u);
+            tc_mma_ta(tmem, aHi + 16, dBh, S::Idesc, 1u);
+          } else {
+            const uint64_t dAh = tc_desc(sstage + S::OffAhi + s * kTcAStep, kTcAStep / 2, 128);
+            const uint64_t dAl = tc_desc(sstage + S::OffAlo + s * kTcAStep, kTcAStep / 2, 128);
+            tc_mma(tmem, dAh, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
+            tc_mma(tmem, dAh, dBl, S::Idesc, 1u);
+            tc_mma(tmem, dAl, dBh, S::Idesc, 1u);
+          }
         }
         tc_commit(smem_u32(&mbar[stg]));
         pendingBits |= 1u << stg;
