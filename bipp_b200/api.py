@@ -749,8 +749,8 @@ class Pipeline:
     def autotune(self, n_steps, s_ptr, xyz_ptr, wl_ptr, on_device=True, repeats=1):
         """Time the candidate launch parameters on these steps (pointers as
         process_device / process_host_ptr), keep the fastest in the process-wide tuning
-        table, and return the per-candidate times (ms per call) with the choices. The
-        images are left as they were."""
+        table, and return the per-candidate times (device ms of the stage each parameter
+        changes) with the choices. The images are left as they were."""
         import json
 
         buf = C.create_string_buffer(8192)

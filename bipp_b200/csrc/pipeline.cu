@@ -619,58 +619,62 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     std::copy(pl->eigMs, pl->eigMs + kEigTimers, eigt);
     const bool timing = pl->timing;
     pl->timing = false;
-    cudaEvent_t e0, e1;
-    B2_CUDA(cudaEventCreate(&e0));
-    B2_CUDA(cudaEventCreate(&e1));
     std::string rep = "{";
     const char* params[] = {"spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                             "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"};
+    // Objective of a parameter: the device time of the stage it changes (CUDA events of
+    // the pipeline's stage timers): spreading (with the tile clearing) for spread.*, the
+    // tridiagonalisation kernel for hetrd.*, the virtual visibilities for vv.*. Every
+    // candidate gets one untimed call; the timed calls then go over the candidates
+    // forwards and backwards in turn (a drift of the device's speed during the pass hits
+    // every candidate alike) and the fastest call of each candidate counts.
+    auto objective = [&](const char* name) {
+      if (!std::strncmp(name, "spread.", 7)) return pl->stageMs[3] + pl->stageMs[6];
+      if (!std::strncmp(name, "hetrd.", 6)) return pl->eigMs[4];
+      return pl->stageMs[1];
+    };
     auto body = [&] {
       pipeline_process(pl, nSteps, s, xyz, wl, onDevice);   // warm-up (allocations, first-use costs)
       bool first = true;
       for (const char* name : params) {
         if (!std::strcmp(name, "vv.ctas_per_sm") && (pl->vvPrecision == 2 || pl->vvPrecision == 3)) continue;
-        int best = tuned(name);
-        float bestMs = 0.f;
-        bool firstBest = true;
-        rep += std::string(first ? "" : ", ") + "\"" + name + "\": {";
-        first = false;
-        bool firstC = true;
-        for (const int c : tuning_candidates(name)) {
-          set_tuned(name, c);
-          // one untimed call first (buffers that the value resizes, first-use costs), then
-          // the fastest of the timed calls
+        const std::vector<int> cands = tuning_candidates(name);
+        std::vector<double> best(cands.size(), 0.0);
+        for (size_t i = 0; i < cands.size(); ++i) {
+          set_tuned(name, cands[i]);
           pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
-          float ms = 0.f;
-          for (int r = 0; r < repeats; ++r) {
-            B2_CUDA(cudaEventRecord(e0, ctx->stream));
+        }
+        pl->timing = true;
+        for (int r = 0; r < std::max(2, repeats); ++r) {
+          for (size_t j = 0; j < cands.size(); ++j) {
+            const size_t i = (r & 1) ? cands.size() - 1 - j : j;
+            set_tuned(name, cands[i]);
+            std::fill(pl->stageMs, pl->stageMs + 7, 0.0);
+            std::fill(pl->eigMs, pl->eigMs + kEigTimers, 0.0);
             pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
-            B2_CUDA(cudaEventRecord(e1, ctx->stream));
-            B2_CUDA(cudaEventSynchronize(e1));
-            float one = 0.f;
-            B2_CUDA(cudaEventElapsedTime(&one, e0, e1));
-            ms = (r == 0) ? one : std::min(ms, one);
-          }
-          char buf[64];
-          std::snprintf(buf, sizeof(buf), "%s\"%d\": %.3f", firstC ? "" : ", ", c, ms);
-          rep += buf;
-          firstC = false;
-          if (firstBest || ms < bestMs) {
-            bestMs = ms;
-            best = c;
-            firstBest = false;
+            const double t = objective(name);
+            best[i] = (r == 0) ? t : std::min(best[i], t);
           }
         }
-        set_tuned(name, best);
+        pl->timing = false;
+        size_t bi = 0;
+        for (size_t i = 1; i < cands.size(); ++i)
+          if (best[i] < best[bi]) bi = i;
+        set_tuned(name, cands[bi]);
+        rep += std::string(first ? "" : ", ") + "\"" + name + "\": {";
+        first = false;
+        for (size_t i = 0; i < cands.size(); ++i) {
+          char buf[64];
+          std::snprintf(buf, sizeof(buf), "%s\"%d\": %.3f", i ? ", " : "", cands[i], best[i]);
+          rep += buf;
+        }
         char buf[64];
-        std::snprintf(buf, sizeof(buf), ", \"chosen\": %d}", best);
+        std::snprintf(buf, sizeof(buf), ", \"chosen\": %d}", cands[bi]);
         rep += buf;
       }
     };
     // the caller's state comes back on every exit path
     auto restore = [&] {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
       cudaMemcpyAsync(pl->images.get(), saved.get(), imgBytes, cudaMemcpyDeviceToDevice, ctx->stream);
       pl->stepsDone = stepsDone;
       std::copy(stage, stage + 7, pl->stageMs);

@@ -376,13 +376,16 @@ BIPP_B200_EXPORT BippError bipp_selftest_wait_timeout(bipp_ctx_t ctx, int spins,
 
 /* Time the candidates of the tunable launch parameters on the caller's sample steps (the
  * arguments of bipp_pipeline_process) with the pipeline `pl`, one parameter at a time
- * (the pipeline's parameters of the tuning table below: spreading work items, stages,
- * CTAs per SM and schedule, threads and persistent CTAs of the tridiagonalisation,
- * virtual-visibility CTAs per SM): every candidate gets one untimed call, then the fastest
- * of `repeats` timed calls counts. The fastest candidate of each parameter is kept in the
- * process-wide tuning table and a JSON report of the per-call times (ms) is written into
- * report (reportLen bytes, truncated). The pipeline's images and step count are left as
- * they were. Results do not depend on the chosen values beyond rounding. */
+ * (the pipeline's parameters of the tuning table below: spreading work items, A-operand
+ * place, stages, CTAs per SM and schedule, threads and persistent CTAs of the
+ * tridiagonalisation, virtual-visibility CTAs per SM). The time of a candidate is the
+ * device time of the stage the parameter changes (spreading with tile clearing, the
+ * tridiagonalisation kernel, or the virtual visibilities): every candidate gets one
+ * untimed call, then max(2, repeats) passes over the candidates, forwards and backwards
+ * in turn, and the fastest call of each counts. The fastest candidate of each parameter
+ * is kept in the process-wide tuning table and a JSON report of those times (ms) is
+ * written into report (reportLen bytes, truncated). The pipeline's images and step count
+ * are left as they were. Results do not depend on the chosen values beyond rounding. */
 BIPP_B200_EXPORT BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz,
                                                   const double* wl, int onDevice, int repeats, char* report,
                                                   size_t reportLen);
