@@ -41,7 +41,7 @@ bool g_fileLoaded = false;
 
 std::vector<Param>& table() {
   static std::vector<Param> t = {
-      {"spread.items_cap", 4096, {2048, 4096, 8192}, "points per spreading work item (heavier tiles are split)", 0},
+      {"spread.items_cap", 2048, {2048, 4096, 8192}, "points per spreading work item (heavier tiles are split)", 0},
       {"spread.ctas_per_sm", 8, {2, 4, 8}, "resident tensor-core spreading CTAs per SM (at most 512 / TMEM columns)",
        0},
       {"spread.stages", 1, {1, 2},

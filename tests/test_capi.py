@@ -151,7 +151,7 @@ def test_tuning_table_without_a_gpu(tmp_path):
     import bipp_b200 as bipp
 
     bipp.tuning_reset()
-    assert bipp.tuning_get("spread.items_cap") == 4096 and bipp.tuning_get("hetrd.threads") == 0
+    assert bipp.tuning_get("spread.items_cap") == 2048 and bipp.tuning_get("hetrd.threads") == 0
     desc = bipp.tuning_describe()
     assert set(desc) == {"spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                          "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm", "direct.ctas_per_sm"}
@@ -165,7 +165,7 @@ def test_tuning_table_without_a_gpu(tmp_path):
     f = tmp_path / "tune.txt"
     bipp.tuning_save(str(f))
     bipp.tuning_reset()
-    assert bipp.tuning_get("spread.items_cap") == 4096
+    assert bipp.tuning_get("spread.items_cap") == 2048
     bipp.tuning_load(str(f))
     assert bipp.tuning_get("spread.items_cap") == 8192 and bipp.tuning_get("hetrd.threads") == 512
     bad = tmp_path / "bad.txt"
