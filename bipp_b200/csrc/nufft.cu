@@ -285,21 +285,21 @@ static void launch_spread(const NufftGeom& g, int nItems, size_t smem, cudaStrea
 
 // tensor-core spreading (4 or 8 channels): persistent CTAs, as many per SM as tensor
 // memory allows
-template <int CH, int STAGES, bool AT>
+template <int CH, int STAGES, bool AT, bool F16>
 static void launch_spread_tc(const NufftGeom& g, int nItems, cudaStream_t st, const int* offs, const PtRec* rec,
                              const float2* vals, long long vs, int nch, const SpreadItem* items, int tw0,
-                             int slabPlanes, float2* out, int* errFlag, int* workCounter) {
-  using S = TcShape<CH, STAGES, AT>;
+                             int slabPlanes, float2* out, int* errFlag, int* workCounter, const unsigned* valScale) {
+  using S = TcShape<CH, STAGES, AT, F16>;
   int dev = 0, sms = 148;
   B2_CUDA(cudaGetDevice(&dev));
   B2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  smem_optin(spread_tc_kernel<CH, STAGES, AT>, S::Smem);
+  smem_optin(spread_tc_kernel<CH, STAGES, AT, F16>, S::Smem);
   // never more CTAs per SM than tensor memory holds (a CTA beyond that would wait in its
   // allocation until another one exits)
   const int grid = std::max(1, std::min(nItems, sms * std::min(S::MinBlocks, tuned("spread.ctas_per_sm"))));
   count_launch();
-  spread_tc_kernel<CH, STAGES, AT><<<grid, kTcThreads, S::Smem, st>>>(g, offs, rec, vals, vs, nch, items, nItems,
-                                                                     tw0, slabPlanes, out, errFlag, workCounter);
+  spread_tc_kernel<CH, STAGES, AT, F16><<<grid, kTcThreads, S::Smem, st>>>(
+      g, offs, rec, vals, vs, nch, items, nItems, tw0, slabPlanes, out, errFlag, workCounter, valScale);
 }
 
 // BIPP_B200_SPREAD=warp selects the shared-memory-atomic spreader for every channel count
@@ -427,6 +427,19 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     lastItems = nItemsAll;
     lastGridBytes = (long long)g_.ntw * kTW * (long long)planeBytes * nch_;
   }
+  // spreader operands (tunable): 0 tf32 split with A in shared memory, 1 with A in tensor
+  // memory, 2 FP16 hi/lo (values scaled per channel by their largest magnitude)
+  const int operands = tc ? tuned("spread.operands") : 0;
+  valScale_.ensure(ctx_, kMaxChan * sizeof(unsigned));
+  if (operands == 2) {
+    B2_CUDA(cudaMemsetAsync(valScale_.get(), 0, kMaxChan * sizeof(unsigned), ctx_->stream));
+    if (lastPoints > 0) {
+      count_launch();
+      value_scale_kernel<<<std::min<long long>(4096, (lastPoints + 255) / 256), 256, 0, ctx_->stream>>>(
+          offsets_.get<int>() + nkeys_, vals_.get<float2>(), nch_, valScale_.get<unsigned>());
+      B2_CHECK_LAUNCH();
+    }
+  }
   const size_t smem = (size_t)nch_ * 2 * kTileCells * sizeof(float);
   errFlag_.ensure(ctx_, sizeof(int));
   B2_CUDA(cudaMemsetAsync(errFlag_.get(), 0, sizeof(int), ctx_->stream));
@@ -450,14 +463,20 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     if (stageMs) B2_CUDA(cudaEventRecord(ev[0], ctx_->stream));
     if (nItems > 0 && tc) {
       const bool two = tuned("spread.stages") == 2;
-      const bool at = tuned("spread.a_tmem") == 1;
-      auto launch = nch_ <= 4 ? (at ? (two ? launch_spread_tc<4, 2, true> : launch_spread_tc<4, 1, true>)
-                                    : (two ? launch_spread_tc<4, 2, false> : launch_spread_tc<4, 1, false>))
-                              : (at ? (two ? launch_spread_tc<8, 2, true> : launch_spread_tc<8, 1, true>)
-                                    : (two ? launch_spread_tc<8, 2, false> : launch_spread_tc<8, 1, false>));
+      using L = decltype(&launch_spread_tc<4, 1, false, false>);
+      // [channels 4 / 8][operands: tf32 split with A in shared memory / in tensor memory /
+      // FP16 hi-lo][stages 1 / 2]
+      static const L table[2][3][2] = {
+          {{launch_spread_tc<4, 1, false, false>, launch_spread_tc<4, 2, false, false>},
+           {launch_spread_tc<4, 1, true, false>, launch_spread_tc<4, 2, true, false>},
+           {launch_spread_tc<4, 1, false, true>, launch_spread_tc<4, 2, false, true>}},
+          {{launch_spread_tc<8, 1, false, false>, launch_spread_tc<8, 2, false, false>},
+           {launch_spread_tc<8, 1, true, false>, launch_spread_tc<8, 2, true, false>},
+           {launch_spread_tc<8, 1, false, true>, launch_spread_tc<8, 2, false, true>}}};
+      const L launch = table[nch_ <= 4 ? 0 : 1][operands][two ? 1 : 0];
       launch(g_, nItems, ctx_->stream, offsets_.get<int>(), rec_.get<PtRec>(), vals_.get<float2>(), valStride_, nch_,
              items_.get<SpreadItem>() + slabBegin[sl], tw0, slabPlanes, grid_.get<float2>(), errFlag_.get<int>(),
-             dynamic ? workCounters_.get<int>() + sl : nullptr);
+             dynamic ? workCounters_.get<int>() + sl : nullptr, valScale_.get<unsigned>());
       B2_CHECK_LAUNCH();
     } else if (nItems > 0) {
       const SpreadItem* it = items_.get<SpreadItem>() + slabBegin[sl];

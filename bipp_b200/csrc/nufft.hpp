@@ -79,6 +79,7 @@ private:
   DevBuf nTilde_, decon_, dl_, dm_, counts_, offsets_, cursor_, blockSums_, rec_, vals_, grid_, acc_;
   DevBuf itemKeys_, itemsAlt_, sortTmp_, workCounters_;
   DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, splitCount_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
+  DevBuf valScale_;   // per-channel value scale of the FP16 spreader operands
   // batched 2-D cuFFT plans by batch size (channels x slab planes)
   std::map<int, cufftHandle> plans_;
   int slabTiles_ = 1;

@@ -799,4 +799,32 @@ inline dim3 direct_sum_grid(long long nOut, long long nIn, int smCount, int ctas
   return dim3((unsigned)bx, (unsigned)by, 1);
 }
 
+// scale[c] = the largest |Re| or |Im| of channel c over the sorted points (vals[p nch + c],
+// p < *total), as FP32 bits (non-negative floats order as unsigned integers); scale[] is
+// zeroed before the launch
+static __global__ void value_scale_kernel(const int* __restrict__ total, const float2* __restrict__ vals, int nch,
+                                          unsigned* __restrict__ scale) {
+  __shared__ unsigned smax[kMaxChan];
+  if (threadIdx.x < kMaxChan) smax[threadIdx.x] = 0u;
+  __syncthreads();
+  const long long n = *total;
+  float m[kMaxChan];
+#pragma unroll
+  for (int c = 0; c < kMaxChan; ++c) m[c] = 0.f;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < kMaxChan; ++c) {
+      if (c < nch) {
+        const float2 v = vals[p * nch + c];
+        m[c] = fmaxf(m[c], fmaxf(fabsf(v.x), fabsf(v.y)));
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxChan; ++c)
+    if (c < nch) atomicMax(&smax[c], __float_as_uint(m[c]));
+  __syncthreads();
+  if (threadIdx.x < nch) atomicMax(scale + threadIdx.x, smax[threadIdx.x]);
+}
+
 }  // namespace bippb200

@@ -620,7 +620,7 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     const bool timing = pl->timing;
     pl->timing = false;
     std::string rep = "{";
-    const char* params[] = {"spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
+    const char* params[] = {"spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                             "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"};
     // Objective of a parameter: the device time of the stage it changes (CUDA events of
     // the pipeline's stage timers): spreading (with the tile clearing) for spread.*, the

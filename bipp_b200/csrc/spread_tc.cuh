@@ -15,6 +15,8 @@
 
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "nufft_kernels.cuh"
 #include "tc_common.cuh"
 
@@ -45,19 +47,24 @@ static_assert(kTX == 16 && kTY == 8 && kTW == 8 && kTcVisits == 16, "prep mappin
 // K-step of B is N rows x 8 tf32; CTAs per SM bounded by TMEM (512 columns) and shared
 // memory. With A in tensor memory the tensor cores read only B from shared memory, and
 // the threads store only B there: about half of the shared-memory traffic of a phase.
+// F16: operands split into FP16 hi + lo (kind::f16, K = 16: one K-step per 16-point
+// phase; half the operand bytes and MMAs of the tf32 split, so that two stages fit the
+// shared memory of 8 CTAs per SM). B is built from values scaled per channel into
+// [-1, 1] (FP16 range), the epilogue scales back.
 constexpr int tc_pow2_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
-template <int CH, int STAGES = 1, bool AT = false>
+template <int CH, int STAGES = 1, bool AT = false, bool F16 = false>
 struct TcShape {
   static constexpr int N = kTW * 2 * CH;
+  static constexpr int KSteps = F16 ? 1 : kTcSteps;              // MMA K-steps per phase
   static constexpr int AStageCols = AT ? 2 * kTcSteps * 8 : 0;   // A_hi, A_lo of a phase (K = 16 each)
   static constexpr int AColBase = N;                             // A of stage s at AColBase + s AStageCols
   static constexpr int Cols = tc_pow2_cols(N + STAGES * AStageCols);   // tensor-memory columns per CTA
   static constexpr int BStep = N * 8 * 4;
   static constexpr int OffAhi = 0;                // operands of stage 0; stage s at + s StageBytes
-  static constexpr int OffAlo = OffAhi + (AT ? 0 : kTcSteps * kTcAStep);
-  static constexpr int OffBhi = OffAlo + (AT ? 0 : kTcSteps * kTcAStep);
-  static constexpr int OffBlo = OffBhi + kTcSteps * BStep;
-  static constexpr int StageBytes = OffBlo + kTcSteps * BStep;
+  static constexpr int OffAlo = OffAhi + (AT ? 0 : KSteps * kTcAStep);
+  static constexpr int OffBhi = OffAlo + (AT ? 0 : KSteps * kTcAStep);
+  static constexpr int OffBlo = OffBhi + KSteps * BStep;
+  static constexpr int StageBytes = OffBlo + KSteps * BStep;
   static constexpr int OffEx = STAGES * StageBytes;        // float [16 x][kTcVS]
   static constexpr int OffEy = OffEx + kTX * kTcVS * 4;    // float [8 y][kTcVS]
   static constexpr int OffEw = OffEy + kTY * kTcVS * 4;    // float [8 w][kTcVS]
@@ -65,16 +72,39 @@ struct TcShape {
   static constexpr int Smem = OffVal + 2 * CH * kTcVS * 4;
   static constexpr int BySmem = 233472 / (Smem + 512 + 1024);
   static constexpr int MinBlocks = (512 / Cols) < BySmem ? (512 / Cols) : BySmem;   // CTAs per SM
-  // instruction descriptor: D f32, A/B tf32, both K-major, N, M = 128
-  static constexpr uint32_t Idesc =
-      (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+  // instruction descriptor: D f32, A/B tf32 (2) or f16 (0), both K-major, N, M = 128
+  static constexpr uint32_t Idesc = (1u << 4) | ((F16 ? 0u : 2u) << 7) | ((F16 ? 0u : 2u) << 10) |
+                                    ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
   static_assert(CH == 4 || CH == 8, "4 or 8 channels");
+  static_assert(!(AT && F16), "tensor-memory A with the tf32 split only");
   static_assert(N % 16 == 0 && N <= 256, "MMA N for M = 128");
   static_assert(OffEx % 1024 == 0, "operand blocks 1 KB aligned");
   static_assert(STAGES == 1 || STAGES == 2, "one or two operand stages");
   static_assert(MinBlocks >= 1 && MinBlocks * (Smem + 512 + 1024) <= 233472,
                 "shared memory (dynamic + static <= 512 B + 1 KB reserved) for MinBlocks CTAs per SM");
 };
+
+// FP16 hi + lo of two values, each pair packed in one 32-bit word (low half = first):
+// hi rounded to FP16, lo = FP16 of the exact FP32 remainder
+__device__ __forceinline__ void split_f16x2(float2 x, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __float22half2_rn(x);
+  const float2 hf = __half22float2(h);
+  const __half2 l = __float22half2_rn(make_float2(x.x - hf.x, x.y - hf.y));
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+__device__ __forceinline__ void tc_mma_f16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void st_shared_v4w(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
 
 // The 27 (source direction d, crossing bits) pairs whose key ranges reach a tile, in
 // the order tile_ranges() visits them: d in 0..7, bits a superset of d.
@@ -91,13 +121,13 @@ __device__ __forceinline__ int tc_range_pair(int j) {
 
 // Persistent: each CTA takes work items blockIdx.x, blockIdx.x + gridDim.x, ... or, with
 // a work counter, the next item of the (load-ordered) list whenever it is free
-template <int CH, int STAGES, bool AT = false>
-static __global__ void __launch_bounds__(kTcThreads, TcShape<CH, STAGES, AT>::MinBlocks)
+template <int CH, int STAGES, bool AT = false, bool F16 = false>
+static __global__ void __launch_bounds__(kTcThreads, TcShape<CH, STAGES, AT, F16>::MinBlocks)
 spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __restrict__ rec,
                  const float2* __restrict__ vals, long long valStride, int nch, const SpreadItem* __restrict__ items,
                  int nItems, int tw0, int slabPlanes, float2* __restrict__ grid, int* __restrict__ errFlag,
-                 int* __restrict__ workCounter) {
-  using S = TcShape<CH, STAGES, AT>;
+                 int* __restrict__ workCounter, const unsigned* __restrict__ valScale = nullptr) {
+  using S = TcShape<CH, STAGES, AT, F16>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar[STAGES];   // MMA completion of the phases of each stage
   __shared__ uint32_t tmemSlot;
@@ -188,6 +218,18 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     // data of the next phase are loaded into registers while the current phase is built.
     constexpr int CPR = CH / 2;   // channels per value role
     const int pv = tid & 15, pa = tid >> 4;
+    // F16: this thread's value channels scaled into [-1, 1] (valScale: per-channel max of
+    // |Re|, |Im| as FP32 bits)
+    float invS[CPR];
+#pragma unroll
+    for (int cc = 0; cc < CPR; ++cc) {
+      invS[cc] = 1.f;
+      if constexpr (F16) {
+        const int c = CPR * (pa >= 6 ? pa - 6 : 0) + cc;
+        const float sc = (c < nch) ? __uint_as_float(valScale[c]) : 0.f;
+        invS[cc] = sc > 0.f ? 1.f / sc : 0.f;
+      }
+    }
     int ri = 0;
     int pfL = 0;
     float pfD = 0.f;
@@ -221,7 +263,8 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
     fetch(0);
     for (int v0 = 0; v0 < nvis; v0 += kTcVisits) {
       const int nk = min(kTcVisits, nvis - v0);
-      const int steps = (nk + 7) >> 3;
+      const int steps = F16 ? 1 : (nk + 7) >> 3;
+      const int kpad = F16 ? kTcVisits : steps * 8;   // visits of the phase's K-steps
       // operand stage of this phase
       const int stg = STAGES == 1 ? 0 : (v0 / kTcVisits) & 1;
       const uint32_t sstage = sbase + (uint32_t)(stg * S::StageBytes);
@@ -255,11 +298,11 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
 #pragma unroll
             for (int cc = 0; cc < CPR; ++cc) {
               const int c = CPR * (pa - 6) + cc;
-              val[tab_sw(2 * c, pv)] = pfX[cc].x;
-              val[tab_sw(2 * c + 1, pv)] = pfX[cc].y;
+              val[tab_sw(2 * c, pv)] = pfX[cc].x * invS[cc];
+              val[tab_sw(2 * c + 1, pv)] = pfX[cc].y * invS[cc];
             }
           }
-        } else if (pv < steps * 8) {
+        } else if (pv < kpad) {
           // padding visits of the last K-step contribute nothing (values too: 0 x stale
           // shared memory could be 0 x NaN)
 #pragma unroll
@@ -277,7 +320,23 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       if (!sOk) break;
       if (v0 + kTcVisits < nvis) fetch(v0 + kTcVisits);
       // A: row tid (cell xm, ym), 8 visits per K-step
-      for (int s = 0; s < steps; ++s) {
+      if constexpr (F16) {
+        // one K-step of 16 visits: FP16 hi/lo, k 0-7 and 8-15 in the two 16-byte halves
+        uint32_t h[8], l[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 xq = *reinterpret_cast<const float4*>(ex + tab_sw(xm, 4 * q));
+          const float4 yq = *reinterpret_cast<const float4*>(ey + ym * kTcVS + 4 * q);
+          split_f16x2(__fmul2_rn(make_float2(xq.x, xq.y), make_float2(yq.x, yq.y)), h[2 * q], l[2 * q]);
+          split_f16x2(__fmul2_rn(make_float2(xq.z, xq.w), make_float2(yq.z, yq.w)), h[2 * q + 1], l[2 * q + 1]);
+        }
+        const uint32_t ah = sstage + S::OffAhi + tid * 16, al = sstage + S::OffAlo + tid * 16;
+        st_shared_v4w(ah, h[0], h[1], h[2], h[3]);
+        st_shared_v4w(ah + kTcAStep / 2, h[4], h[5], h[6], h[7]);
+        st_shared_v4w(al, l[0], l[1], l[2], l[3]);
+        st_shared_v4w(al + kTcAStep / 2, l[4], l[5], l[6], l[7]);
+      }
+      for (int s = 0; s < (F16 ? 0 : steps); ++s) {
         float h[8], l[8];
         {
           const float4 x0 = *reinterpret_cast<const float4*>(ex + tab_sw(xm, 8 * s));
@@ -313,7 +372,28 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
       }
       // B: row n = plane * 2 CH + channel * 2 + (re|im); TPR threads per row, each with
       // VPT visits of the K-step
-      {
+      if constexpr (F16) {
+        // one K-step of 16 visits; TPR threads per row, each with 8 (TPR = 2) or 16 visits
+        constexpr int TPR = kTcThreads / S::N, VPT = kTcVisits / TPR;
+        const int n = tid % S::N, kh = tid / S::N;
+        const int plane = n / (2 * CH), cc = n % (2 * CH);
+#pragma unroll
+        for (int q = 0; q < VPT / 8; ++q) {
+          const int v = kh * VPT + 8 * q;   // first visit of this 16-byte chunk
+          const float4 e0 = *reinterpret_cast<const float4*>(ew + plane * kTcVS + v);
+          const float4 e1 = *reinterpret_cast<const float4*>(ew + plane * kTcVS + v + 4);
+          const float4 c0 = *reinterpret_cast<const float4*>(val + tab_sw(cc, v));
+          const float4 c1 = *reinterpret_cast<const float4*>(val + tab_sw(cc, v + 4));
+          uint32_t h[4], l[4];
+          split_f16x2(__fmul2_rn(make_float2(e0.x, e0.y), make_float2(c0.x, c0.y)), h[0], l[0]);
+          split_f16x2(__fmul2_rn(make_float2(e0.z, e0.w), make_float2(c0.z, c0.w)), h[1], l[1]);
+          split_f16x2(__fmul2_rn(make_float2(e1.x, e1.y), make_float2(c1.x, c1.y)), h[2], l[2]);
+          split_f16x2(__fmul2_rn(make_float2(e1.z, e1.w), make_float2(c1.z, c1.w)), h[3], l[3]);
+          const uint32_t off = (uint32_t)((v >> 3) * (S::BStep / 2) + n * 16);
+          st_shared_v4w(sstage + S::OffBhi + off, h[0], h[1], h[2], h[3]);
+          st_shared_v4w(sstage + S::OffBlo + off, l[0], l[1], l[2], l[3]);
+        }
+      } else {
         constexpr int TPR = kTcThreads / S::N, VPT = 8 / TPR;
         const int n = tid % S::N, kh = tid / S::N;
         const int plane = n / (2 * CH), cc = n % (2 * CH);
@@ -353,7 +433,13 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
         for (int s = 0; s < steps; ++s) {
           const uint64_t dBh = tc_desc(sstage + S::OffBhi + s * S::BStep, S::BStep / 2, 128);
           const uint64_t dBl = tc_desc(sstage + S::OffBlo + s * S::BStep, S::BStep / 2, 128);
-          if constexpr (AT) {
+          if constexpr (F16) {
+            const uint64_t dAh = tc_desc(sstage + S::OffAhi, kTcAStep / 2, 128);
+            const uint64_t dAl = tc_desc(sstage + S::OffAlo, kTcAStep / 2, 128);
+            tc_mma_f16(tmem, dAh, dBh, S::Idesc, v0 > 0 ? 1u : 0u);
+            tc_mma_f16(tmem, dAh, dBl, S::Idesc, 1u);
+            tc_mma_f16(tmem, dAl, dBh, S::Idesc, 1u);
+          } else if constexpr (AT) {
             const uint32_t aHi = tmem + (uint32_t)(S::AColBase + stg * S::AStageCols + 8 * s);
             tc_mma_ta(tmem, aHi, dBh, S::Idesc, (v0 > 0 || s > 0) ? 1u : 0u);
             tc_mma_ta(tmem, aHi, dBl, S::Idesc, 1u);
@@ -393,7 +479,12 @@ spread_tc_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __re
 #pragma unroll
           for (int c = 0; c < CH; ++c) {
             if (c < nch) {
-              const float2 v = make_float2(r[pl * 2 * CH + 2 * c], r[pl * 2 * CH + 2 * c + 1]);
+              float2 v = make_float2(r[pl * 2 * CH + 2 * c], r[pl * 2 * CH + 2 * c + 1]);
+              if constexpr (F16) {
+                const float sc = __uint_as_float(__ldg(valScale + c));   // undo the value scaling
+                v.x *= sc;
+                v.y *= sc;
+              }
               float2* dst = grid + slab_index(g, nch, slabPlanes, c, plane, y0 + ym, x0 + xm);
               if (it.nparts == 1) {
                 *dst = v;

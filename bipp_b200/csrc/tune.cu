@@ -46,8 +46,10 @@ std::vector<Param>& table() {
        0},
       {"spread.stages", 1, {1, 2},
        "operand stages of the tensor-core spreader (2: a phase is built while the previous one's MMAs run)", 0},
-      {"spread.a_tmem", 0, {0, 1},
-       "A operand of the tensor-core spreader: 0 shared memory, 1 tensor memory (tcgen05.st by each thread)", 0},
+      {"spread.operands", 0, {0, 1, 2},
+       "tensor-core spreader operands: 0 tf32 split, A in shared memory; 1 tf32 split, A in tensor memory "
+       "(tcgen05.st by each thread); 2 FP16 hi/lo (kind::f16), values scaled per channel",
+       0},
       {"spread.schedule", 0, {0, 1},
        "spreading work items: 0 round-robin over the persistent CTAs, 1 heaviest first from a work counter", 0},
       {"hetrd.threads", 0, {0, 256, 512, 1024}, "threads per matrix in the tridiagonalisation (0: by matrix size)", 0},

@@ -153,7 +153,7 @@ def test_tuning_table_without_a_gpu(tmp_path):
     bipp.tuning_reset()
     assert bipp.tuning_get("spread.items_cap") == 2048 and bipp.tuning_get("hetrd.threads") == 0
     desc = bipp.tuning_describe()
-    assert set(desc) == {"spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
+    assert set(desc) == {"spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                          "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm", "direct.ctas_per_sm"}
     assert desc["spread.items_cap"]["candidates"] == [2048, 4096, 8192]
     with pytest.raises(bipp.InvalidParameterError):

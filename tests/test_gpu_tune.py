@@ -38,7 +38,7 @@ def test_autotune_pipeline(ctx):
     rep = pl.autotune(64, S.data_ptr(), x.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
     print(rep)
     desc = bipp.tuning_describe()
-    for name in ("spread.items_cap", "spread.a_tmem", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
+    for name in ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
                  "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"):
         assert rep[name]["chosen"] == desc[name]["value"]
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
@@ -53,8 +53,9 @@ def test_autotune_pipeline(ctx):
 
 
 def test_spreader_variants_agree(ctx):
-    """The tunable spreader variants (one or two operand stages, A operand in shared or
-    tensor memory, round-robin or heaviest-first dynamic schedule, work-item caps) give the same images to 1e-5
+    """The tunable spreader variants (one or two operand stages; tf32-split operands with
+    A in shared or tensor memory, or FP16 hi/lo operands; round-robin or heaviest-first
+    dynamic schedule; work-item caps) give the same images to 1e-5
     relative L2 per level on a batch that splits heavy tiles (the cap changes which tiles
     are split, so the FP32 sums of their parts are added in another order: differences of
     ~2e-6 were measured)."""
@@ -90,8 +91,9 @@ def test_spreader_variants_agree(ctx):
     base, st = run()
     assert st["split_tiles"] > 0 or bipp.tuning_get("spread.items_cap") > 2048
     for settings in ({"spread.stages": 2}, {"spread.schedule": 1}, {"spread.stages": 2, "spread.schedule": 1},
-                     {"spread.items_cap": 2048, "spread.stages": 2}, {"spread.a_tmem": 1},
-                     {"spread.a_tmem": 1, "spread.stages": 2, "spread.schedule": 1}):
+                     {"spread.items_cap": 2048, "spread.stages": 2}, {"spread.operands": 1},
+                     {"spread.operands": 1, "spread.stages": 2, "spread.schedule": 1}, {"spread.operands": 2},
+                     {"spread.operands": 2, "spread.stages": 2}):
         bipp.tuning_reset()
         for k, v in settings.items():
             bipp.tuning_set(k, v)
