@@ -50,7 +50,7 @@ std::vector<Param>& table() {
        "tensor-core spreader operands: 0 tf32 split, A in shared memory; 1 tf32 split, A in tensor memory "
        "(tcgen05.st by each thread); 2 FP16 hi/lo (kind::f16), values scaled per channel",
        0},
-      {"spread.schedule", 0, {0, 1},
+      {"spread.schedule", 1, {0, 1},
        "spreading work items: 0 round-robin over the persistent CTAs, 1 heaviest first from a work counter", 0},
       {"hetrd.threads", 0, {0, 256, 512, 1024}, "threads per matrix in the tridiagonalisation (0: by matrix size)", 0},
       {"hetrd.ctas_pct", 0, {0, 50, 75, 100, 150},

@@ -90,7 +90,7 @@ def test_spreader_variants_agree(ctx):
 
     base, st = run()
     assert st["split_tiles"] > 0 or bipp.tuning_get("spread.items_cap") > 2048
-    for settings in ({"spread.stages": 2}, {"spread.schedule": 1}, {"spread.stages": 2, "spread.schedule": 1},
+    for settings in ({"spread.stages": 2}, {"spread.schedule": 0}, {"spread.stages": 2, "spread.schedule": 0},
                      {"spread.items_cap": 2048, "spread.stages": 2}, {"spread.operands": 1},
                      {"spread.operands": 1, "spread.stages": 2, "spread.schedule": 1}, {"spread.operands": 2},
                      {"spread.operands": 2, "spread.stages": 2}):
