@@ -326,8 +326,18 @@ def spread_roofline(stats, spread_ms, n_levels):
             "peak_source": label, "traffic": traffic, "algorithmic_bytes_per_launch": int(per_launch),
             "launches_per_step": slabs, "launch_ms": round(dur_s * 1000.0, 3),
             "flops_per_launch": int(flops), "achieved_tflops": round(flops / dur_s / 1e12, 3),
-            "note": "tcgen05 3xTF32 spreading; bound by building the dense operands (issue), "
-                    "the HBM fraction is its floor"}
+            "note": spread_operands_note() + "; bound by building the dense operands (latency at "
+                    "32 warps per SM), the HBM fraction is its floor"}
+
+
+def spread_operands_note():
+    """Which operand form the spreader ran with (the tuning table's spread.operands)."""
+    import bipp_b200 as bipp
+
+    mode = bipp.tuning_get("spread.operands")
+    return {0: "tcgen05 kind::tf32 spreading, 3xTF32 split, A in shared memory",
+            1: "tcgen05 kind::tf32 spreading, 3xTF32 split, A in tensor memory",
+            2: "tcgen05 kind::f16 spreading, FP16 hi/lo split (3 MMAs), values scaled per level"}.get(mode, str(mode))
 
 
 def run_reference(args):

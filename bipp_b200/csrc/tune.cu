@@ -44,9 +44,9 @@ std::vector<Param>& table() {
       {"spread.items_cap", 2048, {2048, 4096, 8192}, "points per spreading work item (heavier tiles are split)", 0},
       {"spread.ctas_per_sm", 8, {2, 4, 8}, "resident tensor-core spreading CTAs per SM (at most 512 / TMEM columns)",
        0},
-      {"spread.stages", 1, {1, 2},
+      {"spread.stages", 2, {1, 2},
        "operand stages of the tensor-core spreader (2: a phase is built while the previous one's MMAs run)", 0},
-      {"spread.operands", 0, {0, 1, 2},
+      {"spread.operands", 2, {0, 1, 2},
        "tensor-core spreader operands: 0 tf32 split, A in shared memory; 1 tf32 split, A in tensor memory "
        "(tcgen05.st by each thread); 2 FP16 hi/lo (kind::f16), values scaled per channel",
        0},
