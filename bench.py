@@ -297,12 +297,12 @@ def measured_peaks():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of the
-# spreading kernel, measured with ncu over all three spreading launches of a 128-step
-# batch of this workload (512 antennas, 1024^2 px, 4 levels, 2 GB w-slabs): 4.773e9 DRAM
-# bytes for 5.493e9 algorithmic bytes. The traffic of a full launch is taken to scale with
+# spreading kernel (FP16 hi/lo operands), measured with ncu over all three spreading
+# launches of a 128-step batch of this workload (512 antennas, 1024^2 px, 4 levels, 2 GB
+# w-slabs): 4.742e9 DRAM bytes for 5.493e9 algorithmic bytes. The traffic of a full launch is taken to scale with
 # the points and cells it processes, as the algorithmic bytes do (tiles without points are
 # cleared by their own kernel, so the ratio is below 1).
-SPREAD_TRAFFIC_PER_ALG_BYTE = 0.869
+SPREAD_TRAFFIC_PER_ALG_BYTE = 0.863
 
 
 def spread_roofline(stats, spread_ms, n_levels):
