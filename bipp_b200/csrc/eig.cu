@@ -367,23 +367,33 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     bt_larft_kernel<C, R><<<dim3(std::max(1, nblk), nb), 256, 0, st>>>(A, w.tau.template get<C>(), nred, Nmax, Tblk,
                                                                        tStride);
     B2_CHECK_LAUNCH();
-    const dim3 grid((Nmax + kBtCB - 1) / kBtCB, nb);
-#define B2_BT(KR, NT)                                                                        \
+#define B2_BT(KR, NT, CB)                                                                    \
   {                                                                                          \
-    auto k = bt_apply_kernel<C, R, KR, NT>;                                                  \
-    const size_t smem = bt_apply_smem(Nmax, sizeof(C), NT);                                  \
+    auto k = bt_apply_kernel<C, R, KR, NT, CB>;                                              \
+    const size_t smem = bt_apply_smem(Nmax, sizeof(C), NT, CB);                              \
     smem_optin(k, smem);                                                                     \
     count_launch();                                                                          \
-    k<<<grid, NT, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange, sizeOrder);       \
+    k<<<dim3((Nmax + CB - 1) / CB, nb), NT, smem, st>>>(A, Tblk, tStride, Z, nred, Nmax, T1, krange, sizeOrder); \
   }
-    // 64 row groups of 256 threads up to 512 rows; 128 row groups of 512 threads above
+    // up to 512 rows: 16-column slices on 256 threads (64 row groups of 4 column groups), or
+    // (tunable) 32-column slices on 512 threads (64 row groups of 8 column groups), which
+    // load every reflector block half as often per column; above 512 rows 16-column
+    // slices on 512 threads (128 row groups)
     if (Nmax <= 512) {
       const int kr = (Nmax + 63) / 64;
-      if (kr <= 2) B2_BT(2, 256) else if (kr <= 4) B2_BT(4, 256) else if (kr <= 6) B2_BT(6, 256) else B2_BT(8, 256)
+      if (tuned("bt.columns") == 32) {
+        if constexpr (sizeof(C) == 8) {
+          if (kr <= 2) B2_BT(2, 512, 32) else if (kr <= 4) B2_BT(4, 512, 32) else if (kr <= 6) B2_BT(6, 512, 32) else B2_BT(8, 512, 32)
+        } else {
+          if (kr <= 2) B2_BT(2, 256, 16) else if (kr <= 4) B2_BT(4, 256, 16) else if (kr <= 6) B2_BT(6, 256, 16) else B2_BT(8, 256, 16)
+        }
+      } else {
+        if (kr <= 2) B2_BT(2, 256, 16) else if (kr <= 4) B2_BT(4, 256, 16) else if (kr <= 6) B2_BT(6, 256, 16) else B2_BT(8, 256, 16)
+      }
     } else {
       if constexpr (sizeof(C) == 8) {
         const int kr = (Nmax + 127) / 128;
-        if (kr <= 6) B2_BT(6, 512) else B2_BT(8, 512)
+        if (kr <= 6) B2_BT(6, 512, 16) else B2_BT(8, 512, 16)
       }
     }
 #undef B2_BT

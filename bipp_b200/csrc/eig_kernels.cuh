@@ -1668,29 +1668,32 @@ bt_larft_kernel(const C* __restrict__ A, const C* __restrict__ taus, const int* 
 constexpr int kBtVS = kBtNB + 2;             // padded row stride of the V block (16-byte aligned rows)
 constexpr int kBtJC = 2;                     // reflectors per register chunk
 
-template <typename C, typename R, int KR, int NT>
+template <typename C, typename R, int KR, int NT, int CB = kBtCB>
 __global__ void __launch_bounds__(NT, (sizeof(C) == 8 ? 512 : 256) / NT > 0 ? (sizeof(C) == 8 ? 512 : 256) / NT : 1)
 bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tStride, const R* __restrict__ Z,
                 const int* __restrict__ nred, int Nmax, C* __restrict__ Y, const int* __restrict__ krange,
                 const int* __restrict__ order = nullptr) {
   const int b = order ? order[blockIdx.y] : blockIdx.y;
   const int n = nred[b];
-  const int c0 = blockIdx.x * kBtCB;
+  const int c0 = blockIdx.x * CB;
   if (c0 >= n) return;
   // only the eigenvector columns [cLo, cHi) are transformed
   const int cLo = krange ? krange[2 * b] : 0, cHi = krange ? krange[2 * b + 1] : n;
-  if (c0 + kBtCB <= cLo || c0 >= cHi) return;
+  if (c0 + CB <= cLo || c0 >= cHi) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* Vs = reinterpret_cast<C*>(smem_raw);              // [Nmax][kBtVS] block of reflectors (row-major)
-  constexpr int RG = NT / 4, NW = NT / 32;
-  static_assert(NT >= kBtNB * kBtCB, "one thread per element of W");
-  C* red = Vs + (long long)Nmax * kBtVS;               // [NW warps][16 j][16 c]
-  C* Ts = red + NW * kBtNB * kBtCB;                    // [16][16]
-  C* Wt = Ts + kBtNB * kBtNB;                          // [16 j][16 c]
+  // CGN column groups of 4 columns; RG row groups (the lanes of a warp with the same
+  // column group are 32 / CGN of them)
+  constexpr int CGN = CB / 4, RG = NT / CGN, NW = NT / 32;
+  static_assert(NT >= kBtNB * CB, "one thread per element of W");
+  static_assert(CB == 16 || CB == 32, "16 or 32 columns per CTA");
+  C* red = Vs + (long long)Nmax * kBtVS;               // [NW warps][16 j][CB c]
+  C* Ts = red + NW * kBtNB * CB;                       // [16][16]
+  C* Wt = Ts + kBtNB * kBtNB;                          // [16 j][CB c]
   const C* Ab = A + (long long)b * Nmax * Nmax;
   const R* Zb = Z + (long long)b * Nmax * Nmax;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int cg = tid & 3, rg = tid >> 2;
+  const int cg = tid % CGN, rg = tid / CGN;
   C y[KR][4];
 #pragma unroll
   for (int q = 0; q < KR; ++q) {
@@ -1744,35 +1747,35 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
 #pragma unroll
-          for (int o = 4; o < 32; o <<= 1) {
+          for (int o = CGN; o < 32; o <<= 1) {
             w[a][u].x += __shfl_xor_sync(0xffffffffu, w[a][u].x, o);
             w[a][u].y += __shfl_xor_sync(0xffffffffu, w[a][u].y, o);
           }
         }
-      if (lane < 4) {
+      if (lane < CGN) {
 #pragma unroll
         for (int a = 0; a < kBtJC; ++a)
 #pragma unroll
-          for (int u = 0; u < 4; ++u) red[(warp * kBtNB + kBtJC * jc + a) * kBtCB + 4 * cg + u] = w[a][u];
+          for (int u = 0; u < 4; ++u) red[(warp * kBtNB + kBtJC * jc + a) * CB + 4 * cg + u] = w[a][u];
       }
     }
     __syncthreads();
     // W[j][c] over the NW warps, then Wt = T W (thread = (j, c))
     {
-      const bool act = tid < kBtNB * kBtCB;
-      const int j = (tid / kBtCB) % kBtNB, c = tid % kBtCB;
+      const bool act = tid < kBtNB * CB;
+      const int j = (tid / CB) % kBtNB, c = tid % CB;
       C s0 = mk(R(0), R(0));
       if (act) {
 #pragma unroll
-        for (int g = 0; g < NW; ++g) s0 = s0 + red[(g * kBtNB + j) * kBtCB + c];
+        for (int g = 0; g < NW; ++g) s0 = s0 + red[(g * kBtNB + j) * CB + c];
       }
       __syncthreads();
-      if (act) red[j * kBtCB + c] = s0;
+      if (act) red[j * CB + c] = s0;
       __syncthreads();
       if (act) {
         C t = mk(R(0), R(0));
-        for (int l = j; l < kBtNB; ++l) cfma(t, Ts[j * kBtNB + l], red[l * kBtCB + c]);
-        Wt[j * kBtCB + c] = t;
+        for (int l = j; l < kBtNB; ++l) cfma(t, Ts[j * kBtNB + l], red[l * CB + c]);
+        Wt[j * CB + c] = t;
       }
     }
     __syncthreads();
@@ -1783,7 +1786,7 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
 #pragma unroll
       for (int a = 0; a < kBtJC; ++a)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) wt[a][u] = Wt[(kBtJC * jc + a) * kBtCB + 4 * cg + u];
+        for (int u = 0; u < 4; ++u) wt[a][u] = Wt[(kBtJC * jc + a) * CB + 4 * cg + u];
 #pragma unroll
       for (int q = 0; q < KR; ++q) {
         const int r = rg + RG * q;
@@ -1818,9 +1821,9 @@ bt_apply_kernel(const C* __restrict__ A, const C* __restrict__ Tin, long long tS
   }
 }
 
-// shared memory of bt_apply_kernel with nt threads
-constexpr size_t bt_apply_smem(int Nmax, size_t complexBytes, int nt) {
-  return ((size_t)Nmax * kBtVS + (nt / 32) * kBtNB * kBtCB + kBtNB * kBtNB + kBtNB * kBtCB) * complexBytes;
+// shared memory of bt_apply_kernel with nt threads and cb columns per CTA
+constexpr size_t bt_apply_smem(int Nmax, size_t complexBytes, int nt, int cb = kBtCB) {
+  return ((size_t)Nmax * kBtVS + (nt / 32) * kBtNB * cb + kBtNB * kBtNB + kBtNB * cb) * complexBytes;
 }
 
 }  // namespace bippb200

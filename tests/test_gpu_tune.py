@@ -39,7 +39,7 @@ def test_autotune_pipeline(ctx):
     print(rep)
     desc = bipp.tuning_describe()
     for name in ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-                 "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"):
+                 "hetrd.threads", "hetrd.ctas_pct", "bt.columns", "vv.ctas_per_sm"):
         assert rep[name]["chosen"] == desc[name]["value"]
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
     assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
@@ -105,10 +105,11 @@ def test_spreader_variants_agree(ctx):
 
 
 def test_persistent_tridiagonalisation_agrees(ctx):
-    """The tridiagonalisation run as persistent CTAs (fewer than the matrices, each taking
-    matrices in the size order) gives the eigenvalues and V diag(d) V^H of the default of
-    one CTA per matrix, to 1e-6 relative, on 40 steps of uneven size (100-160 of 160
-    antennas kept, so that the blocked panels run)."""
+    """The eigensolver's tunable launch shapes give the eigenvalues and V diag(d) V^H of
+    the defaults, to 1e-6 relative, on 40 steps of uneven size (100-160 of 160 antennas
+    kept, so that the blocked panels run): the tridiagonalisation as persistent CTAs
+    (fewer than the matrices, each taking matrices in the size order) and the
+    back-transform on 32-column slices."""
     import bipp_b200 as bipp
     from bipp_b200 import simulate as sim
 
@@ -120,8 +121,9 @@ def test_persistent_tridiagonalisation_agrees(ctx):
     wl = np.full(40, cfg.wl, np.float32)
     v0, d0, n0, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
     try:
-        for pct in (50, 150):
-            bipp.tuning_set("hetrd.ctas_pct", pct)
+        for pct in (("hetrd.ctas_pct", 50), ("hetrd.ctas_pct", 150), ("bt.columns", 32)):
+            bipp.tuning_reset()
+            bipp.tuning_set(*pct)
             v1, d1, n1, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
             assert np.array_equal(n0, n1)
             for b in range(40):
