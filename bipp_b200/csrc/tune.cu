@@ -56,7 +56,9 @@ std::vector<Param>& table() {
       {"hetrd.ctas_pct", 0, {0, 50, 75, 100, 150},
        "persistent tridiagonalisation CTAs in percent of the SM count (0: one CTA per matrix)", 0},
       {"bt.columns", 16, {16, 32},
-       "eigenvector columns per CTA of the blocked back-transform (32: 512 threads, up to 512 rows)", 0},
+       "eigenvector columns per CTA of the blocked back-transform (32: 512 threads, up to 512 rows; "
+       "not autotuned: 6 % faster back-transform but a slower whole call on the 2048-step batch)",
+       0},
       {"vv.ctas_per_sm", 3, {1, 2, 3}, "persistent tensor-core virtual-visibility CTAs per SM", 0},
       {"direct.ctas_per_sm", 4, {2, 4, 8}, "direct-sum CTAs per SM below which the inputs are split", 0},
   };

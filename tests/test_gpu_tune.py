@@ -39,7 +39,7 @@ def test_autotune_pipeline(ctx):
     print(rep)
     desc = bipp.tuning_describe()
     for name in ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-                 "hetrd.threads", "hetrd.ctas_pct", "bt.columns", "vv.ctas_per_sm"):
+                 "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"):
         assert rep[name]["chosen"] == desc[name]["value"]
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
     assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
