@@ -633,6 +633,29 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
       if (!std::strncmp(name, "hetrd.", 6)) return pl->eigMs[4];
       return pl->stageMs[1];
     };
+    // the whole call with a set of values: the faster of two timed calls (CUDA events)
+    auto whole_call_ms = [&](const std::vector<int>& vals) {
+      for (size_t i = 0; i < vals.size(); ++i) set_tuned(params[i], vals[i]);
+      cudaEvent_t a, b;
+      B2_CUDA(cudaEventCreate(&a));
+      B2_CUDA(cudaEventCreate(&b));
+      float best = 0.f;
+      for (int r = 0; r < 2; ++r) {
+        B2_CUDA(cudaEventRecord(a, ctx->stream));
+        pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
+        B2_CUDA(cudaEventRecord(b, ctx->stream));
+        B2_CUDA(cudaEventSynchronize(b));
+        float t = 0.f;
+        B2_CUDA(cudaEventElapsedTime(&t, a, b));
+        best = r ? std::min(best, t) : t;
+      }
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      return (double)best;
+    };
+    const size_t nParams = sizeof(params) / sizeof(params[0]);
+    std::vector<int> startVals(nParams);
+    for (size_t i = 0; i < nParams; ++i) startVals[i] = tuned(params[i]);
     auto body = [&] {
       pipeline_process(pl, nSteps, s, xyz, wl, onDevice);   // warm-up (allocations, first-use costs)
       bool first = true;
@@ -672,6 +695,21 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
         std::snprintf(buf, sizeof(buf), ", \"chosen\": %d}", cands[bi]);
         rep += buf;
       }
+      // a value can speed up its own stage and slow the call down elsewhere: the tuned set
+      // is kept only if the whole call is not slower than with the starting values
+      std::vector<int> tunedVals(nParams);
+      for (size_t i = 0; i < nParams; ++i) tunedVals[i] = tuned(params[i]);
+      pl->timing = false;
+      const double t1 = whole_call_ms(tunedVals), s1 = whole_call_ms(startVals);
+      const double s2 = whole_call_ms(startVals), t2 = whole_call_ms(tunedVals);
+      const double tMs = std::min(t1, t2), sMs = std::min(s1, s2);
+      const bool keep = tMs <= sMs;
+      if (!keep)
+        for (size_t i = 0; i < nParams; ++i) set_tuned(params[i], startVals[i]);
+      char buf[160];
+      std::snprintf(buf, sizeof(buf), ", \"whole_call_ms\": {\"tuned\": %.3f, \"starting\": %.3f, \"kept\": \"%s\"}",
+                    tMs, sMs, keep ? "tuned" : "starting");
+      rep += buf;
     };
     // the caller's state comes back on every exit path
     auto restore = [&] {

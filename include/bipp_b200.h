@@ -383,8 +383,11 @@ BIPP_B200_EXPORT BippError bipp_selftest_wait_timeout(bipp_ctx_t ctx, int spins,
  * tridiagonalisation kernel, or the virtual visibilities): every candidate gets one
  * untimed call, then max(2, repeats) passes over the candidates, forwards and backwards
  * in turn, and the fastest call of each counts. The fastest candidate of each parameter
- * is kept in the process-wide tuning table and a JSON report of those times (ms) is
- * written into report (reportLen bytes, truncated). The pipeline's images and step count
+ * is kept in the process-wide tuning table, unless the whole call with the tuned set is
+ * slower than with the starting values (a value can speed up its own stage and slow the
+ * call down elsewhere; both sets timed twice, interleaved), in which case the starting
+ * values come back. A JSON report of those times (ms, and "whole_call_ms") is written
+ * into report (reportLen bytes, truncated). The pipeline's images and step count
  * are left as they were. Results do not depend on the chosen values beyond rounding. */
 BIPP_B200_EXPORT BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* s, const double* xyz,
                                                   const double* wl, int onDevice, int repeats, char* report,

@@ -35,12 +35,18 @@ def test_autotune_pipeline(ctx):
                        chunk_steps=64, max_steps=64)
     pl.process_device(64, S.data_ptr(), x.data_ptr(), wl.data_ptr())
     base = pl.images().astype(np.float64)
+    names = ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
+             "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm")
+    start = {name: bipp.tuning_get(name) for name in names}
     rep = pl.autotune(64, S.data_ptr(), x.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
     print(rep)
     desc = bipp.tuning_describe()
-    for name in ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-                 "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"):
-        assert rep[name]["chosen"] == desc[name]["value"]
+    whole = rep["whole_call_ms"]
+    assert whole["kept"] in ("tuned", "starting")
+    assert (whole["tuned"] <= whole["starting"]) == (whole["kept"] == "tuned")
+    for name in names:
+        # the tuned values, or the starting ones if the tuned set made the whole call slower
+        assert desc[name]["value"] == (rep[name]["chosen"] if whole["kept"] == "tuned" else start[name])
         assert sorted(int(k) for k in rep[name] if k != "chosen") == desc[name]["candidates"]
     assert np.array_equal(pl.images().astype(np.float64), base)   # images left as they were
     pl.reset()
