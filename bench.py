@@ -604,7 +604,6 @@ def main():
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(stream)
         pp.process_device(ns, S.data_ptr(), xyz.data_ptr(), wl.data_ptr())
-        pp.flush()
         p1.record(stream)
         torch.cuda.synchronize()
         pv = ns / cfg.n_channels / (p0.elapsed_time(p1) / 1000.0)
