@@ -101,8 +101,6 @@ SIGNATURES = {
     "bipp_pipeline_process": [_p, _sz, _p, _p, _p, _i],
     "bipp_pipeline_images": [_p, _p, _i, _i],
     "bipp_pipeline_reset": [_p],
-    "bipp_pipeline_flush": [_p],
-    "bipp_pipeline_images_async": [_p, _p],
     "bipp_pipeline_last_eigenvalues": [_p, _p, _p],
     "bipp_pipeline_stage_times": [_p, _i, _p],
     "bipp_pipeline_kernel_times": [_p, _p],

@@ -721,16 +721,6 @@ class Pipeline:
     def reset(self):
         check(self.ctx._lib.bipp_pipeline_reset(self.handle))
 
-    def flush(self):
-        """Wait for the NUFFT work of the processed calls (bipp_pipeline_flush): batched
-        calls return while their NUFFT still runs on the pipeline's stream."""
-        check(self.ctx._lib.bipp_pipeline_flush(self.handle))
-
-    def images_async(self, ptr):
-        """Copy the accumulated, unnormalised images to ptr (device or pinned host memory)
-        after the last call's NUFFT, without waiting (complete after flush())."""
-        check(self.ctx._lib.bipp_pipeline_images_async(self.handle, C.c_void_p(ptr)))
-
     def last_eigenvalues(self, n_steps):
         d = np.zeros((n_steps, self.n_antenna), dtype=np.float64)
         nr = np.zeros(n_steps, dtype=np.int32)

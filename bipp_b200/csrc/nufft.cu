@@ -324,7 +324,7 @@ void NufftCore::exclusive_scan(const int* in, int* out, long long n) {
   B2_CHECK_LAUNCH();
 }
 
-void NufftCore::execute(float* image, long long ldImage, double* stageMs, int* errAsync) {
+void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   const long long P = num_pixels();
   const size_t planeBytes = (size_t)g_.nx * g_.ny * sizeof(float2);
   // slab size under a memory budget
@@ -514,10 +514,7 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs, int* e
                                                     dl_.get<double>(), dm_.get<double>(), su_, sv_, image, ldImage,
                                                     zeroAcc_.get<double>());
   B2_CHECK_LAUNCH();
-  if (tc && errAsync) {
-    // the caller reads the flag after the stream has passed this copy
-    B2_CUDA(cudaMemcpyAsync(errAsync, errFlag_.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx_->stream));
-  } else if (tc) {
+  if (tc) {
     int err = 0;
     d2h(ctx_, &err, errFlag_.get(), sizeof(int));
     sync(ctx_);

@@ -53,11 +53,7 @@ public:
   // per-channel accumulator of zero-baseline values (added to every pixel)
   double* zero_acc() { return zeroAcc_.get<double>(); }
   // spread/FFT/w-sum over all slabs and accumulate Re(...) into image[ch][P] (ld P)
-  // transform the collected points and add to image. The spreader's error flag is read
-  // back at once (host sync), or, with errAsync (pinned host memory), copied there on the
-  // stream for the caller to check once the stream has passed the copy.
-  void execute(float* image, long long ldImage, double* stageMs = nullptr, int* errAsync = nullptr);
-  cudaStream_t stream() const { return ctx_->stream; }
+  void execute(float* image, long long ldImage, double* stageMs = nullptr);
 
   const NufftGeom& geom() const { return g_; }
   // statistics of the last execute(): points spread, slabs (spreading launches), bytes of

@@ -126,25 +126,6 @@ struct bipp_pipeline_s {
   double tol = 1e-5;
   long long P = 0;
   std::vector<double> intervals;
-  // the NUFFT stream (U) of the pipeline: a context copy whose stream is U (the NUFFT's
-  // buffers are allocated and freed in U's order), the events between U and the context
-  // stream N, and the spreader's error flag copied back on U (pinned). Declared before
-  // `core`, so that it outlives the buffers that U frees.
-  struct NufftStream {
-    bipp_ctx_s nctx;
-    cudaEvent_t evPrep = nullptr, evVV = nullptr, evScatter = nullptr, evDone = nullptr;
-    bool scatterPending = false, donePending = false;
-    int* errHost = nullptr;
-    ~NufftStream() {
-      if (nctx.stream) {
-        cudaStreamSynchronize(nctx.stream);
-        cudaStreamDestroy(nctx.stream);
-      }
-      for (cudaEvent_t e : {evPrep, evVV, evScatter, evDone})
-        if (e) cudaEventDestroy(e);
-      if (errHost) cudaFreeHost(errHost);
-    }
-  } ns;
   NufftCore core;
   EigWork<float> eig;
   DevBuf basis, intervalsD;
@@ -202,49 +183,19 @@ static void pipeline_alloc(bipp_pipeline_s* p, size_t steps) {
   p->pairOff.alloc(ctx, (T + 1) * sizeof(long long));
 }
 
-// The work of a call runs on two streams. The context stream (N) takes the inputs, the
-// flag test and the eigensolve with levels and virtual visibilities; the pipeline's NUFFT
-// stream (U) takes the point count, the scatter of the points and the NUFFT itself. U waits
-// for N's results through events (evPrep, evVV); before N overwrites what U's scatter still
-// reads (the step tables, the virtual visibilities) it waits for U's scatter (evScatter).
-// The NUFFT of a call is thus left running on U when the call returns, and the next call's
-// eigensolve runs beside it; pipeline_join() brings U's work into N (images, reset, timing).
-
-// N waits until U's last scatter has read the step tables and virtual visibilities
-static void wait_scatter(bipp_pipeline_s* p) {
-  if (p->ns.scatterPending) {
-    B2_CUDA(cudaStreamWaitEvent(p->ctx->stream, p->ns.evScatter, 0));
-    p->ns.scatterPending = false;
-  }
-}
-
-// U's work joined into N; a spreader error of an earlier call is reported here
-static void pipeline_join(bipp_pipeline_s* p) {
-  if (!p->ns.donePending) return;
-  B2_CUDA(cudaStreamWaitEvent(p->ctx->stream, p->ns.evDone, 0));
-  B2_CUDA(cudaEventSynchronize(p->ns.evDone));
-  p->ns.donePending = false;
-  if (*p->ns.errHost) {
-    *p->ns.errHost = 0;
-    throw Error(BIPP_GPU_ERROR, "tensor-core spreading: MMA completion wait timed out");
-  }
-}
-
-// eigensolve + levels + VV of steps [s0, s0 + nb) on N (VV of every level when the
-// transform takes all levels, else of the levels [levelOffset, levelOffset +
-// levelsInTransform) are scattered later from the same VV)
-static void pipeline_chunk_eig(bipp_pipeline_s* p, int s0, int nb, double* ms) {
+// eigensolve + levels + VV for steps [s0, s0+nb) of the call, then scatter their points.
+static void pipeline_chunk(bipp_pipeline_s* p, int s0, int nb, const std::vector<long long>& pairOffH,
+                           int levelsInTransform, int levelOffset, bool scatterOnly, double* ms) {
   bipp_ctx_s* ctx = p->ctx;
   const int N = (int)p->nAnt, L = (int)p->nLevels;
   const long long n2 = (long long)N * N;
-  wait_scatter(p);   // the VV buffer and step tables are no longer read by U
   cudaEvent_t e0, e1, e2;
   if (ms) {
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     cudaEventRecord(e0, ctx->stream);
   }
   float2* X = p->eig.X(true);
-  {
+  if (!scatterOnly) {
     EigLaunch<float> E{};
     E.nBatch = nb; E.nBeam = N; E.nAnt = N; E.Nmax = N;
     E.S = p->Sin + (long long)s0 * n2; E.sStride = n2; E.lds = N;
@@ -311,42 +262,18 @@ static void pipeline_chunk_eig(bipp_pipeline_s* p, int s0, int nb, double* ms) {
     }
     B2_CHECK_LAUNCH();
   }
-  B2_CUDA(cudaEventRecord(p->ns.evVV, ctx->stream));
-  if (ms) {
-    cudaEventRecord(e2, ctx->stream);
-    cudaEventSynchronize(e2);
-    float a = 0, b = 0;
-    cudaEventElapsedTime(&a, e0, e1);
-    cudaEventElapsedTime(&b, e1, e2);
-    ms[0] += a;
-    ms[1] += b;
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
-  }
-}
-
-// zero-baseline traces and scatter of the points of steps [s0, s0 + nb) on U, after N's VV
-static void pipeline_chunk_scatter(bipp_pipeline_s* p, int s0, int nb, const std::vector<long long>& pairOffH,
-                                   int levelsInTransform, int levelOffset, double* ms) {
-  const int N = (int)p->nAnt, L = (int)p->nLevels;
-  const long long n2 = (long long)N * N;
-  bipp_ctx_s* nctx = &p->ns.nctx;
-  cudaStream_t u = nctx->stream;
-  B2_CUDA(cudaStreamWaitEvent(u, p->ns.evVV, 0));
-  cudaEvent_t e2, e3;
-  if (ms) {
-    cudaEventCreate(&e2); cudaEventCreate(&e3);
-    cudaEventRecord(e2, u);
-  }
   // zero baselines (r == s) of the levels in this transform
   count_launch();
-  vv_trace_kernel<<<nb * levelsInTransform, 128, 0, u>>>(
+  vv_trace_kernel<<<nb * levelsInTransform, 128, 0, ctx->stream>>>(
       nb, levelsInTransform, p->nred.get<int>() + s0, p->vv.get<float2>() + (long long)levelOffset * n2, n2 * L, n2, N,
       p->core.zero_acc());
   B2_CHECK_LAUNCH();
+  if (ms) cudaEventRecord(e2, ctx->stream);
+  // scatter points of these steps
   std::vector<long long> rel(nb + 1);
   for (int i = 0; i <= nb; ++i) rel[i] = pairOffH[s0 + i] - pairOffH[s0];
-  DevBuf relD(nctx, (nb + 1) * sizeof(long long));
-  h2d(nctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
+  DevBuf relD(ctx, (nb + 1) * sizeof(long long));
+  h2d(ctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
   PipelinePoints pp{};
   pp.nSteps = nb;
   pp.nred = p->nred.get<int>() + s0;
@@ -363,33 +290,36 @@ static void pipeline_chunk_scatter(bipp_pipeline_s* p, int s0, int nb, const std
   if (total > 0) {
     const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
     count_launch();
-    pipeline_scatter_kernel<<<gb, 256, 0, u>>>(p->core.geom(), pp, total, p->core.cursor(), relD.get<long long>(),
-                                               p->core.records(), p->core.values(), p->core.value_stride(),
-                                               p->core.sincos64() ? 1 : 0, p->core.channels());
+    pipeline_scatter_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.cursor(), relD.get<long long>(),
+                                                         p->core.records(), p->core.values(), p->core.value_stride(),
+                                                         p->core.sincos64() ? 1 : 0, p->core.channels());
     B2_CHECK_LAUNCH();
   }
-  B2_CUDA(cudaEventRecord(p->ns.evScatter, u));
-  p->ns.scatterPending = true;
   if (ms) {
-    cudaEventRecord(e3, u);
+    cudaEvent_t e3;
+    cudaEventCreate(&e3);
+    cudaEventRecord(e3, ctx->stream);
     cudaEventSynchronize(e3);
-    float c = 0;
+    float a = 0, b = 0, c = 0;
+    if (!scatterOnly) {
+      cudaEventElapsedTime(&a, e0, e1);
+      cudaEventElapsedTime(&b, e1, e2);
+    }
     cudaEventElapsedTime(&c, e2, e3);
+    ms[0] += a;
+    ms[1] += b;
     ms[2] += c;
-    cudaEventDestroy(e2); cudaEventDestroy(e3);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
   }
 }
 
-// point count of steps [s0, s0 + nb) on U, after N's flag test and uvw (evPrep)
 static void pipeline_count(bipp_pipeline_s* p, int s0, int nb, const std::vector<long long>& pairOffH) {
-  bipp_ctx_s* nctx = &p->ns.nctx;
-  cudaStream_t u = nctx->stream;
-  B2_CUDA(cudaStreamWaitEvent(u, p->ns.evPrep, 0));
+  bipp_ctx_s* ctx = p->ctx;
   const int N = (int)p->nAnt;
   std::vector<long long> rel(nb + 1);
   for (int i = 0; i <= nb; ++i) rel[i] = pairOffH[s0 + i] - pairOffH[s0];
-  DevBuf relD(nctx, (nb + 1) * sizeof(long long));
-  h2d(nctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
+  DevBuf relD(ctx, (nb + 1) * sizeof(long long));
+  h2d(ctx, relD.get(), rel.data(), rel.size() * sizeof(long long));
   PipelinePoints pp{};
   pp.nSteps = nb;
   pp.nred = p->nred.get<int>() + s0;
@@ -402,9 +332,10 @@ static void pipeline_count(bipp_pipeline_s* p, int s0, int nb, const std::vector
   if (total > 0) {
     const int gb = (int)std::min<long long>((total + 255) / 256, 16384);
     count_launch();
-    pipeline_count_kernel<<<gb, 256, 0, u>>>(p->core.geom(), pp, total, p->core.counts(), relD.get<long long>());
+    pipeline_count_kernel<<<gb, 256, 0, ctx->stream>>>(p->core.geom(), pp, total, p->core.counts(), relD.get<long long>());
     B2_CHECK_LAUNCH();
   }
+  sync(ctx);
 }
 
 // Host visibilities to the device: only the lower triangle of each S is read, so it is
@@ -444,11 +375,6 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
   bipp_ctx_s* ctx = p->ctx;
   require(nSteps > 0, "no steps");
   require(s && xyz && wl, "null pointer", BIPP_INVALID_POINTER_ERROR);
-  // stage times are of this call alone: the previous call's NUFFT completes first
-  if (p->timing) pipeline_join(p);
-  // the step tables (idx, nred, antUVW, ...) are rewritten or reallocated below: U's last
-  // scatter read them
-  wait_scatter(p);
   pipeline_alloc(p, nSteps);
   const int N = (int)p->nAnt, L = (int)p->nLevels;
   const long long n2 = (long long)N * N;
@@ -485,7 +411,6 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
                                               nullptr, nullptr, p->status.get<int>(), 1, 0, 0);
     B2_CHECK_LAUNCH();
   }
-  B2_CUDA(cudaEventRecord(p->ns.evPrep, ctx->stream));   // step tables ready for U's count
   std::vector<int> nredH(T);
   std::vector<double> wr(T);
   d2h(ctx, nredH.data(), p->nred.get(), T * sizeof(int));
@@ -511,45 +436,25 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
 
   if (p->mode == 0) {
     // batched: one NUFFT over all steps of the call, all levels as channels
-    if (T <= chunk) {
-      // the eigensolve is queued on N first, so that it runs beside the previous call's
-      // NUFFT, which U still holds (U's count waits for it)
-      pipeline_chunk_eig(p, 0, T, ms);
-      p->core.begin(0.0, Xw);  // points are folded to w >= 0 (real image)
-      pipeline_count(p, 0, T, pairOff);
-      p->core.end_count(pairOff[T]);
-      pipeline_chunk_scatter(p, 0, T, pairOff, L, 0, ms);
-    } else {
-      p->core.begin(0.0, Xw);
-      for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
-      p->core.end_count(pairOff[T]);
-      for (int s0 = 0; s0 < T; s0 += chunk) {
-        pipeline_chunk_eig(p, s0, std::min(chunk, T - s0), ms);
-        pipeline_chunk_scatter(p, s0, std::min(chunk, T - s0), pairOff, L, 0, ms);
-      }
-    }
+    p->core.begin(0.0, Xw);  // points are folded to w >= 0 (real image)
+    for (int s0 = 0; s0 < T; s0 += chunk) pipeline_count(p, s0, std::min(chunk, T - s0), pairOff);
+    p->core.end_count(pairOff[T]);
+    for (int s0 = 0; s0 < T; s0 += chunk) pipeline_chunk(p, s0, std::min(chunk, T - s0), pairOff, L, 0, false, ms);
     check_steps(p, 0, T);
     double nm[4] = {0, 0, 0, 0};
-    // the NUFFT is left running on U (its error flag is checked at the next join), unless
-    // this call is timed stage by stage
-    p->core.execute(p->images.get<float>(), p->P, p->timing ? nm : nullptr, p->timing ? nullptr : p->ns.errHost);
-    if (!p->timing) {
-      B2_CUDA(cudaEventRecord(p->ns.evDone, p->core.stream()));
-      p->ns.donePending = true;
-    }
+    p->core.execute(p->images.get<float>(), p->P, p->timing ? nm : nullptr);
     p->stageMs[3] += nm[0];
     p->stageMs[4] += nm[1];
     p->stageMs[5] += nm[2];
     p->stageMs[6] += nm[3];
   } else {
-    // plain: one step at a time, one NUFFT per step and level (each checked at once)
+    // plain: one step at a time, one NUFFT per step and level
     for (int b = 0; b < T; ++b) {
       for (int l = 0; l < L; ++l) {
-        if (l == 0) pipeline_chunk_eig(p, b, 1, ms);
         p->core.begin(0.0, wr[b]);
         pipeline_count(p, b, 1, pairOff);
         p->core.end_count(pairOff[b + 1] - pairOff[b]);
-        pipeline_chunk_scatter(p, b, 1, pairOff, 1, l, ms);
+        pipeline_chunk(p, b, 1, pairOff, 1, l, l > 0, ms);
         if (l == 0) check_steps(p, b, 1);
         double nm[4] = {0, 0, 0, 0};
         p->core.execute(p->images.get<float>() + (long long)l * p->P, p->P, p->timing ? nm : nullptr);
@@ -559,12 +464,11 @@ static void pipeline_process(bipp_pipeline_s* p, size_t nSteps, const void* s, c
         p->stageMs[6] += nm[3];
       }
     }
-    B2_CUDA(cudaEventRecord(p->ns.evDone, p->core.stream()));
-    p->ns.donePending = true;
   }
   // keep eigenvalues of this call for calibration (host copy on demand)
   p->lastNred = nredH;
   p->stepsDone += T;
+  sync(ctx);
 }
 
 extern "C" {
@@ -599,22 +503,7 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
     lat.Am = cfg->lattice[4]; lat.Bm = cfg->lattice[5];
     p->P = (long long)cfg->gridA * cfg->gridB;
     std::vector<double> n(cfg->pixelN, cfg->pixelN + p->P);
-    {
-      auto& ns = p->ns;
-      ns.nctx.device = ctx->device;
-      ns.nctx.prop = ctx->prop;
-      ns.nctx.smCount = ctx->smCount;
-      ns.nctx.maxSmemOptin = ctx->maxSmemOptin;
-      B2_CUDA(cudaStreamCreateWithFlags(&ns.nctx.stream, cudaStreamNonBlocking));
-      for (cudaEvent_t* e : {&ns.evPrep, &ns.evVV, &ns.evScatter, &ns.evDone})
-        B2_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-      B2_CUDA(cudaMallocHost(&ns.errHost, sizeof(int)));
-      *ns.errHost = 0;
-      // U starts after what the context stream holds so far
-      B2_CUDA(cudaEventRecord(ns.evPrep, ctx->stream));
-      B2_CUDA(cudaStreamWaitEvent(ns.nctx.stream, ns.evPrep, 0));
-    }
-    p->core.setup(&p->ns.nctx, lat, n, p->tol, p->mode == 0 ? (int)cfg->nLevels : 1);
+    p->core.setup(ctx, lat, n, p->tol, p->mode == 0 ? (int)cfg->nLevels : 1);
     p->basis.alloc(ctx, 9 * sizeof(double));
     h2d(ctx, p->basis.get(), cfg->uvwBasis, 9 * sizeof(double));
     p->intervalsD.alloc(ctx, p->intervals.size() * sizeof(double));
@@ -623,7 +512,6 @@ BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg, 
     p->images.zero();
     if (cfg->maxSteps) pipeline_alloc(p.get(), cfg->maxSteps);
     sync(ctx);
-    sync(&p->ns.nctx);
     ctx_retain(ctx);
     *out = p.release();
   });
@@ -695,7 +583,6 @@ BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize,
   return guard([&] {
     require(pl && images, "null pointer", BIPP_INVALID_POINTER_ERROR);
     bipp_ctx_s* ctx = pl->ctx;
-    pipeline_join(pl);
     const long long n = (long long)pl->nLevels * pl->P;
     const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     B2_CUDA(cudaMemcpyAsync(images, pl->images.get(), n * sizeof(float), kind, ctx->stream));
@@ -722,7 +609,6 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
     require(repeats >= 1 && repeats <= 100, "repeats must be in [1, 100]");
     bipp_ctx_s* ctx = pl->ctx;
-    pipeline_join(pl);
     // the caller's images, step count and timers are kept aside and restored afterwards
     const size_t imgBytes = (size_t)pl->nLevels * pl->P * sizeof(float);
     DevBuf saved(ctx, imgBytes);
@@ -757,7 +643,6 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
       for (int r = 0; r < 2; ++r) {
         B2_CUDA(cudaEventRecord(a, ctx->stream));
         pipeline_process(pl, nSteps, s, xyz, wl, onDevice);
-        pipeline_join(pl);
         B2_CUDA(cudaEventRecord(b, ctx->stream));
         B2_CUDA(cudaEventSynchronize(b));
         float t = 0.f;
@@ -828,10 +713,6 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     };
     // the caller's state comes back on every exit path
     auto restore = [&] {
-      try {
-        pipeline_join(pl);
-      } catch (const Error&) {
-      }
       cudaMemcpyAsync(pl->images.get(), saved.get(), imgBytes, cudaMemcpyDeviceToDevice, ctx->stream);
       pl->stepsDone = stepsDone;
       std::copy(stage, stage + 7, pl->stageMs);
@@ -858,27 +739,11 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
 BippError bipp_pipeline_reset(bipp_pipeline_t pl) {
   return guard([&] {
     require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
-    pipeline_join(pl);
     pl->images.zero();
     pl->stepsDone = 0;
     for (double& x : pl->stageMs) x = 0;
     for (double& x : pl->eigMs) x = 0;
     sync(pl->ctx);
-  });
-}
-
-BippError bipp_pipeline_images_async(bipp_pipeline_t pl, float* images) {
-  return guard([&] {
-    require(pl && images, "null pointer", BIPP_INVALID_POINTER_ERROR);
-    const long long n = (long long)pl->nLevels * pl->P;
-    B2_CUDA(cudaMemcpyAsync(images, pl->images.get(), n * sizeof(float), cudaMemcpyDefault, pl->core.stream()));
-  });
-}
-
-BippError bipp_pipeline_flush(bipp_pipeline_t pl) {
-  return guard([&] {
-    require(pl != nullptr, "null pipeline", BIPP_INVALID_HANDLE_ERROR);
-    pipeline_join(pl);
   });
 }
 
@@ -931,11 +796,6 @@ BippError bipp_pipeline_destroy(bipp_pipeline_t pl) {
   return guard([&] {
     if (!pl) return;
     bipp_ctx_s* ctx = pl->ctx;
-    try {
-      pipeline_join(pl);
-    } catch (const Error&) {
-      // a spreader error of the last call: the pipeline goes away all the same
-    }
     delete pl;
     sync(ctx);
     ctx_release(ctx);

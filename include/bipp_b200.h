@@ -318,12 +318,7 @@ typedef struct {
 BIPP_B200_EXPORT BippError bipp_pipeline_create(bipp_ctx_t ctx, const bipp_pipeline_config* cfg,
                                                 bipp_pipeline_t* pipeline);
 /* Process nSteps time steps: s [nSteps][nAntenna x nAntenna] complex float (lower triangle
- * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. In batched mode the
- * call returns while its NUFFT still runs on the pipeline's own stream, so that the next
- * call's eigensolve runs beside it; the images are complete on the context stream after
- * bipp_pipeline_flush, and bipp_pipeline_images / _reset / _autotune_pipeline / _destroy
- * flush first. A spreader error (BIPP_GPU_ERROR) of such a NUFFT is reported by the next
- * flush. onDevice != 0: the
+ * used), xyz [nSteps][nAntenna][3] FP64 positions, wl [nSteps] FP64. onDevice != 0: the
  * three pointers are device pointers (s is read in place, not modified), else host
  * pointers (copied in by the call; of s only the lower triangle is copied, in blocks of
  * 64 columns from each block's diagonal row down). The steps' contributions are
@@ -348,14 +343,6 @@ BIPP_B200_EXPORT BippError bipp_pipeline_process_staged(bipp_pipeline_t pl);
  * to host (onDevice == 0) or device memory. */
 BIPP_B200_EXPORT BippError bipp_pipeline_images(bipp_pipeline_t pl, float* images, int normalize, int onDevice);
 BIPP_B200_EXPORT BippError bipp_pipeline_reset(bipp_pipeline_t pl);
-/* Wait until the NUFFT work of the processed calls is complete: the context stream waits
- * for it and the host too (the spreader's error flag is read). No counterpart in the
- * reference, whose calls are synchronous. */
-BIPP_B200_EXPORT BippError bipp_pipeline_flush(bipp_pipeline_t pl);
-/* Copy the accumulated images [nLevels][nPixel] (not normalised) into `images` (device, or
- * pinned host memory) after the NUFFT of the last processed call, and return at once; the
- * copy is complete after bipp_pipeline_flush. */
-BIPP_B200_EXPORT BippError bipp_pipeline_images_async(bipp_pipeline_t pl, float* images);
 /* Eigenvalues [maxSteps][nAntenna] and nBeamReduced of the last process() call (host).
  * Only the eigenvalues inside [min lo, max hi] of the energy levels are computed by the
  * pipeline (the others do not enter the images); the other entries are zero. */

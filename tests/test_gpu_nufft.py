@@ -323,40 +323,6 @@ def test_pipeline_plain_matches_batched(ctx):
     assert _rel_l2(imgs[1], imgs[0].astype(np.float64)) <= 1e-4
 
 
-def test_pipeline_calls_overlap_like_serial_calls(ctx):
-    """Batched calls return while their NUFFT runs on the pipeline's stream and the next
-    call's eigensolve runs beside it: four calls back to back (then flush) give the images
-    of four calls each flushed at once, and the asynchronous image copy after the last
-    call equals the images read after flush. Calls of 16 steps, multi-chunk (chunk 8)
-    and single-chunk, with the tensor-core spreader."""
-    import torch
-
-    import bipp_b200 as bipp
-
-    cfg, obs, s, xyz = _pipeline_case(n_ant=48, n_steps=16, image=48)
-    intervals = np.array([[0.0, 1.0], [1.0, np.inf]])
-    n = cfg.image_size
-    wl = np.full(s.shape[0], cfg.wl)
-    for chunk in (16, 8):
-        imgs = []
-        for flush_each in (True, False):
-            pl = bipp.Pipeline(ctx, cfg.n_antenna, intervals, _lattice(obs, n), obs.lmn[:, 2], obs.basis,
-                               tolerance=1e-6, chunk_steps=chunk)
-            for _ in range(4):
-                pl.process(s, xyz, wl)
-                if flush_each:
-                    pl.flush()
-            if not flush_each:
-                host = torch.empty(2 * n * n, dtype=torch.float32).pin_memory()
-                pl.images_async(host.data_ptr())
-                pl.flush()
-                async_img = host.numpy().reshape(2, n * n).astype(np.float64)
-            imgs.append(pl.images(normalize=False).astype(np.float64))
-            pl.close()
-        assert _rel_l2(imgs[1], imgs[0]) <= 1e-6, chunk
-        assert _rel_l2(async_img, imgs[1]) == 0.0
-
-
 def test_pipeline_accumulates_over_calls(ctx):
     """Splitting the steps over two process() calls gives the same normalised image
     (linearity of the synthesis in the steps)."""
