@@ -166,9 +166,11 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   g_ = NufftGeom{};
   g_.l0 = lat.l0; g_.m0 = lat.m0; g_.Al = lat.Al; g_.Bl = lat.Bl; g_.Am = lat.Am; g_.Bm = lat.Bm;
   g_.Na = lat.Na; g_.Nb = lat.Nb;
-  // oversampling 1.75: the same kernel width as 2 at the tolerances of interest
-  // (W = 6 at 1e-5) on (7/8)^3 of the fine grid
-  const double sigma = kNufftSigma;
+  // oversampling (tunable, fine cells per 1024 pixels along a lattice axis; the w axis
+  // takes the same factor): 1792 / 1024 = 1.75 gives the same kernel width as 2 at the
+  // tolerances of interest (W = 6 at 1e-5) on (7/8)^3 of the fine grid; 1728 and 1680 keep
+  // W = 6 at 1e-5 on smaller grids, with less margin in the width rule
+  const double sigma = tuned("nufft.grid_per_1024") / 1024.0;
   es_params(eps, sigma, g_.W, g_.beta);
   g_.nx = next_smooth((int)std::ceil(sigma * g_.Nb));
   g_.ny = next_smooth((int)std::ceil(sigma * g_.Na));

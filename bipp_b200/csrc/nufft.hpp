@@ -25,7 +25,7 @@ Lattice fit_lattice(const std::vector<double>& l, const std::vector<double>& m);
 
 // ES kernel width and shape for a tolerance at upsampling factor 2 (as used by type-1/3
 // NUFFTs with the "exponential of semicircle" kernel).
-constexpr double kNufftSigma = 1.75;   // fine-grid oversampling in x, y and w
+// fine-grid oversampling in x, y and w: the tuning table's nufft.grid_per_1024 / 1024
 constexpr int kMaxPipelineLevels = 8;  // energy levels of one pipeline (NUFFT channels)
 void es_params(double eps, double sigma, int& W, float& beta);
 

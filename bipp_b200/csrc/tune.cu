@@ -61,6 +61,10 @@ std::vector<Param>& table() {
        0},
       {"vv.ctas_per_sm", 3, {1, 2, 3}, "persistent tensor-core virtual-visibility CTAs per SM", 0},
       {"direct.ctas_per_sm", 4, {2, 4, 8}, "direct-sum CTAs per SM below which the inputs are split", 0},
+      {"nufft.grid_per_1024", 1792, {1680, 1728, 1792},
+       "NUFFT fine-grid cells per 1024 pixels (oversampling x 1024; read when a NUFFT is set up; not autotuned, "
+       "as it trades accuracy for speed)",
+       0},
   };
   static bool init = false;
   if (!init) {
