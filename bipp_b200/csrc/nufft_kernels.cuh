@@ -196,100 +196,52 @@ static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long
   }
 }
 
-// pass 2: scatter records + values ([point][channel]). A thread takes kScatterIlp points
-// at a time, stage by stage (step search, pair, antenna loads, coordinates, key and
-// phase for all of them, then their cursor atomics, then their records and values), so
-// that the memory round trips of the points overlap instead of queueing one behind the
-// other (the kernel is bound by the latency of its atomics and dependent loads).
-constexpr int kScatterIlp = 4;
-static __global__ void __launch_bounds__(256, 3) pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
+// pass 2: scatter records + values (channel-major: vals[ch][sortedIndex])
+static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
                                         const long long* __restrict__ chunkPairOffset, PtRec* __restrict__ rec,
                                         float2* __restrict__ vals, long long valStride, int sincos64, int nchAll) {
-  constexpr int K = kScatterIlp;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; t0 < total; t0 += K * stride) {
-    long long t[K];
-    int lo[K], hi[K];
-    bool ok[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      t[i] = t0 + i * stride;
-      ok[i] = t[i] < total;
-      lo[i] = 0;
-      hi[i] = P.nSteps;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = P.nSteps;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (chunkPairOffset[mid] <= t) lo = mid; else hi = mid;
     }
-    // step of each point: bisection over the chunk's pair offsets (same number of rounds
-    // for every point)
-    for (int span = P.nSteps; span > 1; span = (span + 1) >> 1) {
-#pragma unroll
-      for (int i = 0; i < K; ++i) {
-        if (hi[i] - lo[i] > 1) {
-          const int mid = (lo[i] + hi[i]) >> 1;
-          if (chunkPairOffset[mid] <= (ok[i] ? t[i] : 0)) lo[i] = mid; else hi[i] = mid;
-        }
-      }
-    }
-    int st[K], r[K], sc[K], ar[K], as[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      st[i] = lo[i];
-      r[i] = sc[i] = 0;
-      if (ok[i]) {
-        pair_from_linear(t[i] - chunkPairOffset[st[i]], P.nred[st[i]], r[i], sc[i]);
-        ok[i] = r[i] != sc[i];   // zero baseline: added analytically (Re of the trace of VV)
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      ar[i] = ok[i] ? P.idx[(long long)st[i] * P.Nmax + r[i]] : 0;
-      as[i] = ok[i] ? P.idx[(long long)st[i] * P.Nmax + sc[i]] : 0;
-    }
-    PtCoord c[K];
-    int key[K];
-    float sn[K], cs[K];
-    bool flip[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      key[i] = 0;
-      flip[i] = false;
-      sn[i] = 0.f;
-      cs[i] = 1.f;
-      if (!ok[i]) continue;
-      const double* U = P.antUVW + (long long)st[i] * P.nAnt * 3;
-      const double scl = P.uvwScale[st[i]];
-      double u = (U[ar[i] * 3 + 0] - U[as[i] * 3 + 0]) * scl;
-      double v = (U[ar[i] * 3 + 1] - U[as[i] * 3 + 1]) * scl;
-      double w = (U[ar[i] * 3 + 2] - U[as[i] * 3 + 2]) * scl;
-      // only the real part of the image is kept, and a point and its mirror (-u, -v, -w,
-      // conjugate value) have the same real part: every point is taken with w >= 0, so the
-      // w-grid spans [0, max w] instead of [-max w, max w]
-      flip[i] = w < 0.0;
-      if (flip[i]) { u = -u; v = -v; w = -w; }
-      c[i] = point_coord(g, u, v, w);
-      key[i] = tile_key(g, c[i]);
-      const double ph = point_phase(g, u, v, w);
-      if (sincos64) { double s64, c64; sincos(ph, &s64, &c64); sn[i] = (float)s64; cs[i] = (float)c64; }
-      else sincosf((float)ph, &sn[i], &cs[i]);
-    }
-    int pos[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) pos[i] = ok[i] ? atomicAdd(cursor + key[i], 1) : -1;
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      if (pos[i] < 0 || pos[i] >= valStride) continue;  // invalid point (keys of both passes agree)
-      PtRec pr;
-      pr.ix0 = c[i].ix0; pr.iy0 = c[i].iy0; pr.iw0 = c[i].iw0;
-      pr.dx = c[i].dx; pr.dy = c[i].dy; pr.dw = c[i].dw;
-      pr.pad0 = 0; pr.pad1 = 0;
-      rec[pos[i]] = pr;
-      const float wgt = 2.0f;   // lower triangle (r > s) stands for (r,s) and (s,r)
-      const float2* vvb = P.vv + (long long)st[i] * P.vvStepStride + r[i] + (long long)sc[i] * P.Nmax;
-      for (int l = 0; l < P.levels; ++l) {
-        float2 a = vvb[(long long)l * P.vvLevelStride];
-        if (flip[i]) a.y = -a.y;
-        vals[(long long)pos[i] * nchAll + l] =
-            make_float2(wgt * (a.x * cs[i] - a.y * sn[i]), wgt * (a.x * sn[i] + a.y * cs[i]));
-      }
+    const int st = lo;
+    const int n = P.nred[st];
+    int r, s;
+    pair_from_linear(t - chunkPairOffset[st], n, r, s);
+    if (r == s) continue;  // zero baseline: added analytically (Re of the trace of VV)
+    const int ar = P.idx[(long long)st * P.Nmax + r], as = P.idx[(long long)st * P.Nmax + s];
+    const double* U = P.antUVW + (long long)st * P.nAnt * 3;
+    const double sc = P.uvwScale[st];
+    double u = (U[ar * 3 + 0] - U[as * 3 + 0]) * sc;
+    double v = (U[ar * 3 + 1] - U[as * 3 + 1]) * sc;
+    double w = (U[ar * 3 + 2] - U[as * 3 + 2]) * sc;
+    // only the real part of the image is kept, and a point and its mirror (-u, -v, -w,
+    // conjugate value) have the same real part: every point is taken with w >= 0, so the
+    // w-grid spans [0, max w] instead of [-max w, max w]
+    const bool flip = w < 0.0;
+    if (flip) { u = -u; v = -v; w = -w; }
+    const PtCoord c = point_coord(g, u, v, w);
+    const int key = tile_key(g, c);
+    const int pos = atomicAdd(cursor + key, 1);
+    if (pos < 0 || pos >= valStride) continue;  // keys of both passes agree; never taken
+    PtRec pr;
+    pr.ix0 = c.ix0; pr.iy0 = c.iy0; pr.iw0 = c.iw0;
+    pr.dx = c.dx; pr.dy = c.dy; pr.dw = c.dw;
+    pr.pad0 = 0; pr.pad1 = 0;
+    rec[pos] = pr;
+    const double ph = point_phase(g, u, v, w);
+    float sn, cs;
+    if (sincos64) { double s64, c64; sincos(ph, &s64, &c64); sn = (float)s64; cs = (float)c64; }
+    else sincosf((float)ph, &sn, &cs);
+    const float wgt = (r == s) ? 1.0f : 2.0f;   // lower triangle stands for (r,s) and (s,r)
+    const float2* vvb = P.vv + (long long)st * P.vvStepStride + r + (long long)s * P.Nmax;
+    for (int l = 0; l < P.levels; ++l) {
+      float2 a = vvb[(long long)l * P.vvLevelStride];
+      if (flip) a.y = -a.y;
+      vals[(long long)pos * nchAll + l] = make_float2(wgt * (a.x * cs - a.y * sn), wgt * (a.x * sn + a.y * cs));
     }
   }
 }
