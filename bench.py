@@ -582,11 +582,16 @@ def main():
 
         stride = max(1, T // args.check_steps)
         sel = torch.arange(0, T, stride, device=device)[:args.check_steps]
-        parity = verify.check_batch(ctx, S[sel].contiguous(), xyz[sel].contiguous(), wl[sel].contiguous(), obs, n,
-                                    intervals, cfg.eps, n_pix=args.check_pixels,
-                                    chunk_steps=min(args.chunk_steps, len(sel)), vv_precision=args.vv_precision)
-        parity["reference"] = ("FP64: bipp_eigh_gram_batched_d + FP64 V diag(d) V^H + direct sum with FP64 phase "
-                               "and trigonometry (the library's FP64 pieces pinned to the compiled reference)")
+        try:
+            parity = verify.check_batch(ctx, S[sel].contiguous(), xyz[sel].contiguous(), wl[sel].contiguous(), obs,
+                                        n, intervals, cfg.eps, n_pix=args.check_pixels,
+                                        chunk_steps=min(args.chunk_steps, len(sel)), vv_precision=args.vv_precision)
+            parity["reference"] = ("FP64: bipp_eigh_gram_batched_d + FP64 V diag(d) V^H + direct sum with FP64 "
+                                   "phase and trigonometry (the library's FP64 pieces pinned to the compiled "
+                                   "reference)")
+        except bipp.GPUError as err:
+            # a second pipeline beside the benchmark's (larger workloads): reported, not fatal
+            parity = {"skipped": str(err)[:200], "hint": "lower --check-steps"}
 
     # the plain GPU form of the metric on a bounded sample: the same kernels, one step at a
     # time and one NUFFT per step and level (no batching across steps or levels)
