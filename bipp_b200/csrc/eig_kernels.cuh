@@ -1314,50 +1314,16 @@ tridiag_kernel(const double* __restrict__ dIn, const double* __restrict__ eIn, c
     for (int i = threadIdx.x; i < n; i += blockDim.x)
       if (i < vLo || i >= vHi) lam[i] = 0.0;
   }
-  // multisection for each eigenvalue index: a group of G lanes (1, 2 or 4: as many as the
-  // CTA has lanes for the range, so that the idle lanes of a small range work too) takes
-  // one eigenvalue and evaluates the Sturm counts at G x 2 interior points of its interval
-  // per round (two independent counts per lane), which keeps the subinterval holding the
-  // eigenvalue: log2(2 G + 1) bits per round instead of one. The same stopping rule as a
-  // bisection; the eigenvalue is the midpoint of the final interval.
-  {
-    const int cnt = vHi - vLo;
-    const int G = (cnt * 4 <= (int)blockDim.x) ? 4 : (cnt * 2 <= (int)blockDim.x) ? 2 : 1;
-    constexpr int PPL = 2;   // points per lane
-    const int lane = threadIdx.x & 31;
-    const int gl = lane % G;                                       // lane within the group
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane - gl);
-    const int M = G * PPL;                                         // points per round
-    // the lanes of a group share i, so they run the same iterations (G divides 32)
-    for (int i = vLo + (int)threadIdx.x / G; i < vHi; i += (int)blockDim.x / G) {
-      double a = lo, c = hi;
-      for (int it = 0; it < 128; ++it) {
-        if (c - a <= fmax(2.0 * eps * fmax(fabs(a), fabs(c)), eps * tnorm) + pivmin) break;
-        const double h = (c - a) / (double)(M + 1);
-        double x[PPL];
-        int k[PPL];
-#pragma unroll
-        for (int q = 0; q < PPL; ++q) x[q] = a + h * (double)(gl * PPL + q + 1);
-#pragma unroll
-        for (int q = 0; q < PPL; ++q) k[q] = sturm_count(d, e2, n, x[q], pivmin);
-        // this lane's bounds: the largest point with count <= i, the smallest with count > i
-        double na = a, nc = c;
-#pragma unroll
-        for (int q = 0; q < PPL; ++q) {
-          if (x[q] > a && x[q] < c) {
-            if (k[q] > i) nc = fmin(nc, x[q]); else na = fmax(na, x[q]);
-          }
-        }
-        for (int o = 1; o < G; o <<= 1) {
-          na = fmax(na, __shfl_xor_sync(gmask, na, o));
-          nc = fmin(nc, __shfl_xor_sync(gmask, nc, o));
-        }
-        if (na <= a && nc >= c) break;   // no interior point representable
-        a = na;
-        c = nc;
-      }
-      if (gl == 0) lam[i] = 0.5 * (a + c);
+  // bisection for each eigenvalue index
+  for (int i = vLo + threadIdx.x; i < vHi; i += blockDim.x) {
+    double a = lo, c = hi;
+    for (int it = 0; it < 128; ++it) {
+      const double mid = 0.5 * (a + c);
+      if (mid <= a || mid >= c) break;
+      if (c - a <= fmax(2.0 * eps * fmax(fabs(a), fabs(c)), eps * tnorm) + pivmin) break;
+      if (sturm_count(d, e2, n, mid, pivmin) > i) c = mid; else a = mid;
     }
+    lam[i] = 0.5 * (a + c);
   }
   __syncthreads();
   if (predK && vLo > 0 && lam[vLo] >= vecLo) {
