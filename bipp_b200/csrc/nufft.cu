@@ -495,8 +495,9 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
     if (stageMs) B2_CUDA(cudaEventRecord(ev[2], ctx_->stream));
     const int blocks = (int)std::min<long long>((P + 255) / 256, 65535);
     count_launch();
-    wsum_kernel<<<blocks, 256, 0, ctx_->stream>>>(g_, grid_.get<float2>(), nch_, slabPlanes, tw0 * kTW,
-                                                  tiles * kTW, nTilde_.get<double>(), acc_.get<float2>(), P);
+    auto wk = nch_ <= 4 ? wsum_kernel<4> : wsum_kernel<kMaxChan>;
+    wk<<<blocks, 256, 0, ctx_->stream>>>(g_, grid_.get<float2>(), nch_, slabPlanes, tw0 * kTW, tiles * kTW,
+                                         nTilde_.get<double>(), acc_.get<float2>(), P);
     B2_CHECK_LAUNCH();
     if (stageMs) {
       B2_CUDA(cudaEventRecord(ev[3], ctx_->stream));

@@ -612,10 +612,16 @@ spread_warp_kernel(NufftGeom g, const int* __restrict__ offsets, const PtRec* __
 // ---------------------------------------------------------------------------------------
 // w-sum: acc[ch][p] += sum_{planes j of slab} F[ch][j][a'][b'] exp(i n~_p t_j)
 // ---------------------------------------------------------------------------------------
-static __global__ void wsum_kernel(NufftGeom g, const float2* __restrict__ F, int nch, int slabPlanes, int jFirst,
-                            int planesUsed, const double* __restrict__ nTilde /*[P]*/, float2* __restrict__ acc,
-                            long long accStride) {
+// CH: channels held in registers (4, or kMaxChan for more); with 4 channels the planes are
+// read 4 at a time (their 16 loads issued together), with more one at a time (registers),
+// while the FP64 phase recurrence runs in order
+template <int CH, int kWsumUnroll = (CH <= 4 ? 4 : 1)>
+static __global__ void __launch_bounds__(256) wsum_kernel(NufftGeom g, const float2* __restrict__ F, int nch,
+                                                           int slabPlanes, int jFirst, int planesUsed,
+                                                           const double* __restrict__ nTilde /*[P]*/,
+                                                           float2* __restrict__ acc, long long accStride) {
   const long long P = (long long)g.Na * g.Nb;
+  const long long planeStride = (long long)g.ny * g.nx;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
     const int a = (int)(p / g.Nb), b = (int)(p % g.Nb);
     int ap = a - g.Na / 2; if (ap < 0) ap += g.ny;
@@ -626,25 +632,34 @@ static __global__ void wsum_kernel(NufftGeom g, const float2* __restrict__ F, in
     sincos(nt * (double)(jFirst - g.jc) * g.hw, &s0, &c0);
     sincos(nt * g.hw, &sd, &cd);
     double er = c0, ei = s0;
-    float2 sum[kMaxChan];
+    float2 sum[CH];
 #pragma unroll
-    for (int c = 0; c < kMaxChan; ++c) sum[c] = make_float2(0.f, 0.f);
-    for (int j = 0; j < planesUsed; ++j) {
-      const float fr = (float)er, fi = (float)ei;
+    for (int c = 0; c < CH; ++c) sum[c] = make_float2(0.f, 0.f);
+    const float2* Fp = F + slab_index(g, nch, slabPlanes, 0, 0, ap, bp);   // channel 0, plane 0
+    for (int j0 = 0; j0 < planesUsed; j0 += kWsumUnroll) {
+      float2 f[kWsumUnroll][CH];
 #pragma unroll
-      for (int c = 0; c < kMaxChan; ++c) {
-        if (c < nch) {
-          const float2 f = F[slab_index(g, nch, slabPlanes, c, j, ap, bp)];
-          sum[c].x += f.x * fr - f.y * fi;
-          sum[c].y += f.x * fi + f.y * fr;
+      for (int u = 0; u < kWsumUnroll; ++u)
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+          f[u][c] = (c < nch && j0 + u < planesUsed)
+                        ? Fp[((long long)c * slabPlanes + (j0 + u)) * planeStride]
+                        : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < kWsumUnroll; ++u) {
+        const float fr = (float)er, fi = (float)ei;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+          sum[c].x += f[u][c].x * fr - f[u][c].y * fi;
+          sum[c].y += f[u][c].x * fi + f[u][c].y * fr;
         }
+        const double nr = er * cd - ei * sd;
+        ei = er * sd + ei * cd;
+        er = nr;
       }
-      const double nr = er * cd - ei * sd;
-      ei = er * sd + ei * cd;
-      er = nr;
     }
 #pragma unroll
-    for (int c = 0; c < kMaxChan; ++c) {
+    for (int c = 0; c < CH; ++c) {
       if (c < nch) {
         float2 o = acc[(long long)c * accStride + p];
         o.x += sum[c].x;
