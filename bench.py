@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--chunk-steps", type=int, default=None, help="entries per eigensolver/VV chunk")
     ap.add_argument("--vv-precision", default="tf32x3", choices=["tf32x3", "bf16x3", "fp32", "fp64"],
                     help="arithmetic of the virtual-visibility products of the batched form")
-    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default launch shapes instead of tuning them on the batch first")
     ap.add_argument("--no-e2e", action="store_true")
