@@ -203,7 +203,7 @@ __device__ __forceinline__ double e_div(double a, double d) { return a / d; }
 // memory (as the triangular inverse does per block), a register-tiled product that keeps
 // the kernel at three CTAs per SM in the real case.
 template <typename E>
-__global__ void __launch_bounds__(kCholThreads, sizeof(E) == 8 ? 3 : 1)
+__global__ void __launch_bounds__(kCholThreads, sizeof(E) == 8 ? 4 : 1)
 cholesky_kernel(E* __restrict__ G, const int* __restrict__ nred, int Nmax, int* __restrict__ status,
                 const int* __restrict__ order = nullptr) {
   const int b = order ? order[blockIdx.x] : blockIdx.x;
