@@ -165,7 +165,7 @@ static __device__ __noinline__ void pair_from_linear(long long t, int n, int& r,
 }
 
 // pass 1: keys of pipeline points -> counts
-static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ counts,
+static __global__ void __launch_bounds__(256, 8) pipeline_count_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ counts,
                                       const long long* __restrict__ chunkPairOffset) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -197,7 +197,7 @@ static __global__ void pipeline_count_kernel(NufftGeom g, PipelinePoints P, long
 }
 
 // pass 2: scatter records + values (channel-major: vals[ch][sortedIndex])
-static __global__ void __launch_bounds__(256, 8) pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
+static __global__ void pipeline_scatter_kernel(NufftGeom g, PipelinePoints P, long long total, int* __restrict__ cursor,
                                         const long long* __restrict__ chunkPairOffset, PtRec* __restrict__ rec,
                                         float2* __restrict__ vals, long long valStride, int sincos64, int nchAll) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
