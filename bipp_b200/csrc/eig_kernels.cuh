@@ -375,7 +375,7 @@ constexpr size_t trinv_smem() { return 3 * 32 * 33 * sizeof(E); }
 constexpr size_t kTrinvSmem = trinv_smem<double2>();
 
 template <typename E, typename O>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(E) == 8 ? 8 : 1)
 trinv_kernel(const E* __restrict__ L, E* __restrict__ W64, O* __restrict__ LinvOut, const int* __restrict__ nred,
              int Nmax, const int* __restrict__ order = nullptr) {
   constexpr int NB = 32;
