@@ -349,7 +349,12 @@ void eig_launch(bipp_ctx_s* ctx, const EigLaunch<T>& L, EigWork<T>& w) {
     auto k = tridiag_kernel<R>;
     smem_optin(k, smem);
     count_launch();
-    k<<<nb, kTriThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
+    // threads per matrix (tunable): by default 128 when only the eigenpairs of a range are
+    // computed (one lane per eigenvalue leaves most of 256 idle, and 128-thread CTAs put
+    // twice the matrices on an SM), 256 for every eigenpair
+    const int tt = tuned("tridiag.threads");
+    const int triThreads = tt > 0 ? tt : (L.allValues ? kTriThreads : kTriThreads / 2);
+    k<<<nb, triThreads, smem, st>>>(w.d.template get<double>(), w.e.template get<double>(), nred, Nmax,
                                      L.lam + (long long)L.batchOffset * Nmax, Z, reinterpret_cast<double*>(W64),
                                      L.status + L.batchOffset, L.vecLo, L.vecHi, krange, L.allValues, sizeOrder,
                                      L.mlpModel ? L.predK : nullptr, L.predMargin, L.resTol);

@@ -621,7 +621,7 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     pl->timing = false;
     std::string rep = "{";
     const char* params[] = {"spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-                            "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm"};
+                            "hetrd.threads", "hetrd.ctas_pct", "tridiag.threads", "vv.ctas_per_sm"};
     // Objective of a parameter: the device time of the stage it changes (CUDA events of
     // the pipeline's stage timers): spreading (with the tile clearing) for spread.*, the
     // tridiagonalisation kernel for hetrd.*, the virtual visibilities for vv.*. Every
@@ -631,6 +631,7 @@ BippError bipp_autotune_pipeline(bipp_pipeline_t pl, size_t nSteps, const void* 
     auto objective = [&](const char* name) {
       if (!std::strncmp(name, "spread.", 7)) return pl->stageMs[3] + pl->stageMs[6];
       if (!std::strncmp(name, "hetrd.", 6)) return pl->eigMs[4];
+      if (!std::strncmp(name, "tridiag.", 8)) return pl->eigMs[5];
       return pl->stageMs[1];
     };
     // the whole call with a set of values: the faster of two timed calls (CUDA events)

@@ -55,6 +55,8 @@ std::vector<Param>& table() {
       {"hetrd.threads", 0, {0, 256, 512, 1024}, "threads per matrix in the tridiagonalisation (0: by matrix size)", 0},
       {"hetrd.ctas_pct", 0, {0, 50, 75, 100, 150},
        "persistent tridiagonalisation CTAs in percent of the SM count (0: one CTA per matrix)", 0},
+      {"tridiag.threads", 0, {0, 128, 256},
+       "threads per matrix of the tridiagonal eigenpairs (0: 128 for a range of eigenpairs, 256 for all)", 0},
       {"bt.columns", 16, {16, 32},
        "eigenvector columns per CTA of the blocked back-transform (32: 512 threads, up to 512 rows; "
        "not autotuned: 6 % faster back-transform but a slower whole call on the 2048-step batch)",

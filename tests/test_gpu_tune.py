@@ -36,7 +36,7 @@ def test_autotune_pipeline(ctx):
     pl.process_device(64, S.data_ptr(), x.data_ptr(), wl.data_ptr())
     base = pl.images().astype(np.float64)
     names = ("spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-             "hetrd.threads", "hetrd.ctas_pct", "vv.ctas_per_sm")
+             "hetrd.threads", "hetrd.ctas_pct", "tridiag.threads", "vv.ctas_per_sm")
     start = {name: bipp.tuning_get(name) for name in names}
     rep = pl.autotune(64, S.data_ptr(), x.data_ptr(), wl.data_ptr(), on_device=True, repeats=1)
     print(rep)
@@ -127,7 +127,7 @@ def test_persistent_tridiagonalisation_agrees(ctx):
     wl = np.full(40, cfg.wl, np.float32)
     v0, d0, n0, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
     try:
-        for pct in (("hetrd.ctas_pct", 50), ("hetrd.ctas_pct", 150), ("bt.columns", 32)):
+        for pct in (("hetrd.ctas_pct", 50), ("hetrd.ctas_pct", 150), ("bt.columns", 32), ("tridiag.threads", 128)):
             bipp.tuning_reset()
             bipp.tuning_set(*pct)
             v1, d1, n1, _ = bipp.eigh_gram_batched(wl, s, x, ctx=ctx)
