@@ -137,8 +137,101 @@ NufftCore::~NufftCore() {
   for (auto& kv : plans_) cufftDestroy(kv.second);
 }
 
-// batched inverse 2-D FFT of every (channel, plane) array of the slab
-void NufftCore::inverse_fft(int slabPlanes, float2* slab) {
+// Plan of one pass of the pruned FFT over lines of n values keeping nout outputs, with its
+// compiled kernel (false when n has none: the caller uses cuFFT). Radices: the odd factor
+// first, then the power of two 2^a (a >= 4, as the grid sizes are multiples of 16) as 16s
+// with a remainder of 8 x 4 (a = 5 left), 8, 4 or 2; a lone radix-16 stage becomes 4 x 4,
+// so the first stage's reads precede a barrier that the last stage's in-place writes
+// follow. Threads per line: the fewest warps with which no thread holds more than
+// kFftMaxValues values in any stage. Lines per CTA: 256 threads for the row pass; 4 lines
+// for the column pass (a warp reads 32-byte row segments).
+static bool make_fft_plan(int n, int nout, bool columnPass, FftLinePlan& pl, FftLinesKernel& kernel) {
+  kernel = nullptr;
+  pl = FftLinePlan{};
+  pl.n = n;
+  pl.nout = nout;
+  std::vector<int> r;
+  int m = n;
+  for (int f : {7, 5, 3})
+    while (m % f == 0) {
+      r.push_back(f);
+      m /= f;
+    }
+  int a = 0;
+  while (m % 2 == 0) {
+    ++a;
+    m /= 2;
+  }
+  if (m != 1 || a < 4 || nout < 1 || nout > n) return false;
+  while (a >= 4 && a != 5) {
+    r.push_back(16);
+    a -= 4;
+  }
+  if (a == 5) {
+    r.push_back(8);
+    r.push_back(4);
+  } else if (a == 3) {
+    r.push_back(8);
+  } else if (a == 2) {
+    r.push_back(4);
+  } else if (a == 1) {
+    r.push_back(2);
+  }
+  if (r.size() == 1 && r[0] == 16) r = {4, 4};
+  if (r.size() < 2 || r.size() > (size_t)kFftMaxStages) return false;
+  int T = 32;
+  for (;; T += 32) {
+    if (T > 512) return false;
+    bool ok = true;
+    for (int R : r) ok = ok && (n / R + T - 1) / T <= kFftMaxValues / R;
+    if (ok) break;
+  }
+  pl.ns = (int)r.size();
+  for (int s = 0; s < pl.ns; ++s) pl.radix[s] = r[s];
+  pl.threads = T;
+  pl.lineStride = (fft_pad(n - 1) + 1 + 15) / 16 * 16 + 4;
+  int G = columnPass ? std::min(4, 512 / T) : std::max(1, 256 / T);
+  while (G > 1 && (size_t)G * pl.lineStride * sizeof(float2) > (size_t)227 * 1024) --G;
+  if ((size_t)G * pl.lineStride * sizeof(float2) > (size_t)227 * 1024) return false;
+  pl.lines = G;
+  kernel = fft_lines_kernel_for(pl.radix, pl.ns, columnPass);
+  return kernel != nullptr;
+}
+
+// batched inverse 2-D FFT of the (channel, plane) arrays of the slab
+void NufftCore::inverse_fft(int slabPlanes, int planesUsed, float2* slab, bool pruned) {
+  if (pruned) {
+    FftLines L{};
+    L.data = slab;
+    L.planesUsed = planesUsed;
+    L.slabPlanes = slabPlanes;
+    L.planeStride = (long long)g_.nx * g_.ny;
+    // pass 1: every row along x, keeping Nb outputs
+    L.linesPerPlane = g_.ny;
+    L.nLines = (long long)nch_ * planesUsed * g_.ny;
+    L.lineStep = g_.nx;
+    L.elemStep = 1;
+    size_t smem = (size_t)rowPlan_.lines * rowPlan_.lineStride * sizeof(float2);
+    B2_CUDA(cudaFuncSetAttribute((const void*)rowKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    count_launch();
+    rowKernel_<<<(unsigned)((L.nLines + rowPlan_.lines - 1) / rowPlan_.lines),
+                              rowPlan_.lines * rowPlan_.threads, smem, ctx_->stream>>>(rowPlan_, L,
+                                                                                       fftTw_.get<float2>());
+    B2_CHECK_LAUNCH();
+    // pass 2: the Nb kept columns along y, keeping Na outputs
+    L.linesPerPlane = g_.Nb;
+    L.nLines = (long long)nch_ * planesUsed * g_.Nb;
+    L.lineStep = 1;
+    L.elemStep = g_.nx;
+    smem = (size_t)colPlan_.lines * colPlan_.lineStride * sizeof(float2);
+    B2_CUDA(cudaFuncSetAttribute((const void*)colKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    count_launch();
+    colKernel_<<<(unsigned)((L.nLines + colPlan_.lines - 1) / colPlan_.lines),
+                             colPlan_.lines * colPlan_.threads, smem, ctx_->stream>>>(
+        colPlan_, L, fftTw_.get<float2>() + g_.nx);
+    B2_CHECK_LAUNCH();
+    return;
+  }
   const int batch = nch_ * slabPlanes;
   auto it = plans_.find(batch);
   if (it == plans_.end()) {
@@ -178,6 +271,18 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   g_.ny = std::max(g_.ny, 2 * g_.W);
   g_.hx = 2.0 * M_PI / g_.nx;
   g_.hy = 2.0 * M_PI / g_.ny;
+  fftPlansOk_ = make_fft_plan(g_.nx, g_.Nb, false, rowPlan_, rowKernel_) &&
+                make_fft_plan(g_.ny, g_.Na, true, colPlan_, colKernel_);
+  if (fftPlansOk_) {
+    std::vector<float2> tw((size_t)g_.nx + g_.ny);
+    for (int i = 0; i < g_.nx; ++i)
+      tw[i] = make_float2((float)std::cos(2.0 * M_PI * i / g_.nx), (float)std::sin(2.0 * M_PI * i / g_.nx));
+    for (int i = 0; i < g_.ny; ++i)
+      tw[(size_t)g_.nx + i] =
+          make_float2((float)std::cos(2.0 * M_PI * i / g_.ny), (float)std::sin(2.0 * M_PI * i / g_.ny));
+    fftTw_.alloc(ctx, tw.size() * sizeof(float2));
+    h2d(ctx, fftTw_.get(), tw.data(), tw.size() * sizeof(float2));
+  }
   const long long P = (long long)g_.Na * g_.Nb;
   require((long long)n.size() == P, "pixel n size mismatch");
   double nmin = *std::min_element(n.begin(), n.end()), nmax = *std::max_element(n.begin(), n.end());
@@ -355,6 +460,7 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
   // slab (empty, or split into parts that accumulate with atomics) are cleared first from
   // a compact list; the warp spreader works on a cleared slab
   const bool tc = use_tensor_core_spread(nch_);
+  const bool prunedFft = fftPlansOk_ && tuned("nufft.fft") == 1;
   const int tb = std::min(8192, (ntiles + 255) / 256);
   clearFlag_.ensure(ctx_, (size_t)ntiles * sizeof(int));
   clearOff_.ensure(ctx_, (size_t)(ntiles + 1) * sizeof(int));
@@ -491,13 +597,13 @@ void NufftCore::execute(float* image, long long ldImage, double* stageMs) {
       B2_CHECK_LAUNCH();
     }
     if (stageMs) B2_CUDA(cudaEventRecord(ev[1], ctx_->stream));
-    inverse_fft(slabPlanes, grid_.get<float2>());
+    inverse_fft(slabPlanes, tiles * kTW, grid_.get<float2>(), prunedFft);
     if (stageMs) B2_CUDA(cudaEventRecord(ev[2], ctx_->stream));
     const int blocks = (int)std::min<long long>((P + 255) / 256, 65535);
     count_launch();
     auto wk = nch_ <= 4 ? wsum_kernel<4> : wsum_kernel<kMaxChan>;
     wk<<<blocks, 256, 0, ctx_->stream>>>(g_, grid_.get<float2>(), nch_, slabPlanes, tw0 * kTW, tiles * kTW,
-                                         nTilde_.get<double>(), acc_.get<float2>(), P);
+                                         nTilde_.get<double>(), acc_.get<float2>(), P, prunedFft ? 1 : 0);
     B2_CHECK_LAUNCH();
     if (stageMs) {
       B2_CUDA(cudaEventRecord(ev[3], ctx_->stream));

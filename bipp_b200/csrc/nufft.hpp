@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "context.hpp"
+#include "fft_kernels.cuh"
 #include "nufft_kernels.cuh"
 
 namespace bippb200 {
@@ -82,8 +83,16 @@ private:
   DevBuf valScale_;   // per-channel value scale of the FP16 spreader operands
   // batched 2-D cuFFT plans by batch size (channels x slab planes)
   std::map<int, cufftHandle> plans_;
+  // pruned two-pass inverse FFT (rows along x, then the kept columns along y) and its
+  // twiddle tables (nx entries for the rows, then ny for the columns)
+  FftLinePlan rowPlan_{}, colPlan_{};
+  FftLinesKernel rowKernel_ = nullptr, colKernel_ = nullptr;
+  bool fftPlansOk_ = false;
+  DevBuf fftTw_;
   int slabTiles_ = 1;
-  void inverse_fft(int slabPlanes, float2* slab);
+  // inverse 2-D FFT of the first planesUsed planes of every channel of the slab: pruned
+  // (cell (a, b) of a plane then holds pixel (a, b)'s output) or in full by cuFFT
+  void inverse_fft(int slabPlanes, int planesUsed, float2* slab, bool pruned);
   void exclusive_scan(const int* in, int* out, long long n);
 
 public:

@@ -619,13 +619,19 @@ template <int CH, int kWsumUnroll = (CH <= 4 ? 4 : 1)>
 static __global__ void __launch_bounds__(256) wsum_kernel(NufftGeom g, const float2* __restrict__ F, int nch,
                                                            int slabPlanes, int jFirst, int planesUsed,
                                                            const double* __restrict__ nTilde /*[P]*/,
-                                                           float2* __restrict__ acc, long long accStride) {
+                                                           float2* __restrict__ acc, long long accStride,
+                                                           int pruned) {
   const long long P = (long long)g.Na * g.Nb;
   const long long planeStride = (long long)g.ny * g.nx;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
     const int a = (int)(p / g.Nb), b = (int)(p % g.Nb);
-    int ap = a - g.Na / 2; if (ap < 0) ap += g.ny;
-    int bp = b - g.Nb / 2; if (bp < 0) bp += g.nx;
+    // pixel (a, b) reads frequency ((a - Na/2) mod ny, (b - Nb/2) mod nx): that cell of a
+    // full transform, or cell (a, b) of the pruned one (fft_kernels.cuh)
+    int ap = a, bp = b;
+    if (!pruned) {
+      ap = a - g.Na / 2; if (ap < 0) ap += g.ny;
+      bp = b - g.Nb / 2; if (bp < 0) bp += g.nx;
+    }
     const double nt = nTilde[p];
     // exp(i nt t_j), t_j = (j - jc) hw; recurrence in FP64
     double s0, c0, sd, cd;

@@ -63,6 +63,10 @@ std::vector<Param>& table() {
        0},
       {"vv.ctas_per_sm", 3, {1, 2, 3}, "persistent tensor-core virtual-visibility CTAs per SM", 0},
       {"direct.ctas_per_sm", 4, {2, 4, 8}, "direct-sum CTAs per SM below which the inputs are split", 0},
+      {"nufft.fft", 1, {0, 1},
+       "inverse FFT of the w-planes: 1 = pruned two-pass transform that computes only the cells the pixels read "
+       "(when the grid sizes have a plan), 0 = full 2-D cuFFT transform (not autotuned)",
+       0},
       {"nufft.grid_per_1024", 1792, {1680, 1728, 1792},
        "NUFFT fine-grid cells per 1024 pixels (oversampling x 1024; read when a NUFFT is set up; not autotuned, "
        "as it trades accuracy for speed)",

@@ -360,7 +360,7 @@ BIPP_B200_EXPORT BippError bipp_pipeline_kernel_times(bipp_pipeline_t pl, double
 /* Statistics of the last NUFFT of the pipeline (9 values): points spread, spreading
  * launches (w-slabs), grid bytes written by the spreading, spreading work items, fine
  * grid sizes nx, ny, nw, kernel width W, tiles split into several work items (more points
- * than the spread.items_cap tuning parameter, 4096 by default; their parts accumulate into
+ * than the spread.items_cap tuning parameter, 2048 by default; their parts accumulate into
  * the grid with atomics). */
 BIPP_B200_EXPORT BippError bipp_pipeline_nufft_stats(bipp_pipeline_t pl, long long* stats);
 BIPP_B200_EXPORT BippError bipp_pipeline_destroy(bipp_pipeline_t pl);

@@ -154,7 +154,8 @@ def test_tuning_table_without_a_gpu(tmp_path):
     assert bipp.tuning_get("spread.items_cap") == 2048 and bipp.tuning_get("hetrd.threads") == 0
     desc = bipp.tuning_describe()
     assert set(desc) == {"spread.items_cap", "spread.operands", "spread.stages", "spread.ctas_per_sm", "spread.schedule",
-                         "hetrd.threads", "hetrd.ctas_pct", "tridiag.threads", "bt.columns", "vv.ctas_per_sm", "direct.ctas_per_sm", "nufft.grid_per_1024"}
+                         "hetrd.threads", "hetrd.ctas_pct", "tridiag.threads", "bt.columns", "vv.ctas_per_sm", "direct.ctas_per_sm", "nufft.fft",
+                         "nufft.grid_per_1024"}
     assert desc["spread.items_cap"]["candidates"] == [2048, 4096, 8192]
     with pytest.raises(bipp.InvalidParameterError):
         bipp.tuning_set("spread.items_cap", 1000)

@@ -100,6 +100,44 @@ def test_nufft_collect_get_lattice(ctx, tol):
     plan.close()
 
 
+def test_pruned_fft_rectangular_lattice(ctx):
+    """A 40 x 64-pixel lattice (fine grid 80 x 112: the pruned inverse FFT's row pass of
+    112 = 7 x 16 keeps 64 of the columns, its column pass of 80 = 5 x 16 keeps 40 rows)
+    images like the FP64 direct sum with the pruned transform and with the full 2-D cuFFT
+    transform (nufft.fft = 0), and the two differ in their rounding only, so the pruned
+    kernels, not a fallback, ran."""
+    import bipp_b200 as bipp
+
+    rng = np.random.default_rng(17)
+    na, nb_ = 40, 64
+    a, b = np.meshgrid(np.arange(na), np.arange(nb_), indexing="ij")
+    l = (b.reshape(-1) - nb_ / 2 + 0.5) * 3.1e-3
+    m = (a.reshape(-1) - na / 2 + 0.25) * 2.7e-3
+    lmn = np.stack([l, m, np.sqrt(1 - l * l - m * m)], 1).astype(np.float32)
+    npts = 900
+    pts = [_synthetic_points(rng, npts, 700.0, 60.0) for _ in range(2)]
+    uvw = np.concatenate([p[0] for p in pts]).astype(np.float32).astype(np.float64)
+    c = np.concatenate([p[1] for p in pts]).astype(np.complex64).astype(np.complex128)
+    l64 = lmn.astype(np.float64)
+    imgs = {}
+    try:
+        for fft in (1, 0):
+            bipp.tuning_set("nufft.fft", fft)
+            plan = bipp.NufftSynthesis(ctx, bipp.NufftSynthesisOptions().set_tolerance(1e-7), lmn, 2, npts)
+            for u, v in pts:
+                plan.add(u.astype(np.float32), v.astype(np.complex64))
+            imgs[fft] = [plan.get_image(i) for i in range(2)]
+            plan.close()
+    finally:
+        bipp.tuning_reset()
+    for i in range(2):
+        ref_img = bb.nuft_sum(1.0, c[:, i], uvw[:, 0], uvw[:, 1], uvw[:, 2], l64[:, 0], l64[:, 1], l64[:, 2])
+        for fft in (0, 1):
+            assert _rel_l2(imgs[fft][i], ref_img) <= 2e-6, (fft, i)
+        assert _rel_l2(imgs[1][i], imgs[0][i]) <= 1e-6
+        assert not np.array_equal(imgs[1][i], imgs[0][i])
+
+
 def test_nufft_collect_get_four_images_warp_spreader(ctx):
     """Four images on a make_grids lattice with the first-order residual channels active:
     12 channels, more than the tensor-core spreader takes, so the warp spreader with
