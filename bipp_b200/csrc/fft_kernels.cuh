@@ -21,8 +21,8 @@
 // first stage reads its inputs straight from global memory and the last writes the kept
 // outputs straight back; the stages between exchange through shared memory in place
 // (every thread reads all of its inputs, the block synchronises, then every thread
-// writes). Shared-memory slots are padded by one per 16 (the stride-R writes of a stage
-// otherwise fall into a few banks). Sign convention: exp(+2 pi i jk/n), unnormalised, as
+// writes). Shared-memory slots are padded (the stride-R writes of a stage otherwise fall
+// into a few banks; FftBlockPad). Butterfly additions are packed FP32x2. Sign convention: exp(+2 pi i jk/n), unnormalised, as
 // an inverse cuFFT transform.
 #pragma once
 
@@ -83,19 +83,25 @@ __device__ __forceinline__ float2 fft_rot16(float2 z, int m) {
   }
 }
 
+// complex a + b and a - b as packed FP32x2 instructions (a - b = b (-1) + a, one rounding,
+// the same value as two scalar subtractions)
+__device__ __forceinline__ float2 fft_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fft_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
 __device__ __forceinline__ void fft_dft2(float2& a, float2& b) {
   const float2 t = a;
-  a = t + b;
-  b = t - b;
+  a = fft_add(t, b);
+  b = fft_sub(t, b);
 }
 
 // X_k = sum_j x_j exp(2 pi i jk / 4)
 __device__ __forceinline__ void fft_dft4(float2& x0, float2& x1, float2& x2, float2& x3) {
-  const float2 a = x0 + x2, b = x0 - x2, c = x1 + x3, d = fft_mul_i(x1 - x3);
-  x0 = a + c;
-  x2 = a - c;
-  x1 = b + d;
-  x3 = b - d;
+  const float2 a = fft_add(x0, x2), b = fft_sub(x0, x2), c = fft_add(x1, x3), t = fft_sub(x1, x3);
+  x0 = fft_add(a, c);
+  x2 = fft_sub(a, c);
+  // b +- i t
+  x1 = mk(b.x - t.y, b.y + t.x);
+  x3 = mk(b.x + t.y, b.y - t.x);
 }
 
 // odd radix by the symmetric form: s_j = x_j + x_{R-j}, d_j = x_j - x_{R-j};
@@ -107,9 +113,9 @@ __device__ __forceinline__ void fft_dft_odd(float2 (&x)[R], const float (&cs)[R]
   float2 x0 = x[0];
 #pragma unroll
   for (int j = 1; j <= H; ++j) {
-    s[j] = x[j] + x[R - j];
-    d[j] = x[j] - x[R - j];
-    x0 = x0 + s[j];
+    s[j] = fft_add(x[j], x[R - j]);
+    d[j] = fft_sub(x[j], x[R - j]);
+    x0 = fft_add(x0, s[j]);
   }
 #pragma unroll
   for (int k = 1; k <= H; ++k) {
@@ -217,16 +223,31 @@ __device__ __forceinline__ void fft_apply_twiddles(float2 (&v)[R], const float2*
   }
 }
 
+// Shared-memory slots of a line. The general layout pads one slot per 16 (fft_pad). Lines
+// of N = 256 c (radices c, 16, 16, c odd) use a block layout instead: slot(i) = i + c
+// floor(i / B), B = 16 c, under which every access of the three stages is a per-butterfly
+// base plus a compile-time offset and stays free of bank conflicts: stage 1 writes
+// c b + j -> c b + c floor(b / 16) + j; stages 2 and 3 read b + j B (b < B) -> b + j (B + c);
+// stage 2 writes 16 c q + k + j c (q = floor(b / c), k = b mod c) -> (B + c) q + k + j c, and
+// a half-warp's 16 consecutive b then fall in 16 distinct bank pairs.
+template <int N, int... Rs> struct FftBlockPad {
+  static constexpr int radix[sizeof...(Rs)] = {Rs...};
+  static constexpr bool on = sizeof...(Rs) == 3 && radix[1] == 16 && radix[2] == 16 && (radix[0] & 1) == 1;
+  static constexpr int c = radix[0], B = 16 * radix[0];
+};
+
 // One stage of radix R over the line of this thread's group (see the file comment); N the
 // line length, P the product of the earlier radices, MODE 0 first, 1 middle, 2 last; ES the
 // compile-time stride between a line's values in global memory (1 for rows; 0 takes the
-// runtime es); offsets within one (channel, plane) array fit 32 bits.
-template <int R, int MODE, int N, int P, int ES>
+// runtime es); offsets within one (channel, plane) array fit 32 bits; BP the block slot
+// layout (FftBlockPad) when on, with its c.
+template <int R, int MODE, int N, int P, int ES, bool BP, int BPC>
 __device__ __forceinline__ void fft_stage(const FftLinePlan& pl, int t, bool active, float2* __restrict__ lp, int es,
                                           float2* __restrict__ sl, const float2* __restrict__ tw) {
   constexpr bool first = MODE == 0, last = MODE == 2;
   constexpr int MB = kFftMaxValues / R;   // butterflies per thread (the plan's thread count ensures enough)
   constexpr int Nr = N / R, twStep = N / (P * R);
+  constexpr int BPB = 16 * BPC;           // block of the block layout
   const int T = pl.threads;
   const int st = ES > 0 ? ES : es;
   float2 v[MB][R];
@@ -238,6 +259,7 @@ __device__ __forceinline__ void fft_stage(const FftLinePlan& pl, int t, bool act
       for (int j = 0; j < R; ++j) {
         const int i = b + j * Nr;
         if constexpr (first) v[q][j] = active ? lp[i * st] : mk(0.f, 0.f);
+        else if constexpr (BP) v[q][j] = sl[b + j * (BPB + BPC)];   // Nr == B in stages 2 and 3
         else v[q][j] = sl[fft_pad(i)];
       }
     }
@@ -252,15 +274,28 @@ __device__ __forceinline__ void fft_stage(const FftLinePlan& pl, int t, bool act
       const int k = b % P;
       if constexpr (P > 1) fft_apply_twiddles<R>(v[q], tw, k * twStep);
       fft_dft<R>(v[q]);
-      const int o = (b - k) * R + k;
+      if constexpr (last) {
+        // in the last stage b < P, so output j is i = b + j P; the kept ones are i < nout - h
+        // (cell i + h) and i >= N - h (cell i - (N - h)), h = nout / 2 (fft_crop): the j
+        // ranges of both are found once
+        const int h = pl.nout >> 1, lo = pl.nout - h, hi = N - h;
+        const int j1 = lo > b ? (lo - b + P - 1) / P : 0;
+        const int j2 = hi > b ? (hi - b + P - 1) / P : 0;
+        const int offLo = (b + h) * st, offHi = (b - hi) * st;
 #pragma unroll
-      for (int j = 0; j < R; ++j) {
-        const int i = o + j * P;
-        if constexpr (last) {
-          const int d = fft_crop(i, N, pl.nout);
-          if (active && d >= 0) lp[d * st] = v[q][j];
-        } else {
-          sl[fft_pad(i)] = v[q][j];
+        for (int j = 0; j < R; ++j) {
+          if (active && j < j1) lp[offLo + j * P * st] = v[q][j];
+          else if (active && j >= j2) lp[offHi + j * P * st] = v[q][j];
+        }
+      } else {
+        const int o = (b - k) * R + k;
+        int base = 0;
+        if constexpr (BP && P == 1) base = BPC * b + BPC * (b >> 4);   // stage 1: c b + c floor(b / 16)
+        else if constexpr (BP) base = (BPB + BPC) * (b / BPC) + k;      // stage 2: (B + c) q + k
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          if constexpr (BP) sl[base + j * P] = v[q][j];
+          else sl[fft_pad(o + j * P)] = v[q][j];
         }
       }
     }
@@ -268,11 +303,12 @@ __device__ __forceinline__ void fft_stage(const FftLinePlan& pl, int t, bool act
   if constexpr (!last) __syncthreads();
 }
 
-template <int S, int N, int P, int ES, int R, int... Rest>
+template <int S, int N, int P, int ES, bool BP, int BPC, int R, int... Rest>
 __device__ __forceinline__ void fft_stages(const FftLinePlan& pl, int t, bool active, float2* __restrict__ lp, int es,
                                            float2* __restrict__ sl, const float2* __restrict__ tw) {
-  fft_stage<R, S == 0 ? 0 : (sizeof...(Rest) == 0 ? 2 : 1), N, P, ES>(pl, t, active, lp, es, sl, tw);
-  if constexpr (sizeof...(Rest) > 0) fft_stages<S + 1, N, P * R, ES, Rest...>(pl, t, active, lp, es, sl, tw);
+  fft_stage<R, S == 0 ? 0 : (sizeof...(Rest) == 0 ? 2 : 1), N, P, ES, BP, BPC>(pl, t, active, lp, es, sl, tw);
+  if constexpr (sizeof...(Rest) > 0)
+    fft_stages<S + 1, N, P * R, ES, BP, BPC, Rest...>(pl, t, active, lp, es, sl, tw);
 }
 
 // The pass over lines of N = the product of the radices Rs (at least two stages).
@@ -300,8 +336,9 @@ __global__ void __launch_bounds__(512, 2) fft_lines_kernel(FftLinePlan pl, FftLi
     base = ((long long)c * L.slabPlanes + pj) * L.planeStride + (long long)li * L.lineStep;
   }
   // rows: unit stride (compile time); columns: the row length
-  fft_stages<0, N, 1, LINE_FAST ? 0 : 1, Rs...>(pl, t, active, L.data + base, (int)L.elemStep,
-                                                fft_smem + (size_t)g * pl.lineStride, tw);
+  using BPad = FftBlockPad<N, Rs...>;
+  fft_stages<0, N, 1, LINE_FAST ? 0 : 1, BPad::on, BPad::c, Rs...>(pl, t, active, L.data + base, (int)L.elemStep,
+                                                                   fft_smem + (size_t)g * pl.lineStride, tw);
 }
 
 using FftLinesKernel = void (*)(FftLinePlan, FftLines, const float2*);

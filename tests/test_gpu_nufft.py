@@ -100,19 +100,22 @@ def test_nufft_collect_get_lattice(ctx, tol):
     plan.close()
 
 
-def test_pruned_fft_rectangular_lattice(ctx):
-    """A 40 x 64-pixel lattice (fine grid 80 x 112: the pruned inverse FFT's row pass of
-    112 = 7 x 16 keeps 64 of the columns, its column pass of 80 = 5 x 16 keeps 40 rows)
-    images like the FP64 direct sum with the pruned transform and with the full 2-D cuFFT
-    transform (nufft.fft = 0), and the two differ in their rounding only, so the pruned
-    kernels, not a fallback, ran."""
+@pytest.mark.parametrize("na,nb_", [(40, 64), (16, 1024), (24, 432)])
+def test_pruned_fft_rectangular_lattice(ctx, na, nb_):
+    """Rectangular pixel lattices whose fine grids take different pruned-FFT plans for the
+    rows (along x) and the columns (along y): 40 x 64 px -> 80 x 112 cells (rows
+    112 = 7 x 16, columns 80 = 5 x 16), 16 x 1024 px -> 32 x 1792 (rows 7 x 16 x 16 with
+    the block shared-memory layout, the 1024^2-pixel workload's row length; columns 8 x 4),
+    24 x 432 px -> 48 x 768 (rows 3 x 16 x 16, columns 3 x 16). Each images like the FP64
+    direct sum with the pruned transform and with the full 2-D cuFFT transform
+    (nufft.fft = 0); the two differ in their rounding only, so the pruned kernels, not a
+    fallback, ran."""
     import bipp_b200 as bipp
 
     rng = np.random.default_rng(17)
-    na, nb_ = 40, 64
     a, b = np.meshgrid(np.arange(na), np.arange(nb_), indexing="ij")
-    l = (b.reshape(-1) - nb_ / 2 + 0.5) * 3.1e-3
-    m = (a.reshape(-1) - na / 2 + 0.25) * 2.7e-3
+    l = (b.reshape(-1) - nb_ / 2 + 0.5) * (0.2 / nb_)
+    m = (a.reshape(-1) - na / 2 + 0.25) * (0.11 / na)
     lmn = np.stack([l, m, np.sqrt(1 - l * l - m * m)], 1).astype(np.float32)
     npts = 900
     pts = [_synthetic_points(rng, npts, 700.0, 60.0) for _ in range(2)]
