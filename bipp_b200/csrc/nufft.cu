@@ -212,7 +212,6 @@ void NufftCore::inverse_fft(int slabPlanes, int planesUsed, float2* slab, bool p
     L.lineStep = g_.nx;
     L.elemStep = 1;
     size_t smem = (size_t)rowPlan_.lines * rowPlan_.lineStride * sizeof(float2);
-    B2_CUDA(cudaFuncSetAttribute((const void*)rowKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     count_launch();
     rowKernel_<<<(unsigned)((L.nLines + rowPlan_.lines - 1) / rowPlan_.lines),
                               rowPlan_.lines * rowPlan_.threads, smem, ctx_->stream>>>(rowPlan_, L,
@@ -224,7 +223,6 @@ void NufftCore::inverse_fft(int slabPlanes, int planesUsed, float2* slab, bool p
     L.lineStep = 1;
     L.elemStep = g_.nx;
     smem = (size_t)colPlan_.lines * colPlan_.lineStride * sizeof(float2);
-    B2_CUDA(cudaFuncSetAttribute((const void*)colKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     count_launch();
     colKernel_<<<(unsigned)((L.nLines + colPlan_.lines - 1) / colPlan_.lines),
                              colPlan_.lines * colPlan_.threads, smem, ctx_->stream>>>(
@@ -274,6 +272,11 @@ void NufftCore::setup(bipp_ctx_s* ctx, const Lattice& lat, const std::vector<dou
   fftPlansOk_ = make_fft_plan(g_.nx, g_.Nb, false, rowPlan_, rowKernel_) &&
                 make_fft_plan(g_.ny, g_.Na, true, colPlan_, colKernel_);
   if (fftPlansOk_) {
+    // the passes' shared memory, set once here rather than before every launch
+    B2_CUDA(cudaFuncSetAttribute((const void*)rowKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)((size_t)rowPlan_.lines * rowPlan_.lineStride * sizeof(float2))));
+    B2_CUDA(cudaFuncSetAttribute((const void*)colKernel_, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)((size_t)colPlan_.lines * colPlan_.lineStride * sizeof(float2))));
     std::vector<float2> tw((size_t)g_.nx + g_.ny);
     for (int i = 0; i < g_.nx; ++i)
       tw[i] = make_float2((float)std::cos(2.0 * M_PI * i / g_.nx), (float)std::sin(2.0 * M_PI * i / g_.nx));
