@@ -183,15 +183,6 @@ template <int R> __device__ __forceinline__ void fft_dft(float2 (&x)[R]) {
   }
 }
 
-// output i of a line of n values -> its cell among the nout kept ones (frequency
-// (d - nout/2) mod n at cell d), or -1 when no pixel reads it
-__device__ __forceinline__ int fft_crop(int i, int n, int nout) {
-  const int h = nout >> 1;
-  if (i < nout - h) return i + h;
-  if (i >= n - h) return i - (n - h);
-  return -1;
-}
-
 // Multiply input j (j = 1 .. R-1) of a butterfly by its twiddle w_j = exp(2 pi i j k / (P R))
 // = tw[j m]: w_1 (and, for R >= 8, w_4) from the table, the others as products at most
 // three deep (w_2 = w_1^2, w_3 = w_2 w_1, w_8 = w_4^2, w_12 = w_8 w_4, w_{4a+b} = w_{4a} w_b),
@@ -275,9 +266,10 @@ __device__ __forceinline__ void fft_stage(const FftLinePlan& pl, int t, bool act
       if constexpr (P > 1) fft_apply_twiddles<R>(v[q], tw, k * twStep);
       fft_dft<R>(v[q]);
       if constexpr (last) {
-        // in the last stage b < P, so output j is i = b + j P; the kept ones are i < nout - h
-        // (cell i + h) and i >= N - h (cell i - (N - h)), h = nout / 2 (fft_crop): the j
-        // ranges of both are found once
+        // in the last stage b < P, so output j is frequency i = b + j P. Cell d of the nout
+        // kept ones holds frequency (d - h) mod N, h = nout / 2: i < nout - h goes to cell
+        // i + h, i >= N - h to cell i - (N - h), the others are not kept. The j ranges of
+        // both are found once per butterfly
         const int h = pl.nout >> 1, lo = pl.nout - h, hi = N - h;
         const int j1 = lo > b ? (lo - b + P - 1) / P : 0;
         const int j2 = hi > b ? (hi - b + P - 1) / P : 0;
