@@ -1188,19 +1188,18 @@ __device__ __forceinline__ void hetrd_blk_matrix(C* __restrict__ A, const int* _
           if (lane == 0) tq[(wq < j ? 0 : kTrdNB) + q] = acc;
         }
         __syncthreads();
-        // y -= V (W^H v) + W (V^H v)
-        for (int r = tid; r < m; r += T) {
-          const C* rw = VW + (long long)(c + 1 + r) * kTrdVWS;
-          C s = y[r];
-          for (int q = 0; q < j; ++q) s = s - cmul(rw[2 * q], tq[q]) - cmul(rw[2 * q + 1], tq[kTrdNB + q]);
-          y[r] = s;
-        }
-        __syncthreads();
       }
-      // w = tau y - 1/2 tau ((tau y)^H v) v  -> W column j
+      // y -= V (W^H v) + W (V^H v) (j > 0), then w = tau y - 1/2 tau ((tau y)^H v) v -> W
+      // column j. Each thread reads and writes only its own rows r of y here (tq and v were
+      // published before the last barrier), so one pass does both
       R pr = 0, pi = 0;
       for (int r = tid; r < m; r += T) {
-        const C wv = cmul(tau, y[r]);
+        C s = y[r];
+        if (j > 0) {
+          const C* rw = VW + (long long)(c + 1 + r) * kTrdVWS;
+          for (int q = 0; q < j; ++q) s = s - cmul(rw[2 * q], tq[q]) - cmul(rw[2 * q + 1], tq[kTrdNB + q]);
+        }
+        const C wv = cmul(tau, s);
         y[r] = wv;
         const C pv = cconjmul(wv, v[r]);
         pr += pv.x;
