@@ -81,7 +81,8 @@ private:
   DevBuf itemKeys_, itemsAlt_, sortTmp_, workCounters_;
   DevBuf qz_, qw_, zeroAcc_, load_, items_, errFlag_, splitCount_, parts_, itemOff_, itemSums_, clearFlag_, clearOff_, clearList_;
   DevBuf valScale_;   // per-channel value scale of the FP16 spreader operands
-  // batched 2-D cuFFT plans by batch size (channels x slab planes)
+  // batched 2-D cuFFT plans by batch size (channels x slab planes), for grid sizes without
+  // a compiled pruned-FFT plan or nufft.fft = 0
   std::map<int, cufftHandle> plans_;
   // pruned two-pass inverse FFT (rows along x, then the kept columns along y) and its
   // twiddle tables (nx entries for the rows, then ny for the columns)

@@ -38,9 +38,11 @@ struct NufftGeom {
 
 // Fine-grid slab layout: cell (channel c, plane, y, x) of a slab of slabPlanes w-planes at
 // ((c slabPlanes + plane) ny + y) nx + x, i.e. [channel][plane][y][x]: every (channel,
-// plane) is one contiguous ny x nx array, transformed by one batched 2-D cuFFT plan. (A
-// [y][channel][plane][x] layout that let the pass along x skip the rows no pixel reads
-// made cuFFT's strided pass along y three times slower than the whole 2-D transform.)
+// plane) is one contiguous ny x nx array, transformed in place by the pruned two-pass FFT
+// (fft_kernels.cuh: rows, then the kept columns), or by one batched 2-D cuFFT plan for
+// grid sizes without a compiled pruned plan. (A [y][channel][plane][x] layout that let
+// the pass along x skip the rows no pixel reads made cuFFT's strided pass along y three
+// times slower than the whole 2-D transform.)
 __host__ __device__ __forceinline__ long long slab_index(const NufftGeom& g, int nch, int slabPlanes, int c, int plane,
                                                        int y, int x) {
   (void)nch;
